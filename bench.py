@@ -1,0 +1,334 @@
+"""Benchmark: primary rays per second of the treelet ray cast on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+
+One step = one frame of the workload cast over its resident octree.  The
+device-timed ``value`` has the octree resident in HBM and times the render
+kernel with CUDA events (L2 flushed between steps by writing 256 MB).
+``e2e`` is the same metric through the C ABI call a user makes
+(svo_mm_render_host): kernel plus the copy of the RGBA8 image back to pinned
+host memory, every step.  ``roofline`` relates the kernel's algorithmic bytes
+(8 B per parent-node read, 8 B per hit attribute, 4 B per RGBA8 pixel,
+counted by the kernel's own per-ray counters) to the measured HBM copy
+bandwidth.  ``cpu_baseline`` times the reference's own ray cast compiled for
+the host (oracle/_ref; the oracle port when that is absent) on the host cores.
+
+With N > 1 (torchrun), each rank casts the same workload on its own GPU
+(replicas: rays are independent, there is no exchange), and the step time is
+the maximum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+
+METRIC = "Mrays/s"
+FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="menger")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.is_file():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def make_workload(name):
+    from libsvo_b200 import scenes
+
+    if name == "menger":
+        return scenes.menger()
+    if hasattr(scenes, name):
+        return getattr(scenes, name)()
+    raise SystemExit(f"unknown workload {name}")
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_frames(wl, nodes, attribs, seconds=10.0, max_frames=200):
+    """Times the reference's renderToBuffer compiled for the host (or the
+    oracle port) over whole frames of the workload, all host threads."""
+    import oracle
+
+    threads = os.cpu_count() or 1
+    ref = oracle.reference_lib() is not None
+    params = [bytes(c.frame_params()) for c in wl.cameras]
+    rays = 0
+    frames = 0
+    t0 = time.perf_counter()
+    while True:
+        for p in params:
+            if ref:
+                oracle.reference_render(nodes, attribs, p, threads=threads)
+            else:
+                oracle.render(nodes, attribs, p, stack_size=wl.stack_size, threads=threads)
+            w, h = np.frombuffer(p[:8], dtype=np.uint32)
+            rays += int(w) * int(h)
+        frames += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or frames >= max_frames:
+            break
+    return {"value": rays / el / 1e6, "unit": METRIC, "cores": threads,
+            "kind": "reference" if ref else "port",
+            "sample": f"{frames} whole frame(s) of the workload ({rays} rays) in {el:.1f} s; "
+                      + ("reference treeletRenderer_rgba.cl renderToBuffer compiled for the host"
+                         if ref else "oracle restatement of sample()")}
+
+
+def run_reference(args, wl):
+    import libsvo_b200 as L
+
+    mm = L.TreeletMemoryManagerCuda(wl.scene, wl.scene.info.treelet_bytes * wl.scene.info.num_treelets)
+    mm.insertAll()
+    nodes, attribs = mm.getIncoreBuffer()
+    for _ in range(max(1, args.warmup)):
+        cpu_reference_frames(wl, nodes, attribs, seconds=0.0, max_frames=1)
+    per = []
+    for _ in range(args.steps):
+        r = cpu_reference_frames(wl, nodes, attribs, seconds=0.0, max_frames=1)
+        per.append(r)
+    rays = wl.rays_per_step
+    vals = [p["value"] for p in per]
+    value = statistics.mean(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": rays / value / 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": wl.name, "description": wl.description, "rays_per_step": rays},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": per[0]["cores"],
+                         "kind": per[0]["kind"], "sample": f"one whole frame per step; {per[0]['sample']}"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        run_reference(args, make_workload(args.workload))
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    import libsvo_b200 as L
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    t_build = time.perf_counter()
+    wl = make_workload(args.workload)
+    info = wl.scene.info
+    build_s = time.perf_counter() - t_build
+    incore = info.treelet_bytes * info.num_treelets
+    stream = torch.cuda.Stream(device=dev)
+    mm = L.TreeletMemoryManagerCuda(wl.scene, incore, stream=stream)
+    mm.insertAll()
+    mm.initDeviceBuffer()
+    cfg = L.trace_cfg(L.TRAVERSAL_TREELET, wl.stack_size)
+    params = [c.frame_params() for c in wl.cameras]
+    outs = [torch.empty((p.height, p.width), dtype=torch.int32, device=dev) for p in params]
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+    rays = wl.rays_per_step
+
+    # algorithmic bytes of one step, from the kernel's own per-ray counters
+    fetches = hits = 0
+    with torch.cuda.stream(stream):
+        for p, o in zip(params, outs):
+            hb = torch.empty(p.width * p.height * 16, dtype=torch.uint8, device=dev)
+            mm.render(p, o, hb, cfg=cfg, stream=stream)
+            stream.synchronize()
+            h = hb.cpu().numpy().view(L.HIT_DTYPE)
+            fetches += int(h["fetches"].astype(np.int64).sum())
+            hits += int(h["hit"].astype(np.int64).sum())
+            del hb
+    algo_bytes = 8 * fetches + 8 * hits + 4 * rays
+
+    def step():
+        for p, o in zip(params, outs):
+            mm.render(p, o, None, cfg=cfg, stream=stream)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            flush.fill_(1)
+            step()
+    stream.synchronize()
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = ClockSampler(local_rank)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    with torch.cuda.stream(stream):
+        for i in range(args.steps):
+            flush.fill_(i)
+            starts[i].record(stream)
+            step()
+            ends[i].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    kernel_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    ms = statistics.mean(kernel_ms)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * rays / (ms * 1e-3) / 1e6
+
+    # end to end through the C ABI: host output buffers, image copied back each step
+    host_out = [torch.empty((p.height, p.width), dtype=torch.int32).pin_memory() for p in params]
+    for _ in range(max(1, args.warmup)):
+        for p, ho in zip(params, host_out):
+            mm.render_host(p, ho, cfg=cfg, stream=stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        for p, ho in zip(params, host_out):
+            mm.render_host(p, ho, cfg=cfg, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * rays / (e2e_ms * 1e-3) / 1e6
+    st = mm.sync(stream)
+
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        achieved = algo_bytes / (ms * 1e-3) / 1e9
+        traffic = None
+        tp = ROOT / "profiles" / "dram_traffic.json"
+        if tp.is_file():
+            traffic = json.loads(tp.read_text()).get(wl.name)
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scene generators; see libsvo_b200/scenes.py)",
+            "config": {"workload": wl.name, "description": wl.description, "rays_per_step": rays,
+                       "octree_nodes": int(info.total_nodes), "treelets": int(info.num_treelets),
+                       "treelet_bytes": int(info.treelet_bytes), "stack_size": wl.stack_size,
+                       "l2": "flushed between steps (256 MB write)",
+                       "parallelism": f"replicas x{world}", "scene_build_s": round(build_s, 2)},
+            "clocks": clk,
+            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 4 * rays,
+                    "note": "svo_mm_render_host: launch + RGBA8 image to pinned host memory; "
+                            "frame parameters travel as kernel arguments"},
+            "gpu_launches": args.steps * len(params),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                         if peak_kind == "measured" else "fallback 6650 GB/s",
+                         "algorithmic_bytes_per_step": algo_bytes,
+                         "bytes_per_ray": algo_bytes / rays, "node_reads_per_ray": fetches / rays,
+                         "hit_fraction": hits / rays},
+            "watchdog": {"capped_rays": st.capped_rays, "bounds_errors": st.bounds_errors},
+        }
+        if not args.no_cpu_baseline and world == 1:
+            nodes, attribs = mm.getIncoreBuffer()
+            line["cpu_baseline"] = cpu_reference_frames(wl, nodes, attribs)
+        print(json.dumps(line), flush=True)
+    mm.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,268 @@
+/*
+ * libsvo_b200.h -- C ABI of the B200-native libsvo treelet ray cast.
+ *
+ * The entry points replace, one for one, the reference's OpenCL path:
+ * TreeletMemoryManager / TreeletMemoryManagerCl (src/TreeletMemoryManager.h,
+ * src/TreeletMemoryManagerCl.h) and the renderToBuffer kernel launch
+ * (projects/raycast_serialized_opencl/src/raycast_serialized_opencl.cpp:
+ * 315-324, 716, 729-747; kernel opencl/treeletRenderer_rgba.cl:610-734).
+ *
+ * Conventions
+ *   - Every function returns an int status: SVO_OK (0) or a negative code.
+ *     Nothing calls exit(); errors are never printed in place of a status.
+ *   - Pointers named d_* are CUDA device pointers owned by the caller; h_*
+ *     are host pointers.  `stream` is a cudaStream_t passed as void* (NULL =
+ *     the legacy default stream).
+ *   - Launches are asynchronous on `stream` unless stated otherwise.
+ *   - Handles are not thread-safe: one manager per host thread, or locking
+ *     by the caller (the reference is single-threaded too).
+ */
+#ifndef LIBSVO_B200_H
+#define LIBSVO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define SVO_OK 0
+#define SVO_ERR_NOENT (-2)     /* file not found (the reference exit(0)s)   */
+#define SVO_ERR_IO (-5)        /* short read, bad header, write failure     */
+#define SVO_ERR_NOMEM (-12)    /* host or device allocation failed          */
+#define SVO_ERR_BUSY (-16)     /* no incore slot could be freed             */
+#define SVO_ERR_INVALID (-22)  /* bad argument, id or size                  */
+#define SVO_ERR_RANGE (-34)    /* value beyond a stated maximum             */
+#define SVO_ERR_NOTSUP (-95)   /* mode or variant not supported             */
+#define SVO_ERR_TIMEOUT (-110) /* a bounded wait gave up                    */
+#define SVO_ERR_CANCELED (-125)/* request cancelled                         */
+#define SVO_ERR_CUDA (-1000)   /* a CUDA runtime call failed                */
+
+/* ---- data layouts ------------------------------------------------------ */
+
+/* CpuSvoNode (src/CpuSvoNode.h:100-102; OpenCL SvoNode
+ * opencl/treeletRenderer_rgba.cl:15-19).  masks: leaf bits 0-7, valid bits
+ * 8-15.  first_child is relative to the node itself inside a treelet pool
+ * (stored signed, read unsigned, adds wrap mod 2^32) and absolute in a flat
+ * pool; a treelet leaf with a sub-treelet stores that treelet's gid. */
+typedef struct svo_node {
+  uint32_t first_child;
+  uint32_t masks;
+} svo_node;
+
+/* Attribs (opencl/treeletRenderer_rgba.cl:23-26): packed normal and colour,
+ * colour = r<<24 | g<<16 | b<<8 | a.  Same index as the node. */
+typedef struct svo_attrib {
+  uint32_t packed_normal;
+  uint32_t packed_color;
+} svo_attrib;
+
+/* renderToBuffer kernel arguments 3..9 (opencl/treeletRenderer_rgba.cl:
+ * 614-620) as plain floats.  The w components are ignored. */
+typedef struct svo_frame_params {
+  uint32_t width;           /* frameBufferSize.x                         */
+  uint32_t height;          /* frameBufferSize.y                         */
+  float t_scale_ratio;      /* frameBufferSize.z (LOD footprint per t)   */
+  int32_t mode;             /* otherParams.x: 0 colour, 1 normal,
+                               3 octree depth, 4 pixel depth, 5 loops    */
+  float pixel_far_h[4];     /* pixelFarVectorH                           */
+  float pixel_far_v[4];     /* pixelFarVectorV                           */
+  float far_lower_left[4];  /* far_lower_left                            */
+  float camera_position[4]; /* cameraPosition                            */
+} svo_frame_params;
+
+/* Traversal variant. */
+#define SVO_TRAVERSAL_TREELET 0 /* sample(), treeletRenderer_rgba.cl:201-382 */
+#define SVO_TRAVERSAL_FLAT 1    /* CpuRaycasterSingleRay3::traversSvo        */
+
+typedef struct svo_trace_cfg {
+  int32_t traversal;  /* SVO_TRAVERSAL_*                                   */
+  int32_t stack_size; /* treelet: MAX_STACK_SIZE (13 in the reference; the
+                         descent stops at depth stack_size-1).  flat: the
+                         octree's max depth.  Range 2..24.                 */
+} svo_trace_cfg;
+
+/* Per-pixel hit record (SampleResult fields used for parity). */
+typedef struct svo_hit {
+  uint32_t node_index; /* incore node index of the hit (0 on a miss)       */
+  float t;             /* parent tMin at the hit; root tMax on a miss      */
+  uint16_t depth;      /* SampleResult.depth                               */
+  uint8_t hit;         /* 1 = hit                                          */
+  uint8_t flags;       /* SVO_HITFLAG_*                                    */
+  uint16_t loops;      /* SampleResult.numWhileLoops                       */
+  uint16_t fetches;    /* loop iterations that read the parent node (each
+                          one 8-byte node read of the algorithm)            */
+} svo_hit;
+
+#define SVO_HITFLAG_CAPPED 1  /* the maxLoops watchdog ended the ray           */
+#define SVO_HITFLAG_BOUNDS 2  /* a node index fell outside the pool: ray ended */
+#define SVO_HITFLAG_BOXMISS 4 /* the ray missed the root cube                  */
+
+/* Device-side counters a launch adds to (optional). */
+typedef struct svo_stats {
+  uint32_t capped_rays;   /* rays ended by the loop watchdog             */
+  uint32_t bounds_errors; /* rays that met an out-of-pool node index     */
+  uint32_t reserved[2];
+} svo_stats;
+
+/* ---- scenes (octree construction, host side) --------------------------- */
+
+typedef struct svo_scene svo_scene;
+
+typedef struct svo_scene_info {
+  uint32_t num_treelets;
+  uint32_t treelet_bytes;     /* Treelet::getMemSize(), uniform slot size */
+  uint32_t nodes_per_treelet; /* treelet_bytes / 8                        */
+  uint32_t max_depth;         /* deepest node level                       */
+  uint64_t total_nodes;       /* sum of Treelet::getNumNodes()            */
+  uint64_t leaf_voxels;       /* voxels at max_depth                      */
+} svo_scene_info;
+
+/* Menger sponge of `level` (3^level cells per axis) voxelised at `depth`
+ * (2^depth lattice, sponge centred), colour = hash(x, y, z, seed).  Treelets
+ * are cut breadth first with the reference's fill rule
+ * (src/TreeletBuilderFromFaces.cpp:200) and at most `treelet_levels` levels
+ * below their root (0 = no level limit); treelet_bytes = 0 picks the
+ * smallest size that holds the whole octree in one treelet. */
+int svo_scene_build_menger(uint32_t level, uint32_t depth, uint64_t seed, uint32_t treelet_levels,
+                           uint32_t treelet_bytes, svo_scene** out);
+
+/* Triangle mesh (inside the unit cube centred at the origin) voxelised at
+ * `depth` with a triangle/box overlap test; leaf colour from the averaged
+ * face normal, inner nodes averaged from their children
+ * (src/attribute_generators/Ag_colorAndNormalsTriangles.cpp:175-300). */
+int svo_scene_build_mesh(const float* h_vertices, uint64_t num_vertices,
+                         const uint32_t* h_triangles, uint64_t num_triangles, uint32_t depth,
+                         uint32_t treelet_levels, uint32_t treelet_bytes, int32_t threads,
+                         svo_scene** out);
+
+/* Writes / reads `<path_base>.svo` (the reference's treelet file layout,
+ * src/TreeletBuildManager.cpp:305-312, src/Treelet.cpp:403-419) and
+ * `<path_base>.ia` (per-treelet attribute records). */
+int svo_scene_write(const svo_scene* scene, const char* path_base);
+int svo_scene_read(const char* path_base, svo_scene** out);
+int svo_scene_info_get(const svo_scene* scene, svo_scene_info* out);
+/* Treelet header fields (src/Treelet.h:194-203). */
+int svo_scene_treelet(const svo_scene* scene, uint32_t gid, uint32_t* num_nodes,
+                      uint32_t* num_leaves, int32_t* parent_gid, int32_t* parent_leaf_position,
+                      int32_t* parent_leaf_idx, int32_t* parent_leaf_parent_position);
+/* Flat breadth-first pool with absolute first-child indices (the
+ * SvoBranch::serializeSvo layout, src/incore/SvoBranch.cpp:233-308).
+ * Pass NULL outputs to query the node count. */
+int svo_scene_flatten(const svo_scene* scene, svo_node* h_nodes, svo_attrib* h_attribs,
+                      uint64_t capacity, uint64_t* num_nodes);
+void svo_scene_destroy(svo_scene* scene);
+
+/* ---- treelet memory manager (TreeletMemoryManager + ...Cl) ------------- */
+
+typedef struct svo_mm svo_mm;
+
+typedef struct svo_mm_info {
+  uint32_t num_treelets;
+  uint32_t treelet_bytes;
+  uint32_t nodes_per_treelet;
+  uint32_t num_slots;
+  uint32_t free_slots;
+  uint32_t slots_to_upload;
+  uint64_t incore_nodes;      /* slots * nodes_per_treelet                 */
+  uint64_t device_bytes;      /* node + attribute device buffers           */
+} svo_mm_info;
+
+typedef struct svo_slot_info { /* TreeletMemoryManager::SlotInfo (.h:72-89) */
+  int32_t treelet_gid;         /* -1 = empty                                 */
+  int32_t visibility;
+  float error;
+} svo_slot_info;
+
+/* TreeletMemoryManagerCl(svoFilePath, incoreBufferSizeInByte, ClContext*)
+ * (src/TreeletMemoryManagerCl.h:69-71; loads <path>.svo/.ia and resets the
+ * incore buffer, src/TreeletMemoryManager.cpp:72-102).  `stream` is the
+ * stream renders run on; uploads use a side stream ordered by events. */
+int svo_mm_create(const char* svo_path_base, uint64_t incore_bytes, void* stream, svo_mm** out);
+/* Same, from an in-memory scene (copied; the scene stays owned by the caller). */
+int svo_mm_create_from_scene(const svo_scene* scene, uint64_t incore_bytes, void* stream,
+                             svo_mm** out);
+void svo_mm_destroy(svo_mm* mm);
+
+/* initClBuffer (src/TreeletMemoryManagerCl.cpp:101-113): allocates the
+ * device node and attribute buffers and uploads the whole incore buffer. */
+int svo_mm_init_device_buffer(svo_mm* mm);
+/* getClIncoreBufferGid / getClAttributeIncoreBufferGid (.h:82-85). */
+int svo_mm_get_device_buffers(svo_mm* mm, const svo_node** d_nodes, const svo_attrib** d_attribs,
+                              uint64_t* num_nodes);
+/* insertTreeletIntoIncoreBuffer (src/TreeletMemoryManager.cpp:456-548).
+ * SVO_ERR_BUSY when no slot is free and none can be freed; SVO_ERR_INVALID
+ * when the treelet's parent is not resident (the reference would patch an
+ * unrelated node). */
+int svo_mm_insert_treelet(svo_mm* mm, int32_t treelet_gid, int32_t visibility, float error);
+/* removeTreeletFromIncoreBuffer (src/TreeletMemoryManager.cpp:666-700). */
+int svo_mm_remove_treelet(svo_mm* mm, int32_t treelet_gid);
+/* freeIncorePosition (src/TreeletMemoryManager.cpp:561-653). */
+int svo_mm_free_incore_position(svo_mm* mm);
+/* updateClientSideIncoreBuffer (src/TreeletMemoryManager.cpp:393-443) with
+ * the analysis results passed as arrays (new visible treelets and their
+ * errors; treelets already resident and still visible). */
+int svo_mm_update_client_side(svo_mm* mm, const int32_t* new_gids, const float* new_errors,
+                              uint32_t num_new, const int32_t* old_gids, uint32_t num_old);
+/* updateDeviceMemory (src/TreeletMemoryManagerCl.cpp:155-251): uploads the
+ * dirty slots, merging neighbours with the reference's 0.6 coalescing rule,
+ * as async copies on the side stream; renders issued afterwards wait for
+ * them.  *num_copy_calls (optional) receives the number of ranges. */
+int svo_mm_update_device_memory(svo_mm* mm, uint32_t* num_copy_calls);
+/* resetIncoreBuffer (src/TreeletMemoryManager.cpp:304-380). */
+int svo_mm_reset(svo_mm* mm);
+/* Inserts treelets in gid order (parents first) until every treelet is
+ * resident or the slots run out.  No reference counterpart: it replaces the
+ * analysis-driven fill for fully resident scenes. */
+int svo_mm_insert_all(svo_mm* mm, uint32_t* num_inserted);
+int svo_mm_info_get(svo_mm* mm, svo_mm_info* out);
+/* getSlots (src/TreeletMemoryManager.h:157). */
+int svo_mm_get_slot(svo_mm* mm, uint32_t slot, svo_slot_info* out);
+/* Treelet::getSlotGid for a gid: the slot, or -1 when not resident. */
+int svo_mm_treelet_slot(svo_mm* mm, int32_t treelet_gid, int32_t* slot);
+/* getIncoreBuffer / getAttributeIncoreBuffer (host mirror), nodes
+ * [first, first+count). Either output may be NULL. */
+int svo_mm_copy_incore(svo_mm* mm, uint64_t first, uint64_t count, svo_node* h_nodes,
+                       svo_attrib* h_attribs);
+/* getIncoreSlotsToUpload (.h:153): up to `capacity` slot ids, ascending. */
+int svo_mm_slots_to_upload(svo_mm* mm, uint32_t* h_slots, uint32_t capacity, uint32_t* count);
+
+/* ---- ray cast ---------------------------------------------------------- */
+
+/* renderToBuffer over a whole frame (opencl/treeletRenderer_rgba.cl:
+ * 610-734; enqueue raycast_serialized_opencl.cpp:729-747).  Writes W*H
+ * RGBA8 pixels (byte 0 red) to d_rgba and, when d_hits is not NULL, one
+ * svo_hit per pixel.  d_stats (optional) accumulates counters. */
+int svo_render(const svo_node* d_nodes, const svo_attrib* d_attribs, uint64_t num_nodes,
+               const svo_frame_params* params, const svo_trace_cfg* cfg, uint32_t* d_rgba,
+               svo_hit* d_hits, svo_stats* d_stats, void* stream);
+
+/* sample() on explicit rays (d_origins, d_dirs: n x 3 floats). */
+int svo_trace_rays(const svo_node* d_nodes, uint64_t num_nodes, const float* d_origins,
+                   const float* d_dirs, uint64_t n, float t_scale_ratio,
+                   const svo_trace_cfg* cfg, svo_hit* d_hits, svo_stats* d_stats, void* stream);
+
+/* svo_render over the manager's incore buffer, after its pending uploads.
+ * Counters accumulate in the manager (read with svo_mm_sync). */
+int svo_mm_render(svo_mm* mm, const svo_frame_params* params, const svo_trace_cfg* cfg,
+                  uint32_t* d_rgba, svo_hit* d_hits, void* stream);
+/* Blocking frame into host memory: launch, copy the W*H RGBA8 image to
+ * h_rgba, wait.  This is the reference's blocking enqueueKernel plus the
+ * image read back. */
+int svo_mm_render_host(svo_mm* mm, const svo_frame_params* params, const svo_trace_cfg* cfg,
+                       uint32_t* h_rgba, void* stream);
+/* Waits for `stream` and returns the manager's accumulated counters
+ * (capped rays = the watchdog status word), then clears them. */
+int svo_mm_sync(svo_mm* mm, void* stream, svo_stats* out);
+
+/* ---- misc -------------------------------------------------------------- */
+const char* svo_version(void);
+/* Last CUDA error string seen by the library on this thread ("" if none). */
+const char* svo_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LIBSVO_B200_H */

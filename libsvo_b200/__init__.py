@@ -1,0 +1,478 @@
+"""libsvo_b200 -- B200-native treelet ray cast behind the libsvo C ABI.
+
+Python mirror of the reference's host interface for the ray-cast path:
+``TreeletMemoryManagerCuda`` keeps the method names of
+``TreeletMemoryManager`` / ``TreeletMemoryManagerCl`` (src/TreeletMemoryManager.h,
+src/TreeletMemoryManagerCl.h), ``render`` is the renderToBuffer launch.  All
+work is done by ``_lib/libsvo_b200.so`` (C ABI in include/libsvo_b200.h);
+importing this package fails loudly when that library is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import struct
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "_lib" / "libsvo_b200.so"
+
+if not LIB_PATH.is_file():
+    raise ImportError(
+        f"libsvo_b200: native library {LIB_PATH} is missing; build it with "
+        "`python -c 'import __graft_entry__ as g; g.build()'` (or python libsvo_b200/_build.py)")
+
+_L = ctypes.CDLL(str(LIB_PATH))
+
+# ---- status codes ----------------------------------------------------------
+SVO_OK = 0
+SVO_ERR_NOENT = -2
+SVO_ERR_IO = -5
+SVO_ERR_NOMEM = -12
+SVO_ERR_BUSY = -16
+SVO_ERR_INVALID = -22
+SVO_ERR_RANGE = -34
+SVO_ERR_NOTSUP = -95
+SVO_ERR_TIMEOUT = -110
+SVO_ERR_CANCELED = -125
+SVO_ERR_CUDA = -1000
+
+_ERR_NAMES = {v: k for k, v in dict(globals()).items() if k.startswith("SVO_ERR_")}
+
+TRAVERSAL_TREELET = 0
+TRAVERSAL_FLAT = 1
+HITFLAG_CAPPED = 1
+HITFLAG_BOUNDS = 2
+HITFLAG_BOXMISS = 4
+
+HIT_DTYPE = np.dtype(
+    [("node", "<u4"), ("t", "<f4"), ("depth", "<u2"), ("hit", "u1"), ("flags", "u1"), ("loops", "<u2"),
+     ("fetches", "<u2")]
+)
+
+
+class SvoError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        self.code = code
+        msg = f"{what}: {_ERR_NAMES.get(code, code)}"
+        if code == SVO_ERR_CUDA:
+            msg += f" ({_L.svo_last_error().decode()})"
+        super().__init__(msg)
+
+
+def _check(code: int, what: str) -> int:
+    if code != SVO_OK:
+        raise SvoError(code, what)
+    return code
+
+
+# ---- C structs -------------------------------------------------------------
+class svo_frame_params(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32),
+                ("t_scale_ratio", ctypes.c_float), ("mode", ctypes.c_int32),
+                ("pixel_far_h", ctypes.c_float * 4), ("pixel_far_v", ctypes.c_float * 4),
+                ("far_lower_left", ctypes.c_float * 4), ("camera_position", ctypes.c_float * 4)]
+
+
+class svo_trace_cfg(ctypes.Structure):
+    _fields_ = [("traversal", ctypes.c_int32), ("stack_size", ctypes.c_int32)]
+
+
+class svo_stats(ctypes.Structure):
+    _fields_ = [("capped_rays", ctypes.c_uint32), ("bounds_errors", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32 * 2)]
+
+
+class svo_scene_info(ctypes.Structure):
+    _fields_ = [("num_treelets", ctypes.c_uint32), ("treelet_bytes", ctypes.c_uint32),
+                ("nodes_per_treelet", ctypes.c_uint32), ("max_depth", ctypes.c_uint32),
+                ("total_nodes", ctypes.c_uint64), ("leaf_voxels", ctypes.c_uint64)]
+
+
+class svo_mm_info(ctypes.Structure):
+    _fields_ = [("num_treelets", ctypes.c_uint32), ("treelet_bytes", ctypes.c_uint32),
+                ("nodes_per_treelet", ctypes.c_uint32), ("num_slots", ctypes.c_uint32),
+                ("free_slots", ctypes.c_uint32), ("slots_to_upload", ctypes.c_uint32),
+                ("incore_nodes", ctypes.c_uint64), ("device_bytes", ctypes.c_uint64)]
+
+
+class svo_slot_info(ctypes.Structure):
+    _fields_ = [("treelet_gid", ctypes.c_int32), ("visibility", ctypes.c_int32),
+                ("error", ctypes.c_float)]
+
+
+assert ctypes.sizeof(svo_frame_params) == 80
+
+_vp, _u32, _u64, _i32, _f32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32, ctypes.c_float
+_P = ctypes.POINTER
+
+_SIGS = {
+    "svo_version": ([], ctypes.c_char_p),
+    "svo_last_error": ([], ctypes.c_char_p),
+    "svo_scene_build_menger": ([_u32, _u32, _u64, _u32, _u32, _P(_vp)], ctypes.c_int),
+    "svo_scene_build_mesh": ([_vp, _u64, _vp, _u64, _u32, _u32, _u32, _i32, _P(_vp)], ctypes.c_int),
+    "svo_scene_write": ([_vp, ctypes.c_char_p], ctypes.c_int),
+    "svo_scene_read": ([ctypes.c_char_p, _P(_vp)], ctypes.c_int),
+    "svo_scene_info_get": ([_vp, _P(svo_scene_info)], ctypes.c_int),
+    "svo_scene_treelet": ([_vp, _u32, _P(_u32), _P(_u32), _P(_i32), _P(_i32), _P(_i32), _P(_i32)], ctypes.c_int),
+    "svo_scene_flatten": ([_vp, _vp, _vp, _u64, _P(_u64)], ctypes.c_int),
+    "svo_scene_destroy": ([_vp], None),
+    "svo_mm_create": ([ctypes.c_char_p, _u64, _vp, _P(_vp)], ctypes.c_int),
+    "svo_mm_create_from_scene": ([_vp, _u64, _vp, _P(_vp)], ctypes.c_int),
+    "svo_mm_destroy": ([_vp], None),
+    "svo_mm_init_device_buffer": ([_vp], ctypes.c_int),
+    "svo_mm_get_device_buffers": ([_vp, _P(_vp), _P(_vp), _P(_u64)], ctypes.c_int),
+    "svo_mm_insert_treelet": ([_vp, _i32, _i32, _f32], ctypes.c_int),
+    "svo_mm_remove_treelet": ([_vp, _i32], ctypes.c_int),
+    "svo_mm_free_incore_position": ([_vp], ctypes.c_int),
+    "svo_mm_update_client_side": ([_vp, _vp, _vp, _u32, _vp, _u32], ctypes.c_int),
+    "svo_mm_update_device_memory": ([_vp, _P(_u32)], ctypes.c_int),
+    "svo_mm_reset": ([_vp], ctypes.c_int),
+    "svo_mm_insert_all": ([_vp, _P(_u32)], ctypes.c_int),
+    "svo_mm_info_get": ([_vp, _P(svo_mm_info)], ctypes.c_int),
+    "svo_mm_get_slot": ([_vp, _u32, _P(svo_slot_info)], ctypes.c_int),
+    "svo_mm_treelet_slot": ([_vp, _i32, _P(_i32)], ctypes.c_int),
+    "svo_mm_copy_incore": ([_vp, _u64, _u64, _vp, _vp], ctypes.c_int),
+    "svo_mm_slots_to_upload": ([_vp, _vp, _u32, _P(_u32)], ctypes.c_int),
+    "svo_render": ([_vp, _vp, _u64, _P(svo_frame_params), _P(svo_trace_cfg), _vp, _vp, _vp, _vp], ctypes.c_int),
+    "svo_trace_rays": ([_vp, _u64, _vp, _vp, _u64, _f32, _P(svo_trace_cfg), _vp, _vp, _vp], ctypes.c_int),
+    "svo_mm_render": ([_vp, _P(svo_frame_params), _P(svo_trace_cfg), _vp, _vp, _vp], ctypes.c_int),
+    "svo_mm_render_host": ([_vp, _P(svo_frame_params), _P(svo_trace_cfg), _vp, _vp], ctypes.c_int),
+    "svo_mm_sync": ([_vp, _vp, _P(svo_stats)], ctypes.c_int),
+}
+for _name, (_args, _res) in _SIGS.items():
+    _fn = getattr(_L, _name)
+    _fn.argtypes = _args
+    _fn.restype = _res
+
+lib = _L
+
+
+def version() -> str:
+    return _L.svo_version().decode()
+
+
+def _np_ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _dptr(t) -> int | None:
+    """Device pointer of a torch tensor (or an int address, or None)."""
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    return t.data_ptr()
+
+
+def _stream_ptr(stream) -> int | None:
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+# ---- cameras ---------------------------------------------------------------
+@dataclass
+class Camera:
+    """Pinhole camera producing renderToBuffer's frustum arguments
+    (raycast_serialized_opencl.cpp:670-675, 729-733) and the LOD ratio
+    tScaleRatio = tan(fov/2) * aspect / (W/2) (:303-304).  ``fov_deg`` is the
+    vertical field of view."""
+
+    eye: tuple
+    target: tuple
+    width: int
+    height: int
+    fov_deg: float = 60.0
+    up: tuple = (0.0, 1.0, 0.0)
+    far: float = 20.0
+
+    def frame_params(self, mode: int = 0, t_scale_ratio: float | None = None) -> svo_frame_params:
+        eye = np.asarray(self.eye, dtype=np.float64)
+        fwd = np.asarray(self.target, dtype=np.float64) - eye
+        fwd /= np.linalg.norm(fwd)
+        up = np.asarray(self.up, dtype=np.float64)
+        right = np.cross(fwd, up)
+        if np.linalg.norm(right) < 1e-9:
+            right = np.cross(fwd, np.array([1.0, 0.0, 0.0]))
+        right /= np.linalg.norm(right)
+        true_up = np.cross(right, fwd)
+        aspect = self.width / self.height
+        half_h = self.far * math.tan(math.radians(self.fov_deg) / 2.0)
+        half_w = half_h * aspect
+        center = eye + fwd * self.far
+        fll = center - right * half_w - true_up * half_h
+        flr = center + right * half_w - true_up * half_h
+        ful = center - right * half_w + true_up * half_h
+        h = (flr - fll) / self.width
+        v = (ful - fll) / self.height
+        if t_scale_ratio is None:
+            t_scale_ratio = math.tan(math.radians(self.fov_deg) / 2.0) * aspect / (self.width * 0.5)
+        p = svo_frame_params()
+        p.width, p.height = int(self.width), int(self.height)
+        p.t_scale_ratio = float(np.float32(t_scale_ratio))
+        p.mode = int(mode)
+        for dst, src, w in ((p.pixel_far_h, h, 0.0), (p.pixel_far_v, v, 0.0),
+                            (p.far_lower_left, fll, 1.0), (p.camera_position, eye, 1.0)):
+            for i in range(3):
+                dst[i] = float(np.float32(src[i]))
+            dst[3] = w
+        return p
+
+
+def params_bytes(p: svo_frame_params) -> bytes:
+    return bytes(p)
+
+
+def orbit_camera(seed: int, width: int, height: int, radius=(1.5, 2.5), fov_deg=60.0,
+                 target=(0.0, 0.0, 0.0)) -> Camera:
+    """Camera at a seeded random position on a sphere shell around `target`,
+    looking at it."""
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=3)
+    v /= np.linalg.norm(v)
+    r = rng.uniform(*radius) if isinstance(radius, tuple) else float(radius)
+    eye = np.asarray(target) + v * r
+    up = (0.0, 1.0, 0.0) if abs(v[1]) < 0.95 else (1.0, 0.0, 0.0)
+    return Camera(tuple(eye), tuple(target), width, height, fov_deg, up)
+
+
+def trace_cfg(traversal: int = TRAVERSAL_TREELET, stack_size: int = 13) -> svo_trace_cfg:
+    c = svo_trace_cfg()
+    c.traversal = traversal
+    c.stack_size = stack_size
+    return c
+
+
+# ---- scenes ----------------------------------------------------------------
+class Scene:
+    """An octree cut into treelets (what TreeletBuildManager writes)."""
+
+    def __init__(self, handle):
+        self._h = ctypes.c_void_p(handle)
+
+    @classmethod
+    def menger(cls, level=5, depth=8, seed=1, treelet_levels=0, treelet_bytes=0) -> "Scene":
+        h = ctypes.c_void_p()
+        _check(_L.svo_scene_build_menger(level, depth, seed, treelet_levels, treelet_bytes,
+                                         ctypes.byref(h)), "svo_scene_build_menger")
+        return cls(h.value)
+
+    @classmethod
+    def from_mesh(cls, vertices: np.ndarray, triangles: np.ndarray, depth: int,
+                  treelet_levels=0, treelet_bytes=0, threads=0) -> "Scene":
+        v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
+        t = np.ascontiguousarray(triangles, dtype=np.uint32).reshape(-1, 3)
+        h = ctypes.c_void_p()
+        _check(_L.svo_scene_build_mesh(_np_ptr(v), v.shape[0], _np_ptr(t), t.shape[0], depth,
+                                       treelet_levels, treelet_bytes, threads, ctypes.byref(h)),
+               "svo_scene_build_mesh")
+        return cls(h.value)
+
+    @classmethod
+    def read(cls, path_base: str) -> "Scene":
+        h = ctypes.c_void_p()
+        _check(_L.svo_scene_read(str(path_base).encode(), ctypes.byref(h)), "svo_scene_read")
+        return cls(h.value)
+
+    def write(self, path_base: str):
+        _check(_L.svo_scene_write(self._h, str(path_base).encode()), "svo_scene_write")
+
+    @property
+    def info(self) -> svo_scene_info:
+        i = svo_scene_info()
+        _check(_L.svo_scene_info_get(self._h, ctypes.byref(i)), "svo_scene_info_get")
+        return i
+
+    def treelet(self, gid: int) -> dict:
+        vals = [_u32(), _u32(), _i32(), _i32(), _i32(), _i32()]
+        _check(_L.svo_scene_treelet(self._h, gid, *[ctypes.byref(x) for x in vals]), "svo_scene_treelet")
+        keys = ["num_nodes", "num_leaves", "parent_gid", "parent_leaf_position", "parent_leaf_idx",
+                "parent_leaf_parent_position"]
+        return {k: v.value for k, v in zip(keys, vals)}
+
+    def flatten(self):
+        """Flat breadth-first pool with absolute first-child indices
+        (SvoBranch::serializeSvo layout): (nodes, attribs) uint32 (N, 2)."""
+        n = _u64()
+        _check(_L.svo_scene_flatten(self._h, None, None, 0, ctypes.byref(n)), "svo_scene_flatten")
+        nodes = np.zeros((n.value, 2), dtype=np.uint32)
+        attribs = np.zeros((n.value, 2), dtype=np.uint32)
+        _check(_L.svo_scene_flatten(self._h, _np_ptr(nodes), _np_ptr(attribs), n.value, ctypes.byref(n)),
+               "svo_scene_flatten")
+        return nodes, attribs
+
+    def close(self):
+        if self._h and self._h.value:
+            _L.svo_scene_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---- memory manager ----------------------------------------------------------
+class TreeletMemoryManagerCuda:
+    """TreeletMemoryManager + TreeletMemoryManagerCl with the incore buffer in
+    HBM.  Method names follow the reference; insert/remove/free return bool
+    like the reference, other failures raise SvoError."""
+
+    MAX_VISIBILITY = 8
+
+    def __init__(self, scene_or_path, incore_bytes: int, stream=None):
+        h = ctypes.c_void_p()
+        sp = _stream_ptr(stream)
+        if isinstance(scene_or_path, Scene):
+            _check(_L.svo_mm_create_from_scene(scene_or_path._h, incore_bytes, sp, ctypes.byref(h)),
+                   "svo_mm_create_from_scene")
+        else:
+            _check(_L.svo_mm_create(str(scene_or_path).encode(), incore_bytes, sp, ctypes.byref(h)),
+                   "svo_mm_create")
+        self._h = h
+        self._stream = stream
+
+    # -- reference API --
+    def initDeviceBuffer(self):
+        _check(_L.svo_mm_init_device_buffer(self._h), "svo_mm_init_device_buffer")
+
+    initClBuffer = initDeviceBuffer
+
+    def getDeviceIncoreBuffer(self):
+        """(device node pointer, device attribute pointer, number of nodes)."""
+        n, a, c = ctypes.c_void_p(), ctypes.c_void_p(), _u64()
+        _check(_L.svo_mm_get_device_buffers(self._h, ctypes.byref(n), ctypes.byref(a), ctypes.byref(c)),
+               "svo_mm_get_device_buffers")
+        return n.value, a.value, c.value
+
+    def insertTreeletIntoIncoreBuffer(self, gid: int, visibility: int = MAX_VISIBILITY,
+                                      error: float = 0.0) -> bool:
+        return _L.svo_mm_insert_treelet(self._h, gid, visibility, error) == SVO_OK
+
+    def removeTreeletFromIncoreBuffer(self, gid: int) -> bool:
+        return _L.svo_mm_remove_treelet(self._h, gid) == SVO_OK
+
+    def freeIncorePosition(self) -> bool:
+        return _L.svo_mm_free_incore_position(self._h) == SVO_OK
+
+    def updateClientSideIncoreBuffer(self, new_gids, new_errors=None, old_gids=()):
+        ng = np.ascontiguousarray(new_gids, dtype=np.int32)
+        ne = np.ascontiguousarray(new_errors if new_errors is not None else np.zeros(len(ng)),
+                                  dtype=np.float32)
+        og = np.ascontiguousarray(old_gids, dtype=np.int32)
+        return _L.svo_mm_update_client_side(self._h, _np_ptr(ng), _np_ptr(ne), len(ng), _np_ptr(og),
+                                            len(og))
+
+    def updateDeviceMemory(self) -> int:
+        calls = _u32()
+        _check(_L.svo_mm_update_device_memory(self._h, ctypes.byref(calls)), "svo_mm_update_device_memory")
+        return calls.value
+
+    def resetIncoreBuffer(self):
+        _check(_L.svo_mm_reset(self._h), "svo_mm_reset")
+
+    def insertAll(self) -> int:
+        n = _u32()
+        rc = _L.svo_mm_insert_all(self._h, ctypes.byref(n))
+        if rc not in (SVO_OK, SVO_ERR_BUSY):
+            _check(rc, "svo_mm_insert_all")
+        return n.value
+
+    @property
+    def info(self) -> svo_mm_info:
+        i = svo_mm_info()
+        _check(_L.svo_mm_info_get(self._h, ctypes.byref(i)), "svo_mm_info_get")
+        return i
+
+    def getTreeletSizeInByte(self) -> int:
+        return self.info.treelet_bytes
+
+    def getNumNodesPerTreelet(self) -> int:
+        return self.info.nodes_per_treelet
+
+    def getSlots(self):
+        out = []
+        s = svo_slot_info()
+        for i in range(self.info.num_slots):
+            _check(_L.svo_mm_get_slot(self._h, i, ctypes.byref(s)), "svo_mm_get_slot")
+            out.append((s.treelet_gid, s.visibility, s.error))
+        return out
+
+    def getSlotGid(self, gid: int) -> int:
+        s = _i32()
+        _check(_L.svo_mm_treelet_slot(self._h, gid, ctypes.byref(s)), "svo_mm_treelet_slot")
+        return s.value
+
+    def getIncoreBuffer(self, first: int = 0, count: int | None = None):
+        n = self.info.incore_nodes
+        count = n - first if count is None else count
+        nodes = np.zeros((count, 2), dtype=np.uint32)
+        attribs = np.zeros((count, 2), dtype=np.uint32)
+        _check(_L.svo_mm_copy_incore(self._h, first, count, _np_ptr(nodes), _np_ptr(attribs)),
+               "svo_mm_copy_incore")
+        return nodes, attribs
+
+    def getIncoreSlotsToUpload(self):
+        c = _u32()
+        _check(_L.svo_mm_slots_to_upload(self._h, None, 0, ctypes.byref(c)), "svo_mm_slots_to_upload")
+        out = np.zeros(c.value, dtype=np.uint32)
+        _check(_L.svo_mm_slots_to_upload(self._h, _np_ptr(out), c.value, ctypes.byref(c)),
+               "svo_mm_slots_to_upload")
+        return out
+
+    # -- rendering --
+    def render(self, params: svo_frame_params, rgba, hits=None, cfg: svo_trace_cfg | None = None,
+               stream=None):
+        cfg = cfg or trace_cfg()
+        _check(_L.svo_mm_render(self._h, ctypes.byref(params), ctypes.byref(cfg), _dptr(rgba),
+                                _dptr(hits), _stream_ptr(stream)), "svo_mm_render")
+
+    def render_host(self, params: svo_frame_params, out: np.ndarray | None = None,
+                    cfg: svo_trace_cfg | None = None, stream=None) -> np.ndarray:
+        cfg = cfg or trace_cfg()
+        if out is None:
+            out = np.zeros((params.height, params.width), dtype=np.uint32)
+        ptr = out.data_ptr() if hasattr(out, "data_ptr") else _np_ptr(out)
+        _check(_L.svo_mm_render_host(self._h, ctypes.byref(params), ctypes.byref(cfg), ptr,
+                                     _stream_ptr(stream)), "svo_mm_render_host")
+        return out
+
+    def sync(self, stream=None) -> svo_stats:
+        s = svo_stats()
+        _check(_L.svo_mm_sync(self._h, _stream_ptr(stream), ctypes.byref(s)), "svo_mm_sync")
+        return s
+
+    def close(self):
+        if self._h and self._h.value:
+            _L.svo_mm_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def render(d_nodes, d_attribs, num_nodes: int, params: svo_frame_params, d_rgba, d_hits=None,
+           cfg: svo_trace_cfg | None = None, d_stats=None, stream=None):
+    """renderToBuffer over a node pool already in device memory."""
+    cfg = cfg or trace_cfg()
+    _check(_L.svo_render(_dptr(d_nodes), _dptr(d_attribs), num_nodes, ctypes.byref(params),
+                         ctypes.byref(cfg), _dptr(d_rgba), _dptr(d_hits), _dptr(d_stats),
+                         _stream_ptr(stream)), "svo_render")
+
+
+def trace_rays(d_nodes, num_nodes: int, d_origins, d_dirs, n: int, t_scale_ratio: float,
+               d_hits, cfg: svo_trace_cfg | None = None, d_stats=None, stream=None):
+    cfg = cfg or trace_cfg()
+    _check(_L.svo_trace_rays(_dptr(d_nodes), num_nodes, _dptr(d_origins), _dptr(d_dirs), n,
+                             float(t_scale_ratio), ctypes.byref(cfg), _dptr(d_hits), _dptr(d_stats),
+                             _stream_ptr(stream)), "svo_trace_rays")

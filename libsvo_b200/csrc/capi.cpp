@@ -1,0 +1,390 @@
+// capi.cpp -- the extern "C" boundary declared in include/libsvo_b200.h.
+//
+// Every entry point validates its arguments, turns C++ exceptions (allocation
+// failures) into status codes, and never terminates the process.
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/libsvo_b200.h"
+#include "errors.h"
+#include "memory_manager.h"
+#include "render.h"
+#include "scene.h"
+
+struct svo_mm {
+  explicit svo_mm(cudaStream_t s) : impl(s) {}
+  svo::TreeletMemoryManagerCuda impl;
+};
+
+namespace svo {
+namespace {
+thread_local std::string g_last_error;
+}
+void set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
+const char* last_error() { return g_last_error.c_str(); }
+}  // namespace svo
+
+namespace {
+
+template <class Fn>
+int guarded(Fn&& fn) {
+  try {
+    return fn();
+  } catch (const std::bad_alloc&) {
+    return SVO_ERR_NOMEM;
+  } catch (...) {
+    return SVO_ERR_INVALID;
+  }
+}
+
+int check_cfg(const svo_trace_cfg* cfg) {
+  if (!cfg) return SVO_ERR_INVALID;
+  if (cfg->traversal != SVO_TRAVERSAL_TREELET && cfg->traversal != SVO_TRAVERSAL_FLAT)
+    return SVO_ERR_NOTSUP;
+  if (cfg->stack_size < 2 || cfg->stack_size > 24) return SVO_ERR_RANGE;
+  return SVO_OK;
+}
+
+int check_mode(int32_t mode) {
+  return (mode == 0 || mode == 1 || mode == 3 || mode == 4 || mode == 5) ? SVO_OK : SVO_ERR_NOTSUP;
+}
+
+int build_scene(uint32_t depth, std::vector<uint64_t>& codes, std::vector<svo_attrib>& attribs,
+                uint32_t treelet_levels, uint32_t treelet_bytes, svo_scene** out) {
+  svo::Octree tree;
+  int rc = svo::octree_from_leaves(depth, std::move(codes), std::move(attribs), tree);
+  if (rc != SVO_OK) return rc;
+  svo_scene* s = new svo_scene;
+  rc = svo::cut_treelets(tree, treelet_levels, treelet_bytes, *s);
+  if (rc != SVO_OK) {
+    delete s;
+    return rc;
+  }
+  *out = s;
+  return SVO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* svo_version(void) { return "libsvo_b200 0.1"; }
+const char* svo_last_error(void) { return svo::last_error(); }
+
+// ---- scenes ---------------------------------------------------------------
+
+int svo_scene_build_menger(uint32_t level, uint32_t depth, uint64_t seed, uint32_t treelet_levels,
+                           uint32_t treelet_bytes, svo_scene** out) {
+  if (!out) return SVO_ERR_INVALID;
+  *out = nullptr;
+  return guarded([&] {
+    std::vector<uint64_t> codes;
+    std::vector<svo_attrib> attribs;
+    int rc = svo::build_menger(level, depth, seed, codes, attribs);
+    if (rc != SVO_OK) return rc;
+    return build_scene(depth, codes, attribs, treelet_levels, treelet_bytes, out);
+  });
+}
+
+int svo_scene_build_mesh(const float* h_vertices, uint64_t num_vertices,
+                         const uint32_t* h_triangles, uint64_t num_triangles, uint32_t depth,
+                         uint32_t treelet_levels, uint32_t treelet_bytes, int32_t threads,
+                         svo_scene** out) {
+  if (!out || !h_vertices || !h_triangles) return SVO_ERR_INVALID;
+  *out = nullptr;
+  return guarded([&] {
+    std::vector<uint64_t> codes;
+    std::vector<svo_attrib> attribs;
+    int rc = svo::build_mesh_leaves(h_vertices, num_vertices, h_triangles, num_triangles, depth,
+                                    threads, codes, attribs);
+    if (rc != SVO_OK) return rc;
+    return build_scene(depth, codes, attribs, treelet_levels, treelet_bytes, out);
+  });
+}
+
+int svo_scene_write(const svo_scene* scene, const char* path_base) {
+  if (!scene || !path_base) return SVO_ERR_INVALID;
+  return guarded([&] { return svo::write_scene(*scene, path_base); });
+}
+
+int svo_scene_read(const char* path_base, svo_scene** out) {
+  if (!out || !path_base) return SVO_ERR_INVALID;
+  *out = nullptr;
+  return guarded([&] {
+    svo_scene* s = new svo_scene;
+    const int rc = svo::read_scene(path_base, *s);
+    if (rc != SVO_OK) {
+      delete s;
+      return rc;
+    }
+    *out = s;
+    return SVO_OK;
+  });
+}
+
+int svo_scene_info_get(const svo_scene* scene, svo_scene_info* out) {
+  if (!scene || !out) return SVO_ERR_INVALID;
+  out->num_treelets = (uint32_t)scene->treelets.size();
+  out->treelet_bytes = scene->treelet_bytes;
+  out->nodes_per_treelet = scene->treelet_bytes / 8;
+  out->max_depth = scene->max_depth;
+  uint64_t total = 0;
+  for (const auto& t : scene->treelets) total += t.num_nodes;
+  out->total_nodes = total;
+  out->leaf_voxels = scene->leaf_voxels;
+  return SVO_OK;
+}
+
+int svo_scene_treelet(const svo_scene* scene, uint32_t gid, uint32_t* num_nodes,
+                      uint32_t* num_leaves, int32_t* parent_gid, int32_t* parent_leaf_position,
+                      int32_t* parent_leaf_idx, int32_t* parent_leaf_parent_position) {
+  if (!scene || gid >= scene->treelets.size()) return SVO_ERR_INVALID;
+  const auto& t = scene->treelets[gid];
+  if (num_nodes) *num_nodes = t.num_nodes;
+  if (num_leaves) *num_leaves = t.num_leaves;
+  if (parent_gid) *parent_gid = t.parent_gid;
+  if (parent_leaf_position) *parent_leaf_position = t.parent_leaf_position;
+  if (parent_leaf_idx) *parent_leaf_idx = t.parent_leaf_idx;
+  if (parent_leaf_parent_position) *parent_leaf_parent_position = t.parent_leaf_parent_position;
+  return SVO_OK;
+}
+
+int svo_scene_flatten(const svo_scene* scene, svo_node* h_nodes, svo_attrib* h_attribs,
+                      uint64_t capacity, uint64_t* num_nodes) {
+  if (!scene) return SVO_ERR_INVALID;
+  return guarded([&] {
+    const bool want = h_nodes || h_attribs;
+    std::vector<svo_node> nodes;
+    std::vector<svo_attrib> attribs;
+    uint64_t n = 0;
+    const int rc = svo::flatten_scene(*scene, want ? &nodes : nullptr, want ? &attribs : nullptr, &n);
+    if (rc != SVO_OK) return rc;
+    if (num_nodes) *num_nodes = n;
+    if (!want) return SVO_OK;
+    if (capacity < n) return SVO_ERR_RANGE;
+    if (h_nodes) std::memcpy(h_nodes, nodes.data(), n * sizeof(svo_node));
+    if (h_attribs) std::memcpy(h_attribs, attribs.data(), n * sizeof(svo_attrib));
+    return SVO_OK;
+  });
+}
+
+void svo_scene_destroy(svo_scene* scene) { delete scene; }
+
+// ---- memory manager -------------------------------------------------------
+
+int svo_mm_create_from_scene(const svo_scene* scene, uint64_t incore_bytes, void* stream,
+                             svo_mm** out) {
+  if (!out || !scene) return SVO_ERR_INVALID;
+  *out = nullptr;
+  return guarded([&] {
+    svo_scene copy = *scene;
+    svo_mm* mm = new svo_mm((cudaStream_t)stream);
+    const int rc = mm->impl.init(std::move(copy), incore_bytes);
+    if (rc != SVO_OK) {
+      delete mm;
+      return rc;
+    }
+    *out = mm;
+    return SVO_OK;
+  });
+}
+
+int svo_mm_create(const char* svo_path_base, uint64_t incore_bytes, void* stream, svo_mm** out) {
+  if (!out || !svo_path_base) return SVO_ERR_INVALID;
+  *out = nullptr;
+  return guarded([&] {
+    svo_scene s;
+    int rc = svo::read_scene(svo_path_base, s);
+    if (rc != SVO_OK) return rc;
+    svo_mm* mm = new svo_mm((cudaStream_t)stream);
+    rc = mm->impl.init(std::move(s), incore_bytes);
+    if (rc != SVO_OK) {
+      delete mm;
+      return rc;
+    }
+    *out = mm;
+    return SVO_OK;
+  });
+}
+
+void svo_mm_destroy(svo_mm* mm) { delete mm; }
+
+int svo_mm_init_device_buffer(svo_mm* mm) {
+  if (!mm) return SVO_ERR_INVALID;
+  return guarded([&] { return mm->impl.init_device_buffer(); });
+}
+
+int svo_mm_get_device_buffers(svo_mm* mm, const svo_node** d_nodes, const svo_attrib** d_attribs,
+                              uint64_t* num_nodes) {
+  if (!mm || !mm->impl.device_ready()) return SVO_ERR_INVALID;
+  if (d_nodes) *d_nodes = mm->impl.device_nodes();
+  if (d_attribs) *d_attribs = mm->impl.device_attribs();
+  if (num_nodes) *num_nodes = mm->impl.incore_nodes();
+  return SVO_OK;
+}
+
+int svo_mm_insert_treelet(svo_mm* mm, int32_t treelet_gid, int32_t visibility, float error) {
+  if (!mm) return SVO_ERR_INVALID;
+  return guarded([&] {
+    svo::TreeletMemoryManager::SlotInfo s;
+    s.treelet_gid = treelet_gid;
+    s.visibility = visibility;
+    s.error = error;
+    return mm->impl.insert_treelet(s);
+  });
+}
+
+int svo_mm_remove_treelet(svo_mm* mm, int32_t treelet_gid) {
+  if (!mm) return SVO_ERR_INVALID;
+  return guarded([&] { return mm->impl.remove_treelet(treelet_gid); });
+}
+
+int svo_mm_free_incore_position(svo_mm* mm) {
+  if (!mm) return SVO_ERR_INVALID;
+  return guarded([&] { return mm->impl.free_incore_position(); });
+}
+
+int svo_mm_update_client_side(svo_mm* mm, const int32_t* new_gids, const float* new_errors,
+                              uint32_t num_new, const int32_t* old_gids, uint32_t num_old) {
+  if (!mm || (num_new && !new_gids) || (num_old && !old_gids)) return SVO_ERR_INVALID;
+  return guarded([&] {
+    return mm->impl.update_client_side(new_gids, new_errors, num_new, old_gids, num_old);
+  });
+}
+
+int svo_mm_update_device_memory(svo_mm* mm, uint32_t* num_copy_calls) {
+  if (!mm) return SVO_ERR_INVALID;
+  return guarded([&] { return mm->impl.update_device_memory(num_copy_calls); });
+}
+
+int svo_mm_reset(svo_mm* mm) {
+  if (!mm) return SVO_ERR_INVALID;
+  return guarded([&] { return mm->impl.reset_incore_buffer(); });
+}
+
+int svo_mm_insert_all(svo_mm* mm, uint32_t* num_inserted) {
+  if (!mm) return SVO_ERR_INVALID;
+  return guarded([&] { return mm->impl.insert_all(num_inserted); });
+}
+
+int svo_mm_info_get(svo_mm* mm, svo_mm_info* out) {
+  if (!mm || !out) return SVO_ERR_INVALID;
+  const auto& m = mm->impl;
+  out->num_treelets = m.num_treelets();
+  out->treelet_bytes = m.treelet_bytes();
+  out->nodes_per_treelet = m.nodes_per_treelet();
+  out->num_slots = m.num_slots();
+  out->free_slots = m.free_slots();
+  out->slots_to_upload = (uint32_t)m.slots_to_upload().size();
+  out->incore_nodes = m.incore_nodes();
+  out->device_bytes = m.device_bytes();
+  return SVO_OK;
+}
+
+int svo_mm_get_slot(svo_mm* mm, uint32_t slot, svo_slot_info* out) {
+  if (!mm || !out || slot >= mm->impl.num_slots()) return SVO_ERR_INVALID;
+  const auto& s = mm->impl.slot(slot);
+  out->treelet_gid = s.treelet_gid;
+  out->visibility = s.visibility;
+  out->error = s.error;
+  return SVO_OK;
+}
+
+int svo_mm_treelet_slot(svo_mm* mm, int32_t treelet_gid, int32_t* slot) {
+  if (!mm || !slot || treelet_gid < 0 || (uint32_t)treelet_gid >= mm->impl.num_treelets())
+    return SVO_ERR_INVALID;
+  *slot = mm->impl.treelet_slot(treelet_gid);
+  return SVO_OK;
+}
+
+int svo_mm_copy_incore(svo_mm* mm, uint64_t first, uint64_t count, svo_node* h_nodes,
+                       svo_attrib* h_attribs) {
+  if (!mm) return SVO_ERR_INVALID;
+  const uint64_t n = mm->impl.incore_nodes();
+  if (first > n || count > n - first) return SVO_ERR_RANGE;
+  if (h_nodes) std::memcpy(h_nodes, mm->impl.host_nodes() + first, count * sizeof(svo_node));
+  if (h_attribs)
+    std::memcpy(h_attribs, mm->impl.host_attribs() + first, count * sizeof(svo_attrib));
+  return SVO_OK;
+}
+
+int svo_mm_slots_to_upload(svo_mm* mm, uint32_t* h_slots, uint32_t capacity, uint32_t* count) {
+  if (!mm) return SVO_ERR_INVALID;
+  const auto& up = mm->impl.slots_to_upload();
+  if (count) *count = (uint32_t)up.size();
+  if (!h_slots) return SVO_OK;
+  uint32_t i = 0;
+  for (uint32_t s : up) {
+    if (i == capacity) break;
+    h_slots[i++] = s;
+  }
+  return SVO_OK;
+}
+
+// ---- ray cast -------------------------------------------------------------
+
+int svo_render(const svo_node* d_nodes, const svo_attrib* d_attribs, uint64_t num_nodes,
+               const svo_frame_params* params, const svo_trace_cfg* cfg, uint32_t* d_rgba,
+               svo_hit* d_hits, svo_stats* d_stats, void* stream) {
+  if (!params || !d_nodes || !d_rgba || num_nodes == 0 || num_nodes > 0x100000000ull)
+    return SVO_ERR_INVALID;
+  int rc = check_cfg(cfg);
+  if (rc != SVO_OK) return rc;
+  rc = check_mode(params->mode);
+  if (rc != SVO_OK) return rc;
+  if ((params->mode == 0 || params->mode == 1) && !d_attribs) return SVO_ERR_INVALID;
+  return svo::launch_render(d_nodes, d_attribs, num_nodes, *params, *cfg, d_rgba, d_hits, d_stats,
+                            (cudaStream_t)stream);
+}
+
+int svo_trace_rays(const svo_node* d_nodes, uint64_t num_nodes, const float* d_origins,
+                   const float* d_dirs, uint64_t n, float t_scale_ratio, const svo_trace_cfg* cfg,
+                   svo_hit* d_hits, svo_stats* d_stats, void* stream) {
+  if (!d_nodes || !d_origins || !d_dirs || !d_hits || num_nodes == 0 ||
+      num_nodes > 0x100000000ull)
+    return SVO_ERR_INVALID;
+  const int rc = check_cfg(cfg);
+  if (rc != SVO_OK) return rc;
+  return svo::launch_trace_rays(d_nodes, num_nodes, d_origins, d_dirs, n, t_scale_ratio, *cfg,
+                                d_hits, d_stats, (cudaStream_t)stream);
+}
+
+int svo_mm_render(svo_mm* mm, const svo_frame_params* params, const svo_trace_cfg* cfg,
+                  uint32_t* d_rgba, svo_hit* d_hits, void* stream) {
+  if (!mm || !mm->impl.device_ready()) return SVO_ERR_INVALID;
+  cudaStream_t s = stream ? (cudaStream_t)stream : mm->impl.render_stream();
+  int rc = mm->impl.wait_uploads(s);
+  if (rc != SVO_OK) return rc;
+  return svo_render(mm->impl.device_nodes(), mm->impl.device_attribs(), mm->impl.incore_nodes(),
+                    params, cfg, d_rgba, d_hits, mm->impl.device_stats(), s);
+}
+
+int svo_mm_render_host(svo_mm* mm, const svo_frame_params* params, const svo_trace_cfg* cfg,
+                       uint32_t* h_rgba, void* stream) {
+  if (!mm || !params || !h_rgba || !mm->impl.device_ready()) return SVO_ERR_INVALID;
+  cudaStream_t s = stream ? (cudaStream_t)stream : mm->impl.render_stream();
+  const uint64_t pixels = (uint64_t)params->width * params->height;
+  if (pixels == 0) return SVO_OK;
+  uint32_t* d_rgba = nullptr;
+  int rc = mm->impl.rgba_scratch(pixels, &d_rgba);
+  if (rc != SVO_OK) return rc;
+  rc = svo_mm_render(mm, params, cfg, d_rgba, nullptr, s);
+  if (rc != SVO_OK) return rc;
+  SVO_CUDA_TRY(cudaMemcpyAsync(h_rgba, d_rgba, pixels * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  SVO_CUDA_TRY(cudaStreamSynchronize(s));
+  return SVO_OK;
+}
+
+int svo_mm_sync(svo_mm* mm, void* stream, svo_stats* out) {
+  if (!mm || !mm->impl.device_ready()) return SVO_ERR_INVALID;
+  cudaStream_t s = stream ? (cudaStream_t)stream : mm->impl.render_stream();
+  svo_stats st;
+  SVO_CUDA_TRY(cudaStreamSynchronize(s));
+  SVO_CUDA_TRY(cudaMemcpy(&st, mm->impl.device_stats(), sizeof(st), cudaMemcpyDeviceToHost));
+  SVO_CUDA_TRY(cudaMemset(mm->impl.device_stats(), 0, sizeof(svo_stats)));
+  if (out) *out = st;
+  return SVO_OK;
+}
+
+}  // extern "C"

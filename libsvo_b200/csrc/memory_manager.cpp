@@ -1,0 +1,336 @@
+// memory_manager.cpp -- see memory_manager.h.
+#include "memory_manager.h"
+
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+
+#include "errors.h"
+
+namespace svo {
+
+TreeletMemoryManager::~TreeletMemoryManager() {
+  std::free(incore_);
+  std::free(incore_attr_);
+}
+
+int TreeletMemoryManager::init(svo_scene&& scene, uint64_t incore_bytes) {
+  if (scene.treelets.empty() || scene.treelet_bytes < 128 || scene.treelet_bytes % 8 != 0)
+    return SVO_ERR_INVALID;
+  if (incore_bytes < scene.treelet_bytes) return SVO_ERR_RANGE;  // not even the root treelet
+  scene_ = std::move(scene);
+  N_ = scene_.treelet_bytes / 8;
+  const uint64_t slots = incore_bytes / scene_.treelet_bytes;
+  if (slots * (uint64_t)N_ > 0xFFFFFFFFull) return SVO_ERR_RANGE;  // uint32 node indices
+  slots_.assign(slots, SlotInfo());
+  // lazily zeroed host mirror of the incore buffer
+  incore_ = (svo_node*)std::calloc(slots * N_, sizeof(svo_node));
+  incore_attr_ = (svo_attrib*)std::calloc(slots * N_, sizeof(svo_attrib));
+  if (!incore_ || !incore_attr_) return SVO_ERR_NOMEM;
+  return reset_incore_buffer();
+}
+
+int TreeletMemoryManager::reset_incore_buffer() {
+  before_host_write();
+  free_.clear();
+  upload_.clear();
+  children_.assign(scene_.treelets.size(), std::set<int32_t>());
+  slot_of_.assign(scene_.treelets.size(), -1);
+  for (auto& s : slots_) s = SlotInfo();
+  // push order as in the reference: slot 0 ends on top of the stack
+  const uint32_t n = (uint32_t)slots_.size();
+  for (uint32_t i = 1; i != n + 1; ++i) free_.push_back(n - i);
+  search_pos_ = 1;
+  SlotInfo root;
+  root.treelet_gid = 0;
+  root.visibility = kMaxVisibility;
+  root.error = 999.0f;
+  return insert_treelet(root);
+}
+
+int TreeletMemoryManager::insert_treelet(const SlotInfo& tve) {
+  const int32_t gid = tve.treelet_gid;
+  if (gid < 0 || (uint32_t)gid >= scene_.treelets.size()) return SVO_ERR_INVALID;
+  if (slot_of_[gid] >= 0) return SVO_ERR_INVALID;  // already resident
+  const TreeletData& t = scene_.treelets[gid];
+  if (gid != 0 && slot_of_[t.parent_gid] < 0) return SVO_ERR_INVALID;  // parent not resident
+  if (free_.empty()) {
+    const int rc = free_incore_position();
+    if (rc != SVO_OK) return rc;
+    if (gid != 0 && slot_of_[t.parent_gid] < 0) return SVO_ERR_BUSY;  // parent was evicted
+  }
+  before_host_write();
+  const uint32_t slot = free_.back();
+  free_.pop_back();
+  slots_[slot] = tve;
+  slot_of_[gid] = (int32_t)slot;
+  const uint64_t pos = (uint64_t)slot * N_;
+  std::memcpy(incore_ + pos, t.nodes.data(), (size_t)t.num_nodes * sizeof(svo_node));
+  std::memset(incore_ + pos + t.num_nodes, 0, (size_t)(N_ - t.num_nodes) * sizeof(svo_node));
+  std::memcpy(incore_attr_ + pos, t.attribs.data(), (size_t)t.num_nodes * sizeof(svo_attrib));
+  std::memset(incore_attr_ + pos + t.num_nodes, 0, (size_t)(N_ - t.num_nodes) * sizeof(svo_attrib));
+  mark_upload(slot);
+  if (gid == 0) return SVO_OK;
+  // patch the parent's leaf (TreeletMemoryManager.cpp:518-545)
+  const uint64_t pslot = (uint64_t)slot_of_[t.parent_gid];
+  const uint64_t leaf = pslot * N_ + (uint64_t)t.parent_leaf_position;
+  const uint64_t leaf_parent = pslot * N_ + (uint64_t)t.parent_leaf_parent_position;
+  incore_[leaf] = incore_[pos];
+  incore_[leaf_parent].masks &= ~(1u << (uint32_t)t.parent_leaf_idx);
+  incore_[leaf].first_child = (uint32_t)((int64_t)(pos + 1) - (int64_t)leaf);
+  mark_upload((uint32_t)pslot);
+  children_[t.parent_gid].insert(gid);
+  return SVO_OK;
+}
+
+int TreeletMemoryManager::remove_treelet(int32_t gid) {
+  if (gid <= 0 || (uint32_t)gid >= scene_.treelets.size()) return SVO_ERR_INVALID;
+  if (slot_of_[gid] < 0) return SVO_ERR_INVALID;
+  const TreeletData& t = scene_.treelets[gid];
+  const int32_t pslot = slot_of_[t.parent_gid];
+  if (pslot < 0) return SVO_ERR_INVALID;
+  before_host_write();
+  const uint32_t slot = (uint32_t)slot_of_[gid];
+  const uint64_t leaf = (uint64_t)pslot * N_ + (uint64_t)t.parent_leaf_position;
+  const uint64_t leaf_parent = (uint64_t)pslot * N_ + (uint64_t)t.parent_leaf_parent_position;
+  // restore the original leaf and its leaf flag (TreeletMemoryManager.cpp:679-683)
+  const TreeletData& pt = scene_.treelets[t.parent_gid];
+  incore_[leaf] = (uint32_t)t.parent_leaf_position < pt.num_nodes
+                      ? pt.nodes[t.parent_leaf_position]
+                      : svo_node{0u, 0u};
+  incore_[leaf_parent].masks |= 1u << (uint32_t)t.parent_leaf_idx;
+  mark_upload((uint32_t)pslot);
+  slots_[slot] = SlotInfo();
+  free_.push_back(slot);
+  slot_of_[gid] = -1;
+  children_[t.parent_gid].erase(gid);
+  return SVO_OK;
+}
+
+int TreeletMemoryManager::free_incore_position() {
+  const uint32_t n = (uint32_t)slots_.size();
+  if (n <= 1) return SVO_ERR_BUSY;
+  if (search_pos_ >= n) search_pos_ = 1;
+  int32_t freeable = 0;
+  uint32_t tests = 0;
+  for (uint32_t i = 0; i != n; ++i) {
+    const SlotInfo& s = slots_[search_pos_];
+    if (s.visibility < 0 && s.treelet_gid != -1) {
+      const int32_t parent = scene_.treelets[s.treelet_gid].parent_gid;
+      const int32_t ps = slot_of_[parent];
+      if (ps >= 0 && slots_[ps].visibility < 0) {
+        freeable = s.treelet_gid;
+        break;
+      }
+    }
+    ++search_pos_;
+    ++tests;
+    if (search_pos_ == n) search_pos_ = 1;
+    if (tests == kNumProbes) break;
+  }
+  if (freeable == 0) return SVO_ERR_BUSY;
+  // every treelet attached below the freeable one goes too (.cpp:603-648)
+  std::deque<int32_t> q;
+  q.push_back(freeable);
+  std::vector<int32_t> to_clear;
+  while (!q.empty()) {
+    const int32_t p = q.front();
+    q.pop_front();
+    for (int32_t c : children_[p]) {
+      q.push_back(c);
+      to_clear.push_back(c);
+    }
+    children_[p].clear();
+  }
+  before_host_write();
+  for (int32_t c : to_clear) {
+    const int32_t s = slot_of_[c];
+    if (s > 0) {
+      free_.push_back((uint32_t)s);
+      slot_of_[c] = -1;
+      slots_[s] = SlotInfo();
+    }
+  }
+  return remove_treelet(freeable);
+}
+
+int TreeletMemoryManager::update_client_side(const int32_t* new_gids, const float* new_errors,
+                                             uint32_t num_new, const int32_t* old_gids,
+                                             uint32_t num_old) {
+  for (uint32_t i = 1; i < slots_.size(); ++i) --slots_[i].visibility;
+  for (uint32_t i = 0; i < num_old; ++i) {
+    const int32_t g = old_gids[i];
+    if (g < 0 || (uint32_t)g >= scene_.treelets.size() || slot_of_[g] < 0) return SVO_ERR_INVALID;
+    slots_[slot_of_[g]].visibility = kMaxVisibility;
+  }
+  int rc = SVO_OK;
+  for (uint32_t i = 0; i < num_new; ++i) {
+    SlotInfo s;
+    s.treelet_gid = new_gids[i];
+    s.visibility = kMaxVisibility;
+    s.error = new_errors ? new_errors[i] : 0.0f;
+    const int r = insert_treelet(s);
+    if (r != SVO_OK && rc == SVO_OK) rc = r;  // keep going, report the first failure
+  }
+  return rc;
+}
+
+int TreeletMemoryManager::insert_all(uint32_t* inserted) {
+  uint32_t n = 0;
+  int rc = SVO_OK;
+  for (uint32_t g = 1; g < scene_.treelets.size(); ++g) {
+    if (slot_of_[g] >= 0) continue;
+    if (free_.empty()) {
+      rc = SVO_ERR_BUSY;
+      break;
+    }
+    SlotInfo s;
+    s.treelet_gid = (int32_t)g;
+    s.visibility = kMaxVisibility;
+    s.error = 0.0f;
+    const int r = insert_treelet(s);
+    if (r != SVO_OK) {
+      rc = r;
+      break;
+    }
+    ++n;
+  }
+  if (inserted) *inserted = n;
+  return rc;
+}
+
+std::vector<std::pair<uint32_t, uint32_t>> TreeletMemoryManager::upload_ranges() const {
+  std::vector<std::pair<uint32_t, uint32_t>> out;
+  const float ratio_limit = 0.6f * 2.0f;
+  auto it = upload_.begin();
+  while (it != upload_.end()) {
+    const uint32_t start = *it;
+    uint32_t num_slots = 1, num_treelets = 1;
+    while (it != upload_.end()) {
+      const int dist = (int)*it - (int)start;
+      const float ratio = (float)(num_treelets + 1) / (float)(dist + 1);
+      if (ratio >= ratio_limit) {
+        num_slots = (uint32_t)dist + 1;
+        ++num_treelets;
+        ++it;
+      } else {
+        break;
+      }
+    }
+    out.emplace_back(start, num_slots);
+  }
+  return out;
+}
+
+// ---------------------------------------------------------------------------
+
+TreeletMemoryManagerCuda::~TreeletMemoryManagerCuda() {
+  if (copy_stream_) cudaStreamSynchronize(copy_stream_);
+  cudaFree(d_nodes_);
+  cudaFree(d_attribs_);
+  cudaFree(d_stats_);
+  cudaFree(d_rgba_);
+  for (int i = 0; i < 2; ++i) {
+    if (stage_evt_[i]) cudaEventDestroy(stage_evt_[i]);
+    if (stage_[i]) cudaFreeHost(stage_[i]);
+  }
+  if (upload_done_) cudaEventDestroy(upload_done_);
+  if (copy_stream_) cudaStreamDestroy(copy_stream_);
+}
+
+int TreeletMemoryManagerCuda::init_device_buffer() {
+  if (d_nodes_) return SVO_OK;
+  const uint64_t n = incore_nodes();
+  SVO_CUDA_TRY(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
+  SVO_CUDA_TRY(cudaEventCreateWithFlags(&upload_done_, cudaEventDisableTiming));
+  for (int i = 0; i < 2; ++i) {
+    SVO_CUDA_TRY(cudaEventCreateWithFlags(&stage_evt_[i], cudaEventDisableTiming));
+    SVO_CUDA_TRY(cudaMallocHost(&stage_[i], kStageBytes));
+  }
+  if (cudaMalloc(&d_nodes_, n * sizeof(svo_node)) != cudaSuccess ||
+      cudaMalloc(&d_attribs_, n * sizeof(svo_attrib)) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(d_nodes_);
+    cudaFree(d_attribs_);
+    d_nodes_ = nullptr;
+    d_attribs_ = nullptr;
+    return SVO_ERR_NOMEM;
+  }
+  SVO_CUDA_TRY(cudaMalloc(&d_stats_, sizeof(svo_stats)));
+  SVO_CUDA_TRY(cudaMemsetAsync(d_stats_, 0, sizeof(svo_stats), copy_stream_));
+  device_bytes_ = n * (sizeof(svo_node) + sizeof(svo_attrib));
+  // whole-buffer upload, as clCreateBuffer(COPY_HOST_PTR) does
+  // (TreeletMemoryManagerCl.cpp:106-112)
+  int rc = stage_copy(d_nodes_, incore_, n * sizeof(svo_node));
+  if (rc == SVO_OK) rc = stage_copy(d_attribs_, incore_attr_, n * sizeof(svo_attrib));
+  if (rc != SVO_OK) return rc;
+  SVO_CUDA_TRY(cudaEventRecord(upload_done_, copy_stream_));
+  upload_pending_ = true;
+  return SVO_OK;
+}
+
+int TreeletMemoryManagerCuda::stage_copy(void* dst, const void* src, uint64_t bytes) {
+  const char* s = (const char*)src;
+  char* d = (char*)dst;
+  while (bytes) {
+    const uint64_t n = std::min(bytes, kStageBytes);
+    const int h = stage_next_;
+    stage_next_ ^= 1;
+    SVO_CUDA_TRY(cudaEventSynchronize(stage_evt_[h]));
+    std::memcpy(stage_[h], s, (size_t)n);
+    SVO_CUDA_TRY(cudaMemcpyAsync(d, stage_[h], n, cudaMemcpyHostToDevice, copy_stream_));
+    SVO_CUDA_TRY(cudaEventRecord(stage_evt_[h], copy_stream_));
+    s += n;
+    d += n;
+    bytes -= n;
+  }
+  return SVO_OK;
+}
+
+int TreeletMemoryManagerCuda::update_device_memory(uint32_t* copy_calls) {
+  if (copy_calls) *copy_calls = 0;
+  if (upload_.empty()) return SVO_OK;
+  if (!d_nodes_) return SVO_ERR_INVALID;  // init_device_buffer first
+  const auto ranges = upload_ranges();
+  for (const auto& r : ranges) {
+    const uint64_t first = (uint64_t)r.first * N_;
+    const uint64_t count = (uint64_t)r.second * N_;
+    int rc = stage_copy(d_nodes_ + first, incore_ + first, count * sizeof(svo_node));
+    if (rc == SVO_OK) rc = stage_copy(d_attribs_ + first, incore_attr_ + first, count * sizeof(svo_attrib));
+    if (rc != SVO_OK) return rc;
+  }
+  SVO_CUDA_TRY(cudaEventRecord(upload_done_, copy_stream_));
+  upload_pending_ = true;
+  if (copy_calls) *copy_calls = (uint32_t)ranges.size();
+  upload_.clear();
+  return SVO_OK;
+}
+
+int TreeletMemoryManagerCuda::reset_incore_buffer() {
+  const int rc = TreeletMemoryManager::reset_incore_buffer();
+  if (rc != SVO_OK || !d_nodes_) return rc;
+  // the device copy must match the fresh mirror: upload everything again
+  for (uint32_t s = 0; s < num_slots(); ++s) mark_upload(s);
+  return update_device_memory(nullptr);
+}
+
+int TreeletMemoryManagerCuda::wait_uploads(cudaStream_t stream) {
+  if (!upload_pending_) return SVO_OK;
+  SVO_CUDA_TRY(cudaStreamWaitEvent(stream, upload_done_, 0));
+  return SVO_OK;
+}
+
+int TreeletMemoryManagerCuda::rgba_scratch(uint64_t pixels, uint32_t** out) {
+  if (pixels > d_rgba_pixels_) {
+    cudaFree(d_rgba_);
+    d_rgba_ = nullptr;
+    d_rgba_pixels_ = 0;
+    SVO_CUDA_TRY(cudaMalloc(&d_rgba_, pixels * sizeof(uint32_t)));
+    d_rgba_pixels_ = pixels;
+  }
+  *out = d_rgba_;
+  return SVO_OK;
+}
+
+}  // namespace svo

@@ -1,0 +1,124 @@
+// memory_manager.h -- the treelet incore buffer and its device copy.
+//
+// TreeletMemoryManager keeps the host-side bookkeeping of
+// src/TreeletMemoryManager.{h,cpp}: a fixed number of treelet slots, a stack
+// of free slots, per-slot visibility, the child treelets resident below each
+// treelet, and the set of slots to upload.  TreeletMemoryManagerCuda replaces
+// TreeletMemoryManagerCl (src/TreeletMemoryManagerCl.{h,cpp}): the incore
+// buffer lives in HBM, dirty slots go up through a pinned staging ring with
+// cudaMemcpyAsync on a side stream, and renders wait on an event for them.
+//
+// The host mirror is plain (pageable, lazily zeroed) memory, so that large
+// budgets do not pin host RAM; only the staging ring is pinned.  No CUDA call
+// is made before init_device_buffer(), so the bookkeeping runs without a GPU.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <set>
+#include <vector>
+
+#include "../../include/libsvo_b200.h"
+#include "scene.h"
+
+namespace svo {
+
+class TreeletMemoryManager {
+ public:
+  struct SlotInfo {  // src/TreeletMemoryManager.h:72-89
+    int32_t treelet_gid = -1;
+    int32_t visibility = 0;
+    float error = 100000.0f;
+  };
+  static constexpr int32_t kMaxVisibility = 8;  // MAX_VISIBILITY, TreeletMemoryManager.cpp:47
+  static constexpr uint32_t kNumProbes = 100;   // freeIncorePosition probe budget
+
+  virtual ~TreeletMemoryManager();
+
+  // ctor + loadFromFile + resetIncoreBuffer (TreeletMemoryManager.cpp:72-102)
+  int init(svo_scene&& scene, uint64_t incore_bytes);
+
+  int insert_treelet(const SlotInfo& tve);           // .cpp:456-548
+  int remove_treelet(int32_t gid);                   // .cpp:666-700
+  int free_incore_position();                        // .cpp:561-653
+  int update_client_side(const int32_t* new_gids, const float* new_errors, uint32_t num_new,
+                         const int32_t* old_gids, uint32_t num_old);  // .cpp:393-443
+  virtual int reset_incore_buffer();                 // .cpp:304-380
+  int insert_all(uint32_t* inserted);
+
+  uint32_t num_treelets() const { return (uint32_t)scene_.treelets.size(); }
+  uint32_t treelet_bytes() const { return scene_.treelet_bytes; }
+  uint32_t nodes_per_treelet() const { return N_; }
+  uint32_t num_slots() const { return (uint32_t)slots_.size(); }
+  uint32_t free_slots() const { return (uint32_t)free_.size(); }
+  uint64_t incore_nodes() const { return (uint64_t)slots_.size() * N_; }
+  const std::set<uint32_t>& slots_to_upload() const { return upload_; }
+  const SlotInfo& slot(uint32_t i) const { return slots_[i]; }
+  int32_t treelet_slot(int32_t gid) const { return slot_of_[gid]; }
+  const svo_node* host_nodes() const { return incore_; }
+  const svo_attrib* host_attribs() const { return incore_attr_; }
+  const svo_scene& scene() const { return scene_; }
+
+  // Slot ranges the reference's updateDeviceMemory would copy
+  // (TreeletMemoryManagerCl.cpp:177-236), as (first slot, slot count).
+  std::vector<std::pair<uint32_t, uint32_t>> upload_ranges() const;
+
+ protected:
+  // Called before the host mirror changes, so uploads still reading it
+  // (none with the staging ring) can finish first.
+  virtual void before_host_write() {}
+  void mark_upload(uint32_t slot) { upload_.insert(slot); }
+
+  svo_scene scene_;
+  uint32_t N_ = 0;
+  svo_node* incore_ = nullptr;
+  svo_attrib* incore_attr_ = nullptr;
+  std::vector<SlotInfo> slots_;
+  std::vector<int32_t> slot_of_;
+  std::vector<std::set<int32_t>> children_;
+  std::vector<uint32_t> free_;  // top = back()
+  std::set<uint32_t> upload_;
+  uint32_t search_pos_ = 1;
+};
+
+class TreeletMemoryManagerCuda : public TreeletMemoryManager {
+ public:
+  explicit TreeletMemoryManagerCuda(cudaStream_t render_stream) : render_stream_(render_stream) {}
+  ~TreeletMemoryManagerCuda() override;
+
+  int init_device_buffer();                         // initClBuffer
+  int update_device_memory(uint32_t* copy_calls);   // updateDeviceMemory
+  int reset_incore_buffer() override;
+
+  const svo_node* device_nodes() const { return d_nodes_; }
+  const svo_attrib* device_attribs() const { return d_attribs_; }
+  bool device_ready() const { return d_nodes_ != nullptr; }
+  cudaStream_t render_stream() const { return render_stream_; }
+  svo_stats* device_stats() const { return d_stats_; }
+  uint64_t device_bytes() const { return device_bytes_; }
+
+  // Orders work on `stream` after the pending uploads.
+  int wait_uploads(cudaStream_t stream);
+  // Device RGBA scratch for host-output renders (grown on demand).
+  int rgba_scratch(uint64_t pixels, uint32_t** out);
+
+ private:
+  int stage_copy(void* dst, const void* src, uint64_t bytes);
+
+  cudaStream_t render_stream_ = nullptr;
+  cudaStream_t copy_stream_ = nullptr;
+  cudaEvent_t upload_done_ = nullptr;
+  bool upload_pending_ = false;
+  svo_node* d_nodes_ = nullptr;
+  svo_attrib* d_attribs_ = nullptr;
+  svo_stats* d_stats_ = nullptr;
+  uint64_t device_bytes_ = 0;
+  static constexpr uint64_t kStageBytes = 32ull << 20;  // per half of the ring
+  void* stage_[2] = {nullptr, nullptr};
+  cudaEvent_t stage_evt_[2] = {nullptr, nullptr};
+  int stage_next_ = 0;
+  uint32_t* d_rgba_ = nullptr;
+  uint64_t d_rgba_pixels_ = 0;
+};
+
+}  // namespace svo

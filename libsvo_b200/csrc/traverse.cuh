@@ -1,0 +1,265 @@
+// traverse.cuh -- per-ray sparse-voxel-octree descent for sm_100a.
+//
+// Restates the reference's two traversals bit for bit:
+//   * treelet: sample() in opencl/treeletRenderer_rgba.cl:201-382 over the
+//     TreeletMemoryManager incore pool (first-child indices relative to the
+//     node, added mod 2^32; src/TreeletMemoryManager.cpp:531-539);
+//   * flat:    CpuRaycasterSingleRay3::traversSvo
+//     (src/incore/CpuRaycasterSingleRay3.cpp:159-387) over a breadth-first
+//     pool with absolute first-child indices.
+//
+// Every FP32 operation is an explicit round-to-nearest intrinsic, so no
+// multiply-add is ever contracted and the operation order is the
+// reference's.  Divisions, reciprocals and the square root are the IEEE
+// correctly rounded ones.  OpenCL's max(a, b) is (a < b) ? b : a.
+//
+// Storage.  The reference keeps {node, tMin, tMax, centre} per stack level.
+// Two facts shrink that to {node, tMax}:
+//   - a level's tMin is only read again after popping back to it, and at the
+//     push it was set to the pushed child's tcMax, which is the child frame's
+//     tMax and never changes afterwards; so on a pop tMin := popped tMax;
+//   - node centres are exact dyadic numbers (-0.5 + (2i+1) 2^-(k+1) for a
+//     depth-k node with lattice coordinate i), so they are rebuilt exactly
+//     from integer coordinates instead of being stored.
+// The stack lives in shared memory, one 8-byte word per level per thread,
+// laid out [level][thread] so a warp's accesses are contiguous.
+#pragma once
+#include <cstdint>
+
+#include "../../include/libsvo_b200.h"
+
+namespace svo {
+
+constexpr int kMaxStack = 24;  // largest supported stack_size / flat depth
+
+struct RayHit {
+  uint32_t node;
+  float t;
+  uint32_t depth;
+  uint32_t hit;
+  uint32_t flags;
+  uint32_t loops;
+  uint32_t fetches;  // loop iterations that read the parent node
+};
+
+__device__ __forceinline__ float cl_max(float a, float b) { return (a < b) ? b : a; }
+__device__ __forceinline__ float cl_min(float a, float b) { return (b < a) ? b : a; }
+
+// OpenCL sign(): +-1, the argument itself for +-0, 0 for NaN.
+__device__ __forceinline__ float cl_sign(float v) {
+  return v > 0.0f ? 1.0f : (v < 0.0f ? -1.0f : (v == 0.0f ? v : 0.0f));
+}
+
+// 2^e for -126 <= e <= 0, exact.
+__device__ __forceinline__ float pow2i(int e) { return __int_as_float((127 + e) << 23); }
+
+// Centre coordinate of lattice cell i at depth k: -0.5 + (2i+1) * 2^-(k+1).
+__device__ __forceinline__ float cell_center(uint32_t i, int k) {
+  return __fadd_rn(-0.5f, __fmul_rn((float)(2u * i + 1u), pow2i(-(k + 1))));
+}
+
+// intersectAABB (opencl/treeletRenderer_rgba.cl:100-178) against [-0.5,0.5]^3.
+__device__ __forceinline__ bool root_slab(const float o[3], const float d[3], float& t_min,
+                                          float& t_max) {
+  float t_near = -10000000.0f;
+  float t_far = 10000000.0f;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    if (d[i] == 0.0f && (-0.5f > o[i] || 0.5f < o[i])) return false;
+    float t1 = __fdiv_rn(__fsub_rn(-0.5f, o[i]), d[i]);
+    float t2 = __fdiv_rn(__fsub_rn(0.5f, o[i]), d[i]);
+    if (t1 > t2) {
+      const float s = t1;
+      t1 = t2;
+      t2 = s;
+    }
+    if (t1 > t_near) t_near = t1;
+    if (t2 < t_far) t_far = t2;
+    if (t_near > t_far) return false;
+    if (t_far < 0.0f) return false;
+  }
+  t_min = t_near;
+  t_max = t_far;
+  return true;
+}
+
+// The ray cast.  kFlat selects the CpuRaycasterSingleRay3 rules; S is the
+// stack size (treelet) or the octree depth (flat).  `stack` points at this
+// thread's column of the shared-memory stack, `stride` words apart.
+template <bool kFlat>
+__device__ __forceinline__ RayHit cast_ray(const uint2* __restrict__ nodes, uint64_t num_nodes,
+                                           const float o[3], float dx, float dy, float dz,
+                                           float tsr, int S, uint2* stack, int stride) {
+  RayHit h;
+  h.node = 0u;
+  h.t = 0.0f;
+  h.depth = 0u;
+  h.hit = 0u;
+  h.flags = 0u;
+  h.loops = 0u;
+  h.fetches = 0u;
+
+  float t_min, t_max;
+  {
+    const float d0[3] = {dx, dy, dz};
+    if (!root_slab(o, d0, t_min, t_max)) {
+      h.flags = SVO_HITFLAG_BOXMISS;
+      return h;
+    }
+  }
+  // Direction clamp: sample() replaces |d| < 1e-4 by 1e-4 * sign(d)
+  // (:231-239); traversSvo replaces |d| < 1e-5 by 1e-5 * sign(d) * 10 (:184-186).
+  const float eps = 0.00001f;
+  if (kFlat) {
+    if (fabsf(dx) < eps) dx = __fmul_rn(__fmul_rn(eps, cl_sign(dx)), 10.0f);
+    if (fabsf(dy) < eps) dy = __fmul_rn(__fmul_rn(eps, cl_sign(dy)), 10.0f);
+    if (fabsf(dz) < eps) dz = __fmul_rn(__fmul_rn(eps, cl_sign(dz)), 10.0f);
+  } else {
+    const float mn = 0.0001f;
+    if (fabsf(dx) < mn) dx = __fmul_rn(mn, cl_sign(dx));
+    if (fabsf(dy) < mn) dy = __fmul_rn(mn, cl_sign(dy));
+    if (fabsf(dz) < mn) dz = __fmul_rn(mn, cl_sign(dz));
+  }
+  const float rx = __frcp_rn(dx), px = __fmul_rn(-o[0], rx);
+  const float ry = __frcp_rn(dy), py = __fmul_rn(-o[1], ry);
+  const float rz = __frcp_rn(dz), pz = __fmul_rn(-o[2], rz);
+
+  const uint32_t max_loops = (uint32_t)((S + 1) * (S + 1) * 5);
+  int scale = S - 1;
+  // Current frame: node, tMin, tMax, lattice coordinate (depth S-1-scale).
+  uint32_t node = 0u;
+  float tmin = t_min, tmax = t_max;
+  uint32_t ix = 0u, iy = 0u, iz = 0u;
+  uint2 nd = make_uint2(0u, 0u);
+  bool have_node = false;
+  uint32_t loops = 0u, fetches = 0u;
+
+  while (scale < S) {
+    const int k = S - 1 - scale;  // depth of the current node
+    const float sx2 = pow2i(scale - S);
+    const float half = __fmul_rn(sx2, 0.5f);
+    ++loops;
+    if (loops == max_loops) {
+      h.flags = SVO_HITFLAG_CAPPED;
+      h.loops = loops;
+      h.fetches = fetches;
+      if (!kFlat) {  // sample() reports the current node as a hit (:268-277)
+        h.hit = 1u;
+        h.node = node;
+        h.depth = (uint32_t)(S - scale);
+        h.t = tmin;
+      }
+      return h;
+    }
+    bool pop;
+    if (kFlat)
+      pop = (tmax < 0.0f) || (fabsf(__fsub_rn(tmin, tmax)) < eps) || !(tmin < tmax);
+    else
+      pop = (tmax < 0.0f) || !(fabsf(__fsub_rn(tmin, tmax)) > eps);
+    if (pop) {
+      ++scale;
+      if (scale < S) {
+        const uint2 e = stack[(S - 1 - scale) * stride];
+        tmin = tmax;
+        node = e.x;
+        tmax = __uint_as_float(e.y);
+        ix >>= 1;
+        iy >>= 1;
+        iz >>= 1;
+        have_node = false;
+      }
+      continue;
+    }
+    const float cx = cell_center(ix, k), cy = cell_center(iy, k), cz = cell_center(iz, k);
+    const float te = __fadd_rn(tmin, eps);
+    const float ex = __fsub_rn(__fadd_rn(o[0], __fmul_rn(te, dx)), cx);
+    const float ey = __fsub_rn(__fadd_rn(o[1], __fmul_rn(te, dy)), cy);
+    const float ez = __fsub_rn(__fadd_rn(o[2], __fmul_rn(te, dz)), cz);
+    const uint32_t bx = ex > 0.0f, by = ey > 0.0f, bz = ez > 0.0f;
+    const uint32_t ci = (bx << 2) | (by << 1) | bz;
+    const float ccx = __fadd_rn(__fmul_rn(bx ? 0.5f : -0.5f, sx2), cx);
+    const float ccy = __fadd_rn(__fmul_rn(by ? 0.5f : -0.5f, sx2), cy);
+    const float ccz = __fadd_rn(__fmul_rn(bz ? 0.5f : -0.5f, sx2), cz);
+    float tx0 = __fadd_rn(__fmul_rn(rx, __fsub_rn(ccx, half)), px);
+    float tx1 = __fadd_rn(__fmul_rn(rx, __fadd_rn(ccx, half)), px);
+    if (tx0 > tx1) {
+      const float s = tx0;
+      tx0 = tx1;
+      tx1 = s;
+    }
+    float ty0 = __fadd_rn(__fmul_rn(ry, __fsub_rn(ccy, half)), py);
+    float ty1 = __fadd_rn(__fmul_rn(ry, __fadd_rn(ccy, half)), py);
+    if (ty0 > ty1) {
+      const float s = ty0;
+      ty0 = ty1;
+      ty1 = s;
+    }
+    float tz0 = __fadd_rn(__fmul_rn(rz, __fsub_rn(ccz, half)), pz);
+    float tz1 = __fadd_rn(__fmul_rn(rz, __fadd_rn(ccz, half)), pz);
+    if (tz0 > tz1) {
+      const float s = tz0;
+      tz0 = tz1;
+      tz1 = s;
+    }
+    const float tc_min = cl_max(tx0, cl_max(ty0, tz0));
+    const float tc_max = cl_min(tx1, cl_min(ty1, tz1));
+
+    if (!have_node) {
+      if ((uint64_t)node >= num_nodes) {
+        h.flags = SVO_HITFLAG_BOUNDS;
+        h.loops = loops;
+        h.fetches = fetches;
+        return h;
+      }
+      nd = __ldg(nodes + node);
+      have_node = true;
+    }
+    ++fetches;
+    const uint32_t masks = nd.y;
+    if ((masks >> (ci + 8u)) & 1u) {
+      const uint32_t below = __popc((masks >> 8) & ((1u << ci) - 1u));
+      const uint32_t child = (kFlat ? 0u : node) + nd.x + below;
+      if ((masks >> ci) & 1u) {  // leaf
+        h.hit = 1u;
+        h.node = child;
+        h.depth = (uint32_t)(S - scale);
+        h.t = tmin;
+        h.loops = loops;
+        h.fetches = fetches;
+        return h;
+      }
+      const bool lod = kFlat ? (__fmul_rn(tsr, tc_max) > sx2)
+                             : (__fmul_rn(tsr, tc_min) > sx2 || scale == 1);
+      if (lod) {
+        h.hit = 1u;
+        h.node = child;
+        h.depth = (uint32_t)(kFlat ? (S - scale) : (S - scale + 1));
+        h.t = tmin;
+        h.loops = loops;
+        h.fetches = fetches;
+        return h;
+      }
+      // push: the current frame's tMin becomes tc_max (recovered on pop).
+      stack[(S - 1 - scale) * stride] = make_uint2(node, __float_as_uint(tmax));
+      --scale;
+      node = child;
+      tmin = tc_min;
+      tmax = tc_max;
+      ix = (ix << 1) | bx;
+      iy = (iy << 1) | by;
+      iz = (iz << 1) | bz;
+      have_node = false;
+      continue;
+    }
+    tmin = tc_max;  // advance to the next sibling
+  }
+  h.hit = 0u;
+  h.node = 0u;
+  h.depth = 0u;
+  h.t = kFlat ? 0.0f : t_max;
+  h.loops = loops;
+  h.fetches = fetches;
+  return h;
+}
+
+}  // namespace svo

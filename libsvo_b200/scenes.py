@@ -1,0 +1,49 @@
+"""Seeded synthetic scenes and cameras for the benchmark configurations.
+
+The reference measured on laser scans that are not part of it; these seeded
+scenes stand in for them with the shapes and sizes the benchmark
+configurations name:
+
+* ``menger``    -- Menger sponge level 5 (243^3 cells) in a depth-8 octree
+                   (256^3), one treelet, colour = hash(x, y, z); 512x512 view
+                   from a seeded camera outside the cube, 60 degree fov.
+* ``icosphere`` -- icosphere subdivided 6 times (81,920 triangles), radius
+                   0.4 displaced radially by 3-octave value noise of amplitude
+                   0.05, depth-11 octree cut into 6-level treelets, colour from
+                   the face normal; one 1920x1080 view from radius 2.5.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import Camera, Scene, orbit_camera
+
+
+@dataclass
+class Workload:
+    name: str
+    scene: Scene
+    cameras: list
+    stack_size: int = 13
+    description: str = ""
+
+    @property
+    def rays_per_step(self) -> int:
+        return sum(c.width * c.height for c in self.cameras)
+
+
+def menger(level=5, depth=8, seed=1, width=512, height=512) -> Workload:
+    scene = Scene.menger(level=level, depth=depth, seed=seed)
+    cam = orbit_camera(seed, width, height, radius=(1.5, 2.5), fov_deg=60.0)
+    return Workload("menger_l5_d8_512", scene, [cam],
+                    description=f"Menger level {level}, depth {depth}, one treelet, {width}x{height}")
+
+
+def orbit_pose(radius: float, angle_deg: float, elevation_deg: float, width: int, height: int,
+               fov_deg=60.0) -> Camera:
+    a, e = math.radians(angle_deg), math.radians(elevation_deg)
+    eye = (radius * math.cos(e) * math.cos(a), radius * math.sin(e), radius * math.cos(e) * math.sin(a))
+    return Camera(eye, (0.0, 0.0, 0.0), width, height, fov_deg)

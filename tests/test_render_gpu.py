@@ -1,0 +1,222 @@
+"""GPU parity: the sm_100a ray cast against the CPU oracle, bit for bit.
+
+Every comparison here is exact: node indices, hit flags, depths, loop counts,
+the FP32 hit distance t compared as bits, and the RGBA8 pixels.
+"""
+import numpy as np
+import pytest
+
+import libsvo_b200 as L
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def _hits_np(t):
+    return t.cpu().numpy().view(np.uint8).view(L.HIT_DTYPE).reshape(-1)
+
+
+def assert_hits_equal(got, want, what=""):
+    got = got.reshape(-1)
+    want = want.reshape(-1)
+    for k in ("node", "depth", "hit", "flags", "loops", "fetches"):
+        bad = np.nonzero(got[k] != want[k])[0]
+        assert bad.size == 0, f"{what}: {k} differs at {bad.size} rays, first {bad[:5]}: " \
+                              f"{got[k][bad[:5]]} vs {want[k][bad[:5]]}"
+    bt = np.nonzero(got["t"].view(np.uint32) != want["t"].view(np.uint32))[0]
+    assert bt.size == 0, f"{what}: t differs at {bt.size} rays: {got['t'][bt[:5]]} vs {want['t'][bt[:5]]}"
+
+
+def gpu_frame(mm, params, cfg=None):
+    torch = _torch()
+    rgba = torch.empty((params.height, params.width), dtype=torch.int32, device="cuda")
+    hits = torch.empty((params.height * params.width * 16,), dtype=torch.uint8, device="cuda")
+    mm.render(params, rgba, hits, cfg=cfg, stream=torch.cuda.current_stream())
+    torch.cuda.synchronize()
+    return rgba.cpu().numpy().view(np.uint32), _hits_np(hits)
+
+
+@pytest.fixture(scope="module")
+def menger_mm(menger_scene, cuda):
+    mm = L.TreeletMemoryManagerCuda(menger_scene, menger_scene.info.treelet_bytes)
+    mm.initDeviceBuffer()
+    yield mm
+    mm.close()
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3, 4])
+def test_menger_frame_matches_oracle(menger_mm, seed):
+    cam = L.orbit_camera(seed, 512, 512)
+    p = cam.frame_params()
+    rgba, hits = gpu_frame(menger_mm, p)
+    nodes, attribs = menger_mm.getIncoreBuffer()
+    o_rgba, o_hits, _, _ = oracle.render(nodes, attribs, bytes(p))
+    assert_hits_equal(hits, o_hits, f"seed {seed}")
+    assert np.array_equal(rgba, o_rgba)
+    assert o_hits["hit"].sum() > 1000  # the camera sees the sponge
+
+
+def test_menger_full_depth_and_coarse_lod(menger_mm):
+    cam = L.orbit_camera(11, 384, 256, radius=1.2)
+    nodes, attribs = menger_mm.getIncoreBuffer()
+    for tsr in (0.0, 0.02):
+        p = cam.frame_params(t_scale_ratio=tsr)
+        rgba, hits = gpu_frame(menger_mm, p)
+        o_rgba, o_hits, _, _ = oracle.render(nodes, attribs, bytes(p))
+        assert_hits_equal(hits, o_hits, f"tsr {tsr}")
+        assert np.array_equal(rgba, o_rgba)
+
+
+@pytest.mark.parametrize("mode", [1, 3, 4, 5])
+def test_view_modes(menger_mm, mode):
+    p = L.orbit_camera(5, 200, 120).frame_params(mode=mode)
+    rgba, hits = gpu_frame(menger_mm, p)
+    nodes, attribs = menger_mm.getIncoreBuffer()
+    o_rgba, o_hits, _, _ = oracle.render(nodes, attribs, bytes(p))
+    assert np.array_equal(rgba, o_rgba)
+
+
+@pytest.mark.parametrize("w,h", [(1, 1), (17, 13), (8, 4), (1000, 3)])
+def test_ragged_frame_sizes(menger_mm, w, h):
+    p = L.orbit_camera(6, w, h, radius=1.6).frame_params()
+    rgba, hits = gpu_frame(menger_mm, p)
+    nodes, attribs = menger_mm.getIncoreBuffer()
+    o_rgba, o_hits, _, _ = oracle.render(nodes, attribs, bytes(p))
+    assert_hits_equal(hits, o_hits)
+    assert np.array_equal(rgba, o_rgba)
+
+
+def test_flat_traversal_matches_oracle(menger_scene, cuda):
+    torch = _torch()
+    nodes, attribs = menger_scene.flatten()
+    depth = menger_scene.info.max_depth
+    dn = torch.from_numpy(nodes.view(np.int32)).to(cuda)
+    da = torch.from_numpy(attribs.view(np.int32)).to(cuda)
+    for seed in (1, 2):
+        p = L.orbit_camera(seed, 320, 240).frame_params()
+        rgba = torch.empty((p.height, p.width), dtype=torch.int32, device=cuda)
+        hits = torch.empty((p.height * p.width * 16,), dtype=torch.uint8, device=cuda)
+        L.render(dn, da, nodes.shape[0], p, rgba, hits, cfg=L.trace_cfg(L.TRAVERSAL_FLAT, depth))
+        torch.cuda.synchronize()
+        o_rgba, o_hits, _, _ = oracle.render(nodes, attribs, bytes(p), flat=True, stack_size=depth)
+        assert_hits_equal(_hits_np(hits), o_hits, "flat")
+        assert np.array_equal(rgba.cpu().numpy().view(np.uint32), o_rgba)
+
+
+def edge_rays(n_random=20000, seed=0):
+    rng = np.random.default_rng(seed)
+    o, d = [], []
+    # axis-aligned and zero components, from outside and inside the cube
+    for origin in ([0.1, 0.2, 3.0], [0.0, 0.0, 2.0], [0.0, 0.0, 0.0], [0.25, -0.25, 0.1],
+                   [0.5, 0.5, 2.0], [-0.5, 0.3, -3.0]):
+        for dirv in ([0, 0, -1], [0, 0, 1], [1, 0, 0], [0, -1, 0], [0, 0.00005, -1], [1e-6, 0, -1],
+                     [-0.0, 0.0, -1.0], [0.3, 0.4, -0.866]):
+            o.append(origin)
+            v = np.asarray(dirv, dtype=np.float64)
+            d.append(v / np.linalg.norm(v))
+    # grazing rays along cube faces and edges
+    for s in np.linspace(-0.5, 0.5, 11):
+        o.append([s, 0.5, 2.0]); d.append([0.0, 0.0, -1.0])
+        o.append([0.5, s, -2.0]); d.append([0.0, 0.0, 1.0])
+        o.append([-2.0, s, s]); d.append([1.0, 0.0, 0.0])
+    # random rays from a shell and from inside
+    eo = rng.normal(size=(n_random, 3))
+    eo = eo / np.linalg.norm(eo, axis=1, keepdims=True) * rng.uniform(0.0, 2.5, size=(n_random, 1))
+    tgt = rng.uniform(-0.5, 0.5, size=(n_random, 3))
+    ed = tgt - eo
+    ed /= np.linalg.norm(ed, axis=1, keepdims=True)
+    o = np.concatenate([np.asarray(o, dtype=np.float64), eo]).astype(np.float32)
+    d = np.concatenate([np.asarray(d, dtype=np.float64), ed]).astype(np.float32)
+    return o, d
+
+
+@pytest.mark.parametrize("tsr", [0.0, 0.003])
+def test_explicit_rays_edge_cases(menger_mm, cuda, tsr):
+    torch = _torch()
+    o, d = edge_rays()
+    nodes, _ = menger_mm.getIncoreBuffer()
+    dn = torch.from_numpy(nodes.view(np.int32)).to(cuda)
+    do = torch.from_numpy(o).to(cuda)
+    dd = torch.from_numpy(d).to(cuda)
+    hits = torch.empty((o.shape[0] * 16,), dtype=torch.uint8, device=cuda)
+    L.trace_rays(dn, nodes.shape[0], do, dd, o.shape[0], tsr, hits)
+    torch.cuda.synchronize()
+    o_hits, _ = oracle.cast_rays(nodes, o, d, tsr)
+    assert_hits_equal(_hits_np(hits), o_hits, "edge rays")
+
+
+def paged_menger_manager():
+    """A Menger octree cut into 3-level treelets and paged so that child
+    treelets sit in slots below their parents: first-child deltas are then
+    negative and the index arithmetic wraps mod 2^32."""
+    scene = L.Scene.menger(level=4, depth=7, seed=3, treelet_levels=3, treelet_bytes=8 * 1024)
+    ntl = scene.info.num_treelets
+    parents = np.array([scene.treelet(g)["parent_gid"] for g in range(ntl)])
+    top = [g for g in range(1, ntl) if parents[g] == 0]
+    mm = L.TreeletMemoryManagerCuda(scene, scene.info.treelet_bytes * ntl)
+    for g in top:
+        assert mm.insertTreeletIntoIncoreBuffer(g)
+    # free the low slots of the first few top treelets, then page in the
+    # children of the last ones: they land below their parents
+    k = min(8, len(top) // 2)
+    for g in top[:k]:
+        assert mm.removeTreeletFromIncoreBuffer(g)
+    for g in top[::-1][:k]:
+        for c in np.nonzero(parents == g)[0]:
+            if c != 0:
+                assert mm.insertTreeletIntoIncoreBuffer(int(c))
+    for g in top[:k]:
+        assert mm.insertTreeletIntoIncoreBuffer(g)
+    return scene, mm
+
+
+def test_paged_pool_with_relative_indices(cuda):
+    scene, mm = paged_menger_manager()
+    mm.initDeviceBuffer()
+    nodes, attribs = mm.getIncoreBuffer()
+    assert (nodes[:, 0].view(np.int32) < 0).any(), "expected negative relative first-child indices"
+    for seed in (7, 8):
+        p = L.orbit_camera(seed, 256, 256, radius=1.4).frame_params(t_scale_ratio=0.0)
+        rgba, hits = gpu_frame(mm, p)
+        o_rgba, o_hits, _, _ = oracle.render(nodes, attribs, bytes(p))
+        assert_hits_equal(hits, o_hits, "paged")
+        assert np.array_equal(rgba, o_rgba)
+    mm.close()
+
+
+def test_bounds_errors_are_reported_not_faulted(cuda):
+    torch = _torch()
+    nodes = np.zeros((9, 2), dtype=np.uint32)
+    nodes[0] = [1, 0xFF00]  # 8 valid inner children
+    nodes[1:, 0] = 0x7FFFFFF0  # children point far outside the pool
+    nodes[1:, 1] = 0xFF00
+    attribs = np.zeros((9, 2), dtype=np.uint32)
+    dn = torch.from_numpy(nodes.view(np.int32)).to(cuda)
+    da = torch.from_numpy(attribs.view(np.int32)).to(cuda)
+    p = L.orbit_camera(1, 64, 64, radius=1.3).frame_params(t_scale_ratio=0.0)
+    rgba = torch.empty((64, 64), dtype=torch.int32, device=cuda)
+    hits = torch.empty((64 * 64 * 16,), dtype=torch.uint8, device=cuda)
+    stats = torch.zeros(4, dtype=torch.int32, device=cuda)
+    L.render(dn, da, 9, p, rgba, hits, d_stats=stats)
+    torch.cuda.synchronize()
+    h = _hits_np(hits)
+    o_rgba, o_hits, _, _ = oracle.render(nodes, attribs, bytes(p))
+    assert_hits_equal(h, o_hits, "bounds")
+    nb = int((h["flags"] == L.HITFLAG_BOUNDS).sum())
+    assert nb > 0
+    assert int(stats[1].item()) == nb
+
+
+def test_mm_render_host_matches_device(menger_mm):
+    p = L.orbit_camera(2, 300, 200).frame_params()
+    host = menger_mm.render_host(p)
+    rgba, _ = gpu_frame(menger_mm, p)
+    assert np.array_equal(host, rgba)
+    st = menger_mm.sync()
+    assert st.capped_rays == 0 and st.bounds_errors == 0
