@@ -123,9 +123,11 @@ typedef struct svo_scene_info {
 /* Menger sponge of `level` (3^level cells per axis) voxelised at `depth`
  * (2^depth lattice, sponge centred), colour = hash(x, y, z, seed).  Treelets
  * are cut breadth first with the reference's fill rule
- * (src/TreeletBuilderFromFaces.cpp:200) and at most `treelet_levels` levels
- * below their root (0 = no level limit); treelet_bytes = 0 picks the
- * smallest size that holds the whole octree in one treelet. */
+ * (src/TreeletBuilderFromFaces.cpp:200).  treelet_levels = L > 0 puts
+ * treelet boundaries at depths D, D-L, D-2L, ... (D = octree depth): every
+ * treelet below the top one spans L levels and ends on the leaves; 0 = no
+ * level boundaries.  treelet_bytes = 0 picks the smallest slot size that
+ * holds the largest treelet whole (the whole octree when L = 0). */
 int svo_scene_build_menger(uint32_t level, uint32_t depth, uint64_t seed, uint32_t treelet_levels,
                            uint32_t treelet_bytes, svo_scene** out);
 
@@ -137,6 +139,20 @@ int svo_scene_build_mesh(const float* h_vertices, uint64_t num_vertices,
                          const uint32_t* h_triangles, uint64_t num_triangles, uint32_t depth,
                          uint32_t treelet_levels, uint32_t treelet_bytes, int32_t threads,
                          svo_scene** out);
+
+/* Seeded synthetic meshes (inputs for svo_scene_build_mesh).  The reference
+ * voxelises scanned PLY meshes that are not part of it; these stand in with
+ * the triangle counts of the benchmark configurations.  Call *_size first.
+ * Icosphere: 20 * 4^subdivisions faces, vertex radius
+ * radius + amplitude * fbm(direction) (3D value noise, `octaves` octaves
+ * from base `frequency`).  Terrain: grid x grid vertices over [-0.5,0.5]^2 in
+ * x/z, y = base + height * fbm01(x, z). */
+int svo_mesh_icosphere_size(uint32_t subdivisions, uint64_t* num_vertices, uint64_t* num_triangles);
+int svo_mesh_icosphere(uint32_t subdivisions, float radius, uint32_t octaves, float amplitude,
+                       float frequency, uint64_t seed, float* h_vertices, uint32_t* h_triangles);
+int svo_mesh_terrain_size(uint32_t grid, uint64_t* num_vertices, uint64_t* num_triangles);
+int svo_mesh_terrain(uint32_t grid, uint32_t octaves, float base, float height, float frequency,
+                     uint64_t seed, float* h_vertices, uint32_t* h_triangles);
 
 /* Writes / reads `<path_base>.svo` (the reference's treelet file layout,
  * src/TreeletBuildManager.cpp:305-312, src/Treelet.cpp:403-419) and
@@ -211,6 +227,11 @@ int svo_mm_update_client_side(svo_mm* mm, const int32_t* new_gids, const float* 
  * as async copies on the side stream; renders issued afterwards wait for
  * them.  *num_copy_calls (optional) receives the number of ranges. */
 int svo_mm_update_device_memory(svo_mm* mm, uint32_t* num_copy_calls);
+/* The copy ranges the next svo_mm_update_device_memory will issue: slot
+ * ranges (first slot, slot count) merged with the 0.6 rule of
+ * TreeletMemoryManagerCl.cpp:177-211.  Pass NULL arrays to query the count. */
+int svo_mm_plan_uploads(svo_mm* mm, uint32_t* h_first_slots, uint32_t* h_slot_counts,
+                        uint32_t capacity, uint32_t* num_ranges);
 /* resetIncoreBuffer (src/TreeletMemoryManager.cpp:304-380). */
 int svo_mm_reset(svo_mm* mm);
 /* Inserts treelets in gid order (parents first) until every treelet is

@@ -114,6 +114,10 @@ _SIGS = {
     "svo_last_error": ([], ctypes.c_char_p),
     "svo_scene_build_menger": ([_u32, _u32, _u64, _u32, _u32, _P(_vp)], ctypes.c_int),
     "svo_scene_build_mesh": ([_vp, _u64, _vp, _u64, _u32, _u32, _u32, _i32, _P(_vp)], ctypes.c_int),
+    "svo_mesh_icosphere_size": ([_u32, _P(_u64), _P(_u64)], ctypes.c_int),
+    "svo_mesh_icosphere": ([_u32, _f32, _u32, _f32, _f32, _u64, _vp, _vp], ctypes.c_int),
+    "svo_mesh_terrain_size": ([_u32, _P(_u64), _P(_u64)], ctypes.c_int),
+    "svo_mesh_terrain": ([_u32, _u32, _f32, _f32, _f32, _u64, _vp, _vp], ctypes.c_int),
     "svo_scene_write": ([_vp, ctypes.c_char_p], ctypes.c_int),
     "svo_scene_read": ([ctypes.c_char_p, _P(_vp)], ctypes.c_int),
     "svo_scene_info_get": ([_vp, _P(svo_scene_info)], ctypes.c_int),
@@ -130,6 +134,7 @@ _SIGS = {
     "svo_mm_free_incore_position": ([_vp], ctypes.c_int),
     "svo_mm_update_client_side": ([_vp, _vp, _vp, _u32, _vp, _u32], ctypes.c_int),
     "svo_mm_update_device_memory": ([_vp, _P(_u32)], ctypes.c_int),
+    "svo_mm_plan_uploads": ([_vp, _vp, _vp, _u32, _P(_u32)], ctypes.c_int),
     "svo_mm_reset": ([_vp], ctypes.c_int),
     "svo_mm_insert_all": ([_vp, _P(_u32)], ctypes.c_int),
     "svo_mm_info_get": ([_vp, _P(svo_mm_info)], ctypes.c_int),
@@ -247,6 +252,30 @@ def trace_cfg(traversal: int = TRAVERSAL_TREELET, stack_size: int = 13) -> svo_t
     c.traversal = traversal
     c.stack_size = stack_size
     return c
+
+
+# ---- meshes ----------------------------------------------------------------
+def icosphere(subdivisions: int, radius=0.4, octaves=3, amplitude=0.05, frequency=2.0, seed=1):
+    """(vertices float32 (V,3), triangles uint32 (T,3)) of a noise-displaced icosphere."""
+    nv, nt = _u64(), _u64()
+    _check(_L.svo_mesh_icosphere_size(subdivisions, ctypes.byref(nv), ctypes.byref(nt)),
+           "svo_mesh_icosphere_size")
+    v = np.zeros((nv.value, 3), dtype=np.float32)
+    t = np.zeros((nt.value, 3), dtype=np.uint32)
+    _check(_L.svo_mesh_icosphere(subdivisions, radius, octaves, amplitude, frequency, seed,
+                                 _np_ptr(v), _np_ptr(t)), "svo_mesh_icosphere")
+    return v, t
+
+
+def terrain(grid: int, octaves=6, base=-0.45, height=0.3, frequency=2.0, seed=1):
+    """(vertices, triangles) of an fBm height field over the unit square."""
+    nv, nt = _u64(), _u64()
+    _check(_L.svo_mesh_terrain_size(grid, ctypes.byref(nv), ctypes.byref(nt)), "svo_mesh_terrain_size")
+    v = np.zeros((nv.value, 3), dtype=np.float32)
+    t = np.zeros((nt.value, 3), dtype=np.uint32)
+    _check(_L.svo_mesh_terrain(grid, octaves, base, height, frequency, seed, _np_ptr(v), _np_ptr(t)),
+           "svo_mesh_terrain")
+    return v, t
 
 
 # ---- scenes ----------------------------------------------------------------
@@ -374,6 +403,16 @@ class TreeletMemoryManagerCuda:
         calls = _u32()
         _check(_L.svo_mm_update_device_memory(self._h, ctypes.byref(calls)), "svo_mm_update_device_memory")
         return calls.value
+
+    def planUploads(self):
+        """[(first slot, slot count)] the next updateDeviceMemory copies."""
+        n = _u32()
+        _check(_L.svo_mm_plan_uploads(self._h, None, None, 0, ctypes.byref(n)), "svo_mm_plan_uploads")
+        f = np.zeros(n.value, dtype=np.uint32)
+        c = np.zeros(n.value, dtype=np.uint32)
+        _check(_L.svo_mm_plan_uploads(self._h, _np_ptr(f), _np_ptr(c), n.value, ctypes.byref(n)),
+               "svo_mm_plan_uploads")
+        return list(zip(f.tolist(), c.tolist()))
 
     def resetIncoreBuffer(self):
         _check(_L.svo_mm_reset(self._h), "svo_mm_reset")

@@ -258,6 +258,22 @@ int svo_mm_update_device_memory(svo_mm* mm, uint32_t* num_copy_calls) {
   return guarded([&] { return mm->impl.update_device_memory(num_copy_calls); });
 }
 
+int svo_mm_plan_uploads(svo_mm* mm, uint32_t* h_first_slots, uint32_t* h_slot_counts,
+                        uint32_t capacity, uint32_t* num_ranges) {
+  if (!mm) return SVO_ERR_INVALID;
+  return guarded([&] {
+    const auto r = mm->impl.upload_ranges();
+    if (num_ranges) *num_ranges = (uint32_t)r.size();
+    if (!h_first_slots && !h_slot_counts) return SVO_OK;
+    if (capacity < r.size()) return SVO_ERR_RANGE;
+    for (size_t i = 0; i < r.size(); ++i) {
+      if (h_first_slots) h_first_slots[i] = r[i].first;
+      if (h_slot_counts) h_slot_counts[i] = r[i].second;
+    }
+    return SVO_OK;
+  });
+}
+
 int svo_mm_reset(svo_mm* mm) {
   if (!mm) return SVO_ERR_INVALID;
   return guarded([&] { return mm->impl.reset_incore_buffer(); });

@@ -9,8 +9,10 @@
 // (src/TreeletBuilderFromFaces.cpp:189-365), leaves left in the queue become
 // the roots of sub-treelets whose gid is written into the leaf
 // (src/TreeletBuildManager.cpp:211-233), treelets processed first in, first
-// out.  One addition: a treelet stops expanding `treelet_levels` below its
-// root, so a scene can be cut into treelets of a given number of levels.
+// out.  One addition: treelet boundaries at fixed levels (every
+// `treelet_levels` levels, counted up from the leaves), so a scene can be cut
+// into treelets of a given number of levels; the slot size then defaults to
+// the largest such treelet.
 #include "scene.h"
 
 #include <algorithm>
@@ -182,6 +184,24 @@ uint64_t bounded_count(const Octree& t, uint32_t level, uint64_t index, uint32_t
   return total;
 }
 
+// Treelet boundaries sit at the levels D, D-L, D-2L, ...: a treelet rooted
+// at level r expands down to the next boundary below it, so every treelet
+// but the top one spans exactly L levels and ends on the octree's leaves.
+//
+// A treelet other than the top one never spans a single level above the
+// leaves.  Its sub-treelet leaves would then hang off its root node, and the
+// manager clears their leaf flag in the treelet's own slot
+// (TreeletMemoryManager.cpp:535) while the traversal reads the copy of that
+// root made earlier in the parent's leaf (:532): the sub-treelets would be
+// resident but never reached.
+uint32_t stop_level(uint32_t D, uint32_t L, uint32_t r) {
+  if (L == 0) return D;
+  const uint32_t m = (D - r) % L;
+  uint32_t stop = r + (m == 0 ? L : m);
+  if (stop == r + 1 && stop < D && r > 0) stop = std::min(D, stop + L);
+  return stop;
+}
+
 struct TreeletRoot {
   uint32_t level;
   uint64_t index;
@@ -208,9 +228,9 @@ int cut_treelets(const Octree& tree, uint32_t treelet_levels, uint32_t treelet_b
     if (treelet_levels == 0) {
       need = tree.total_nodes();
     } else {
-      for (uint32_t r = 0; r < D; r += treelet_levels)
+      for (uint32_t r = 0; r < D; r = stop_level(D, treelet_levels, r))
         for (uint64_t i = 0; i < tree.codes[r].size(); ++i)
-          need = std::max(need, bounded_count(tree, r, i, treelet_levels));
+          need = std::max(need, bounded_count(tree, r, i, stop_level(D, treelet_levels, r) - r));
     }
     N = need + 8;
   } else {
@@ -241,11 +261,11 @@ int cut_treelets(const Octree& tree, uint32_t treelet_levels, uint32_t treelet_b
     t.parent_leaf_parent_position = r.leaf_parent_pos;
     t.nodes.push_back(svo_node{0u, 0u});
     t.attribs.push_back(tree.attribs[r.level][r.index]);
-    const uint32_t stop_level = treelet_levels ? std::min(D, r.level + treelet_levels) : D;
+    const uint32_t stop = stop_level(D, treelet_levels, r.level);
     q.clear();
     q.push_back(FillItem{r.level, r.index, 0u, 0u, 0u});
     uint64_t current = 1;
-    while (!q.empty() && current < N - 8 && q.front().level < stop_level) {
+    while (!q.empty() && current < N - 8 && q.front().level < stop) {
       const FillItem f = q.front();
       const uint8_t m = tree.masks[f.level][f.index];
       const uint64_t fc = tree.first[f.level][f.index];
@@ -268,6 +288,8 @@ int cut_treelets(const Octree& tree, uint32_t treelet_levels, uint32_t treelet_b
     t.num_leaves = (uint32_t)q.size();
     for (const FillItem& f : q) {
       if (f.local == 0) return SVO_ERR_RANGE;  // treelet too small to expand its root
+      // see stop_level(): sub-treelets must not hang off a non-top root
+      if (t.gid != 0 && f.parent_local == 0 && f.level < D) return SVO_ERR_RANGE;
       t.nodes[f.parent_local].masks |= 1u << f.idx;
       if (f.level < D) {
         if (next_gid > 0x7FFFFFFFull) return SVO_ERR_RANGE;

@@ -10,7 +10,10 @@ configurations name:
 * ``icosphere`` -- icosphere subdivided 6 times (81,920 triangles), radius
                    0.4 displaced radially by 3-octave value noise of amplitude
                    0.05, depth-11 octree cut into 6-level treelets, colour from
-                   the face normal; one 1920x1080 view from radius 2.5.
+                   the face normal; one 1920x1080 view from an orbit of radius
+                   2.5.  The configuration names no field of view; 25 degrees
+                   (vertical) makes the sphere fill the frame height, so most
+                   rays enter the octree.
 """
 from __future__ import annotations
 
@@ -19,7 +22,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from . import Camera, Scene, orbit_camera
+from . import Camera, Scene, icosphere as icosphere_mesh, orbit_camera, terrain as terrain_mesh
 
 
 @dataclass
@@ -47,3 +50,16 @@ def orbit_pose(radius: float, angle_deg: float, elevation_deg: float, width: int
     a, e = math.radians(angle_deg), math.radians(elevation_deg)
     eye = (radius * math.cos(e) * math.cos(a), radius * math.sin(e), radius * math.cos(e) * math.sin(a))
     return Camera(eye, (0.0, 0.0, 0.0), width, height, fov_deg)
+
+
+def icosphere(subdivisions=6, depth=11, treelet_levels=6, seed=1, width=1920, height=1080,
+              fov_deg=25.0, radius=2.5) -> Workload:
+    v, t = icosphere_mesh(subdivisions, radius=0.4, octaves=3, amplitude=0.05, frequency=2.0, seed=seed)
+    scene = Scene.from_mesh(v, t, depth, treelet_levels=treelet_levels)
+    rng = np.random.default_rng(seed)
+    cam = orbit_pose(radius, float(rng.uniform(0, 360)), float(rng.uniform(-30, 30)), width, height,
+                     fov_deg)
+    return Workload(f"icosphere_s{subdivisions}_d{depth}_{width}x{height}", scene, [cam],
+                    description=f"icosphere {subdivisions}x subdivided ({t.shape[0]} triangles), 3-octave "
+                                f"noise 0.05, depth {depth}, {treelet_levels}-level treelets, {width}x{height}, "
+                                f"orbit radius {radius}, fov {fov_deg}")

@@ -1,0 +1,65 @@
+"""Generates the golden fixtures in this directory from the reference's own
+ray cast (opencl/treeletRenderer_rgba.cl compiled for the host by
+oracle/build_ref.py).  Needs the reference checkout; run from the repo root:
+
+    python tests/golden/make_golden.py
+
+Each fixture holds a node/attribute pool, frame parameters and rays, and the
+reference's outputs for them: renderToBuffer's float RGBA per pixel and
+sample()'s hit record per ray (node index, t, depth, hit, loop count).
+"""
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "tests"))
+
+import libsvo_b200 as L  # noqa: E402
+import oracle  # noqa: E402
+from rays import edge_rays, paged_menger_manager, random_octree_pool  # noqa: E402
+
+HERE = Path(__file__).resolve().parent
+
+
+def fixture(name, nodes, attribs, frames, rays, tsrs):
+    oracle.build_reference()
+    assert oracle.reference_lib() is not None, "reference build missing"
+    out = {"nodes": nodes, "attribs": attribs}
+    for i, p in enumerate(frames):
+        out[f"params_{i}"] = np.frombuffer(bytes(p), dtype=np.uint8)
+        out[f"rgbaf_{i}"] = oracle.reference_render(nodes, attribs, bytes(p))
+    o, d = rays
+    out["origins"], out["dirs"] = o, d
+    for j, tsr in enumerate(tsrs):
+        h = oracle.reference_sample_rays(nodes, o, d, tsr)
+        out[f"tsr_{j}"] = np.float32(tsr)
+        for k in ("node", "t", "depth", "hit", "loops"):
+            out[f"hits_{j}_{k}"] = h[k]
+    np.savez_compressed(HERE / f"{name}.npz", **out)
+    print(name, sum(v.nbytes for v in out.values() if hasattr(v, "nbytes")), "bytes raw")
+
+
+def main():
+    s = L.Scene.menger(level=3, depth=5, seed=7)
+    mm = L.TreeletMemoryManagerCuda(s, s.info.treelet_bytes)
+    n, a = mm.getIncoreBuffer()
+    cams = [L.orbit_camera(1, 64, 48, radius=1.6), L.orbit_camera(2, 40, 40, radius=1.2)]
+    frames = [cams[0].frame_params(), cams[0].frame_params(t_scale_ratio=0.0),
+              cams[1].frame_params(mode=3), cams[1].frame_params(mode=5, t_scale_ratio=0.01)]
+    fixture("menger_l3_d5", n, a, frames, edge_rays(n_random=3000, seed=1), [0.0, 0.004])
+
+    n, a = random_octree_pool(11, depth=5)
+    frames = [L.orbit_camera(3, 48, 48, radius=(1.0, 2.0)).frame_params(t_scale_ratio=0.0)]
+    fixture("random_d5", n, a, frames, edge_rays(n_random=2000, seed=2), [0.0, 0.01])
+
+    _, mm = paged_menger_manager()
+    n, a = mm.getIncoreBuffer()
+    frames = [L.orbit_camera(7, 64, 64, radius=1.4).frame_params(t_scale_ratio=0.0)]
+    fixture("menger_paged", n, a, frames, edge_rays(n_random=2000, seed=3), [0.0])
+
+
+if __name__ == "__main__":
+    main()

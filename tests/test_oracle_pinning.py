@@ -1,0 +1,111 @@
+"""Pins the oracle to the reference: the restated traversal must agree bit for
+bit with the reference's own treelet kernel source (opencl/
+treeletRenderer_rgba.cl), compiled for the host by oracle/build_ref.py.
+
+These tests need the reference build (oracle/_ref); where it is absent the
+committed golden fixtures (tests/test_golden.py) carry the same check.
+"""
+import numpy as np
+import pytest
+
+import libsvo_b200 as L
+import oracle
+from rays import edge_rays, paged_menger_manager, random_octree_pool
+
+ref_needed = pytest.mark.skipif(oracle.reference_lib() is None,
+                                reason="reference kernel build (oracle/_ref) not present")
+
+
+def check_rays(nodes, o, d, tsr):
+    got, _ = oracle.cast_rays(nodes, o, d, tsr)
+    want = oracle.reference_sample_rays(nodes, o, d, tsr)
+    for k in ("node", "depth", "hit", "loops"):
+        bad = np.nonzero(got[k] != want[k])[0]
+        assert bad.size == 0, f"{k} differs at {bad.size} rays, first {bad[:5]}"
+    assert np.array_equal(got["t"].view(np.uint32), want["t"].view(np.uint32))
+    return got
+
+
+def check_frame(nodes, attribs, params):
+    rgba, hits, _, rgbaf = oracle.render(nodes, attribs, bytes(params), want_rgbaf=True)
+    ref = oracle.reference_render(nodes, attribs, bytes(params))
+    defined = np.ones(hits.shape, dtype=bool)
+    if params.mode == 4:
+        # pixel-depth shading reads SampleResult.t, which sample() leaves
+        # unwritten for rays that miss the root cube (uninitialised in the
+        # reference); the library defines t = 0 there
+        defined = (hits["flags"] & oracle.FLAG_BOX_MISS) == 0
+        assert defined.sum() > 0
+    assert np.array_equal(rgbaf[defined].view(np.uint32), ref[defined].view(np.uint32)), \
+        "fragment colours differ"
+    assert np.array_equal(rgba[defined], oracle.to_rgba8(ref)[defined])
+    o, d = oracle.pixel_rays(bytes(params))
+    check_rays(nodes, o, d, params.t_scale_ratio)
+    return hits
+
+
+@ref_needed
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_menger_frames(menger_scene, seed):
+    mm = L.TreeletMemoryManagerCuda(menger_scene, menger_scene.info.treelet_bytes)
+    nodes, attribs = mm.getIncoreBuffer()
+    cam = L.orbit_camera(seed, 320, 240)
+    for tsr in (None, 0.0, 0.02):
+        hits = check_frame(nodes, attribs, cam.frame_params(t_scale_ratio=tsr))
+        assert hits["hit"].sum() > 0
+
+
+@ref_needed
+@pytest.mark.parametrize("mode", [0, 1, 3, 4, 5])
+def test_view_modes(menger_scene, mode):
+    mm = L.TreeletMemoryManagerCuda(menger_scene, menger_scene.info.treelet_bytes)
+    nodes, attribs = mm.getIncoreBuffer()
+    check_frame(nodes, attribs, L.orbit_camera(4, 160, 100).frame_params(mode=mode))
+
+
+@ref_needed
+@pytest.mark.parametrize("tsr", [0.0, 0.003, 0.05])
+def test_edge_rays(menger_scene, tsr):
+    mm = L.TreeletMemoryManagerCuda(menger_scene, menger_scene.info.treelet_bytes)
+    nodes, _ = mm.getIncoreBuffer()
+    o, d = edge_rays(n_random=5000)
+    check_rays(nodes, o, d, tsr)
+
+
+@ref_needed
+def test_paged_pool():
+    _, mm = paged_menger_manager()
+    nodes, attribs = mm.getIncoreBuffer()
+    assert (nodes[:, 0].view(np.int32) < 0).any()
+    check_frame(nodes, attribs, L.orbit_camera(7, 200, 200, radius=1.4).frame_params(t_scale_ratio=0.0))
+
+
+@ref_needed
+@pytest.mark.parametrize("seed", range(8))
+def test_random_octrees(seed):
+    nodes, attribs = random_octree_pool(seed, depth=3 + seed % 4)
+    check_frame(nodes, attribs, L.orbit_camera(seed, 96, 64, radius=(1.0, 2.0)).frame_params(t_scale_ratio=0.0))
+    o, d = edge_rays(n_random=2000, seed=seed)
+    check_rays(nodes, o, d, 0.0)
+
+
+@ref_needed
+def test_icosphere_frame():
+    from libsvo_b200 import scenes
+
+    wl = scenes.icosphere(subdivisions=5, depth=9, treelet_levels=4, width=320, height=180)
+    info = wl.scene.info
+    mm = L.TreeletMemoryManagerCuda(wl.scene, info.treelet_bytes * info.num_treelets)
+    mm.insertAll()
+    nodes, attribs = mm.getIncoreBuffer()
+    hits = check_frame(nodes, attribs, wl.cameras[0].frame_params())
+    assert hits["hit"].mean() > 0.1
+
+
+def test_unorm8_conversion_is_exact_for_packed_bytes():
+    """The colour epilogue maps each packed byte b to b * 0.003921569f and
+    back to round(c * 255): every byte survives."""
+    b = np.arange(256, dtype=np.float32)
+    c = b * np.float32(0.003921569)
+    back = np.floor(c * np.float32(255.0) + np.float32(0.5))
+    assert np.array_equal(back, b)

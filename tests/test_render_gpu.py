@@ -8,6 +8,7 @@ import pytest
 
 import libsvo_b200 as L
 import oracle
+from rays import edge_rays, paged_menger_manager, random_octree_pool
 
 pytestmark = pytest.mark.gpu
 
@@ -109,33 +110,6 @@ def test_flat_traversal_matches_oracle(menger_scene, cuda):
         assert np.array_equal(rgba.cpu().numpy().view(np.uint32), o_rgba)
 
 
-def edge_rays(n_random=20000, seed=0):
-    rng = np.random.default_rng(seed)
-    o, d = [], []
-    # axis-aligned and zero components, from outside and inside the cube
-    for origin in ([0.1, 0.2, 3.0], [0.0, 0.0, 2.0], [0.0, 0.0, 0.0], [0.25, -0.25, 0.1],
-                   [0.5, 0.5, 2.0], [-0.5, 0.3, -3.0]):
-        for dirv in ([0, 0, -1], [0, 0, 1], [1, 0, 0], [0, -1, 0], [0, 0.00005, -1], [1e-6, 0, -1],
-                     [-0.0, 0.0, -1.0], [0.3, 0.4, -0.866]):
-            o.append(origin)
-            v = np.asarray(dirv, dtype=np.float64)
-            d.append(v / np.linalg.norm(v))
-    # grazing rays along cube faces and edges
-    for s in np.linspace(-0.5, 0.5, 11):
-        o.append([s, 0.5, 2.0]); d.append([0.0, 0.0, -1.0])
-        o.append([0.5, s, -2.0]); d.append([0.0, 0.0, 1.0])
-        o.append([-2.0, s, s]); d.append([1.0, 0.0, 0.0])
-    # random rays from a shell and from inside
-    eo = rng.normal(size=(n_random, 3))
-    eo = eo / np.linalg.norm(eo, axis=1, keepdims=True) * rng.uniform(0.0, 2.5, size=(n_random, 1))
-    tgt = rng.uniform(-0.5, 0.5, size=(n_random, 3))
-    ed = tgt - eo
-    ed /= np.linalg.norm(ed, axis=1, keepdims=True)
-    o = np.concatenate([np.asarray(o, dtype=np.float64), eo]).astype(np.float32)
-    d = np.concatenate([np.asarray(d, dtype=np.float64), ed]).astype(np.float32)
-    return o, d
-
-
 @pytest.mark.parametrize("tsr", [0.0, 0.003])
 def test_explicit_rays_edge_cases(menger_mm, cuda, tsr):
     torch = _torch()
@@ -149,31 +123,6 @@ def test_explicit_rays_edge_cases(menger_mm, cuda, tsr):
     torch.cuda.synchronize()
     o_hits, _ = oracle.cast_rays(nodes, o, d, tsr)
     assert_hits_equal(_hits_np(hits), o_hits, "edge rays")
-
-
-def paged_menger_manager():
-    """A Menger octree cut into 3-level treelets and paged so that child
-    treelets sit in slots below their parents: first-child deltas are then
-    negative and the index arithmetic wraps mod 2^32."""
-    scene = L.Scene.menger(level=4, depth=7, seed=3, treelet_levels=3, treelet_bytes=8 * 1024)
-    ntl = scene.info.num_treelets
-    parents = np.array([scene.treelet(g)["parent_gid"] for g in range(ntl)])
-    top = [g for g in range(1, ntl) if parents[g] == 0]
-    mm = L.TreeletMemoryManagerCuda(scene, scene.info.treelet_bytes * ntl)
-    for g in top:
-        assert mm.insertTreeletIntoIncoreBuffer(g)
-    # free the low slots of the first few top treelets, then page in the
-    # children of the last ones: they land below their parents
-    k = min(8, len(top) // 2)
-    for g in top[:k]:
-        assert mm.removeTreeletFromIncoreBuffer(g)
-    for g in top[::-1][:k]:
-        for c in np.nonzero(parents == g)[0]:
-            if c != 0:
-                assert mm.insertTreeletIntoIncoreBuffer(int(c))
-    for g in top[:k]:
-        assert mm.insertTreeletIntoIncoreBuffer(g)
-    return scene, mm
 
 
 def test_paged_pool_with_relative_indices(cuda):
@@ -214,9 +163,43 @@ def test_bounds_errors_are_reported_not_faulted(cuda):
 
 
 def test_mm_render_host_matches_device(menger_mm):
+    menger_mm.sync()  # clear counters left by earlier tests
     p = L.orbit_camera(2, 300, 200).frame_params()
     host = menger_mm.render_host(p)
     rgba, _ = gpu_frame(menger_mm, p)
     assert np.array_equal(host, rgba)
     st = menger_mm.sync()
     assert st.capped_rays == 0 and st.bounds_errors == 0
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_random_octrees(cuda, seed):
+    torch = _torch()
+    nodes, attribs = random_octree_pool(seed, depth=4 + seed % 3)
+    dn = torch.from_numpy(nodes.view(np.int32)).to(cuda)
+    da = torch.from_numpy(attribs.view(np.int32)).to(cuda)
+    p = L.orbit_camera(seed, 160, 120, radius=(1.0, 2.0)).frame_params(t_scale_ratio=0.0)
+    rgba = torch.empty((p.height, p.width), dtype=torch.int32, device=cuda)
+    hits = torch.empty((p.height * p.width * 16,), dtype=torch.uint8, device=cuda)
+    L.render(dn, da, nodes.shape[0], p, rgba, hits)
+    torch.cuda.synchronize()
+    o_rgba, o_hits, _, _ = oracle.render(nodes, attribs, bytes(p))
+    assert_hits_equal(_hits_np(hits), o_hits, "random octree")
+    assert np.array_equal(rgba.cpu().numpy().view(np.uint32), o_rgba)
+
+
+def test_icosphere_frame_matches_oracle(cuda):
+    from libsvo_b200 import scenes
+
+    wl = scenes.icosphere(subdivisions=5, depth=9, treelet_levels=4, width=480, height=270)
+    info = wl.scene.info
+    mm = L.TreeletMemoryManagerCuda(wl.scene, info.treelet_bytes * info.num_treelets)
+    assert mm.insertAll() == info.num_treelets - 1
+    mm.initDeviceBuffer()
+    nodes, attribs = mm.getIncoreBuffer()
+    for p in (wl.cameras[0].frame_params(), wl.cameras[0].frame_params(t_scale_ratio=0.0)):
+        rgba, hits = gpu_frame(mm, p)
+        o_rgba, o_hits, _, _ = oracle.render(nodes, attribs, bytes(p))
+        assert_hits_equal(hits, o_hits, "icosphere")
+        assert np.array_equal(rgba, o_rgba)
+    mm.close()
