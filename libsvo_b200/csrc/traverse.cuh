@@ -83,9 +83,192 @@ __device__ __forceinline__ bool root_slab(const float o[3], const float d[3], fl
   return true;
 }
 
-// The ray cast.  kFlat selects the CpuRaycasterSingleRay3 rules; S is the
-// stack size (treelet) or the octree depth (flat).  `stack` points at this
-// thread's column of the shared-memory stack, `stride` words apart.
+// The descent loop.  kFlat selects the CpuRaycasterSingleRay3 rules; S is
+// the stack size (treelet) or the octree depth (flat).  `stack` points at
+// this thread's column of the shared-memory stack, `stride` words apart.
+//
+// Per frame (set on push and pop) the registers hold the node, its tMin and
+// tMax, its centre, the child size sx2 and half of it, and the node record,
+// which is loaded as soon as the node is known so the load overlaps the
+// entry-point arithmetic of the next iteration.
+//
+// kSigned: the reference orders each child's slab distances with a compare
+// and swap (tx0 > tx1).  When the reciprocal r is finite, rounding is
+// monotone, so the swap happens exactly when r < 0 (equal values swap to
+// themselves): the near face is lo when r > 0 and hi when r < 0.  With
+// m = bit + neg - 1 for the near face and bit - neg for the far face
+// (neg = 1 when r < 0), the faces are c + m * sx2 with m in {-1, 0, 1}, which
+// is exact, so the distances are the reference's bits computed on the FMA
+// pipe instead of the compare/select pipe.  Rays with an infinite or NaN
+// reciprocal (a direction component of exactly zero) take kSigned = false,
+// the literal compare and swap.
+template <bool kFlat, bool kSigned>
+__device__ __forceinline__ void descend(const uint2* __restrict__ nodes, uint64_t num_nodes,
+                                        const float o[3], float dx, float dy, float dz, float rx,
+                                        float px, float ry, float py, float rz, float pz,
+                                        float t_min, float t_max, float tsr, int S, uint2* stack,
+                                        int stride, RayHit& h) {
+  const float eps = 0.00001f;
+  // per-axis near/far offsets (kSigned): near m = bit + kn, far m = bit + kf
+  const float knx = rx < 0.0f ? 0.0f : -1.0f, kfx = rx < 0.0f ? -1.0f : 0.0f;
+  const float kny = ry < 0.0f ? 0.0f : -1.0f, kfy = ry < 0.0f ? -1.0f : 0.0f;
+  const float knz = rz < 0.0f ? 0.0f : -1.0f, kfz = rz < 0.0f ? -1.0f : 0.0f;
+  const uint32_t max_loops = (uint32_t)((S + 1) * (S + 1) * 5);
+  int scale = S - 1;
+  uint32_t node = 0u;
+  float tmin = t_min, tmax = t_max;
+  uint32_t ix = 0u, iy = 0u, iz = 0u;  // lattice coordinate at depth S-1-scale
+  float cx = 0.0f, cy = 0.0f, cz = 0.0f;
+  float sx2 = 0.5f, half = 0.25f;
+  bool in_pool = num_nodes > 0u;
+  uint2 nd = in_pool ? __ldg(nodes) : make_uint2(0u, 0u);
+  uint32_t loops = 0u, fetches = 0u;
+
+  while (scale < S) {
+    ++loops;
+    if (loops == max_loops) {
+      h.flags = SVO_HITFLAG_CAPPED;
+      h.loops = loops;
+      h.fetches = fetches;
+      if (!kFlat) {  // sample() reports the current node as a hit (:268-277)
+        h.hit = 1u;
+        h.node = node;
+        h.depth = (uint32_t)(S - scale);
+        h.t = tmin;
+      }
+      return;
+    }
+    bool pop;
+    if (kFlat)
+      pop = (tmax < 0.0f) || (fabsf(__fsub_rn(tmin, tmax)) < eps) || !(tmin < tmax);
+    else
+      pop = (tmax < 0.0f) || !(fabsf(__fsub_rn(tmin, tmax)) > eps);
+    if (pop) {
+      ++scale;
+      if (scale < S) {
+        const uint2 e = stack[(S - 1 - scale) * stride];
+        tmin = tmax;
+        node = e.x;
+        tmax = __uint_as_float(e.y);
+        in_pool = (uint64_t)node < num_nodes;
+        if (in_pool) nd = __ldg(nodes + node);
+        ix >>= 1;
+        iy >>= 1;
+        iz >>= 1;
+        const int k = S - 1 - scale;
+        cx = cell_center(ix, k);
+        cy = cell_center(iy, k);
+        cz = cell_center(iz, k);
+        sx2 = __fmul_rn(sx2, 2.0f);
+        half = __fmul_rn(sx2, 0.5f);
+      }
+      continue;
+    }
+    const float te = __fadd_rn(tmin, eps);
+    const float ex = __fsub_rn(__fadd_rn(o[0], __fmul_rn(te, dx)), cx);
+    const float ey = __fsub_rn(__fadd_rn(o[1], __fmul_rn(te, dy)), cy);
+    const float ez = __fsub_rn(__fadd_rn(o[2], __fmul_rn(te, dz)), cz);
+    const float fbx = ex > 0.0f ? 1.0f : 0.0f;
+    const float fby = ey > 0.0f ? 1.0f : 0.0f;
+    const float fbz = ez > 0.0f ? 1.0f : 0.0f;
+    float tx0, tx1, ty0, ty1, tz0, tz1;
+    if (kSigned) {
+      tx0 = __fadd_rn(__fmul_rn(rx, __fadd_rn(cx, __fmul_rn(__fadd_rn(fbx, knx), sx2))), px);
+      tx1 = __fadd_rn(__fmul_rn(rx, __fadd_rn(cx, __fmul_rn(__fadd_rn(fbx, kfx), sx2))), px);
+      ty0 = __fadd_rn(__fmul_rn(ry, __fadd_rn(cy, __fmul_rn(__fadd_rn(fby, kny), sx2))), py);
+      ty1 = __fadd_rn(__fmul_rn(ry, __fadd_rn(cy, __fmul_rn(__fadd_rn(fby, kfy), sx2))), py);
+      tz0 = __fadd_rn(__fmul_rn(rz, __fadd_rn(cz, __fmul_rn(__fadd_rn(fbz, knz), sx2))), pz);
+      tz1 = __fadd_rn(__fmul_rn(rz, __fadd_rn(cz, __fmul_rn(__fadd_rn(fbz, kfz), sx2))), pz);
+    } else {
+      // child centre (-0.5 + b) * sx2 + c = c +- half; faces ccx -+ half
+      const float ccx = __fadd_rn(fbx != 0.0f ? half : -half, cx);
+      const float ccy = __fadd_rn(fby != 0.0f ? half : -half, cy);
+      const float ccz = __fadd_rn(fbz != 0.0f ? half : -half, cz);
+      tx0 = __fadd_rn(__fmul_rn(rx, __fsub_rn(ccx, half)), px);
+      tx1 = __fadd_rn(__fmul_rn(rx, __fadd_rn(ccx, half)), px);
+      if (tx0 > tx1) {
+        const float s = tx0;
+        tx0 = tx1;
+        tx1 = s;
+      }
+      ty0 = __fadd_rn(__fmul_rn(ry, __fsub_rn(ccy, half)), py);
+      ty1 = __fadd_rn(__fmul_rn(ry, __fadd_rn(ccy, half)), py);
+      if (ty0 > ty1) {
+        const float s = ty0;
+        ty0 = ty1;
+        ty1 = s;
+      }
+      tz0 = __fadd_rn(__fmul_rn(rz, __fsub_rn(ccz, half)), pz);
+      tz1 = __fadd_rn(__fmul_rn(rz, __fadd_rn(ccz, half)), pz);
+      if (tz0 > tz1) {
+        const float s = tz0;
+        tz0 = tz1;
+        tz1 = s;
+      }
+    }
+    const float tc_min = cl_max(tx0, cl_max(ty0, tz0));
+    const float tc_max = cl_min(tx1, cl_min(ty1, tz1));
+
+    if (!in_pool) {
+      h.flags = SVO_HITFLAG_BOUNDS;
+      h.loops = loops;
+      h.fetches = fetches;
+      return;
+    }
+    ++fetches;
+    const uint32_t bx = fbx != 0.0f, by = fby != 0.0f, bz = fbz != 0.0f;
+    const uint32_t ci = (bx << 2) | (by << 1) | bz;
+    const uint32_t masks = nd.y;
+    if ((masks >> (ci + 8u)) & 1u) {
+      const uint32_t below = __popc((masks >> 8) & ((1u << ci) - 1u));
+      const uint32_t child = (kFlat ? 0u : node) + nd.x + below;
+      const bool leaf = (masks >> ci) & 1u;
+      const bool lod = kFlat ? (__fmul_rn(tsr, tc_max) > sx2)
+                             : (__fmul_rn(tsr, tc_min) > sx2 || scale == 1);
+      if (leaf || lod) {
+        h.hit = 1u;
+        h.node = child;
+        h.depth = (uint32_t)((leaf || kFlat) ? (S - scale) : (S - scale + 1));
+        h.t = tmin;
+        h.loops = loops;
+        h.fetches = fetches;
+        return;
+      }
+      if (kFlat && scale == 0) {  // non-leaf below the octree's depth: corrupt pool
+        h.flags = SVO_HITFLAG_BOUNDS;
+        h.loops = loops;
+        h.fetches = fetches;
+        return;
+      }
+      // push: the current frame's tMin becomes tc_max (recovered on pop)
+      stack[(S - 1 - scale) * stride] = make_uint2(node, __float_as_uint(tmax));
+      --scale;
+      node = child;
+      in_pool = (uint64_t)node < num_nodes;
+      if (in_pool) nd = __ldg(nodes + node);
+      tmin = tc_min;
+      tmax = tc_max;
+      ix = (ix << 1) | bx;
+      iy = (iy << 1) | by;
+      iz = (iz << 1) | bz;
+      cx = __fadd_rn(bx ? half : -half, cx);
+      cy = __fadd_rn(by ? half : -half, cy);
+      cz = __fadd_rn(bz ? half : -half, cz);
+      sx2 = half;
+      half = __fmul_rn(half, 0.5f);
+      continue;
+    }
+    tmin = tc_max;  // advance to the next sibling
+  }
+  h.hit = 0u;
+  h.node = 0u;
+  h.depth = 0u;
+  h.t = kFlat ? 0.0f : t_max;
+  h.loops = loops;
+  h.fetches = fetches;
+}
+
+// One ray: root box test, direction clamp, then the descent.
 template <bool kFlat>
 __device__ __forceinline__ RayHit cast_ray(const uint2* __restrict__ nodes, uint64_t num_nodes,
                                            const float o[3], float dx, float dy, float dz,
@@ -109,8 +292,8 @@ __device__ __forceinline__ RayHit cast_ray(const uint2* __restrict__ nodes, uint
   }
   // Direction clamp: sample() replaces |d| < 1e-4 by 1e-4 * sign(d)
   // (:231-239); traversSvo replaces |d| < 1e-5 by 1e-5 * sign(d) * 10 (:184-186).
-  const float eps = 0.00001f;
   if (kFlat) {
+    const float eps = 0.00001f;
     if (fabsf(dx) < eps) dx = __fmul_rn(__fmul_rn(eps, cl_sign(dx)), 10.0f);
     if (fabsf(dy) < eps) dy = __fmul_rn(__fmul_rn(eps, cl_sign(dy)), 10.0f);
     if (fabsf(dz) < eps) dz = __fmul_rn(__fmul_rn(eps, cl_sign(dz)), 10.0f);
@@ -123,142 +306,12 @@ __device__ __forceinline__ RayHit cast_ray(const uint2* __restrict__ nodes, uint
   const float rx = __frcp_rn(dx), px = __fmul_rn(-o[0], rx);
   const float ry = __frcp_rn(dy), py = __fmul_rn(-o[1], ry);
   const float rz = __frcp_rn(dz), pz = __fmul_rn(-o[2], rz);
-
-  const uint32_t max_loops = (uint32_t)((S + 1) * (S + 1) * 5);
-  int scale = S - 1;
-  // Current frame: node, tMin, tMax, lattice coordinate (depth S-1-scale).
-  uint32_t node = 0u;
-  float tmin = t_min, tmax = t_max;
-  uint32_t ix = 0u, iy = 0u, iz = 0u;
-  uint2 nd = make_uint2(0u, 0u);
-  bool have_node = false;
-  uint32_t loops = 0u, fetches = 0u;
-
-  while (scale < S) {
-    const int k = S - 1 - scale;  // depth of the current node
-    const float sx2 = pow2i(scale - S);
-    const float half = __fmul_rn(sx2, 0.5f);
-    ++loops;
-    if (loops == max_loops) {
-      h.flags = SVO_HITFLAG_CAPPED;
-      h.loops = loops;
-      h.fetches = fetches;
-      if (!kFlat) {  // sample() reports the current node as a hit (:268-277)
-        h.hit = 1u;
-        h.node = node;
-        h.depth = (uint32_t)(S - scale);
-        h.t = tmin;
-      }
-      return h;
-    }
-    bool pop;
-    if (kFlat)
-      pop = (tmax < 0.0f) || (fabsf(__fsub_rn(tmin, tmax)) < eps) || !(tmin < tmax);
-    else
-      pop = (tmax < 0.0f) || !(fabsf(__fsub_rn(tmin, tmax)) > eps);
-    if (pop) {
-      ++scale;
-      if (scale < S) {
-        const uint2 e = stack[(S - 1 - scale) * stride];
-        tmin = tmax;
-        node = e.x;
-        tmax = __uint_as_float(e.y);
-        ix >>= 1;
-        iy >>= 1;
-        iz >>= 1;
-        have_node = false;
-      }
-      continue;
-    }
-    const float cx = cell_center(ix, k), cy = cell_center(iy, k), cz = cell_center(iz, k);
-    const float te = __fadd_rn(tmin, eps);
-    const float ex = __fsub_rn(__fadd_rn(o[0], __fmul_rn(te, dx)), cx);
-    const float ey = __fsub_rn(__fadd_rn(o[1], __fmul_rn(te, dy)), cy);
-    const float ez = __fsub_rn(__fadd_rn(o[2], __fmul_rn(te, dz)), cz);
-    const uint32_t bx = ex > 0.0f, by = ey > 0.0f, bz = ez > 0.0f;
-    const uint32_t ci = (bx << 2) | (by << 1) | bz;
-    const float ccx = __fadd_rn(__fmul_rn(bx ? 0.5f : -0.5f, sx2), cx);
-    const float ccy = __fadd_rn(__fmul_rn(by ? 0.5f : -0.5f, sx2), cy);
-    const float ccz = __fadd_rn(__fmul_rn(bz ? 0.5f : -0.5f, sx2), cz);
-    float tx0 = __fadd_rn(__fmul_rn(rx, __fsub_rn(ccx, half)), px);
-    float tx1 = __fadd_rn(__fmul_rn(rx, __fadd_rn(ccx, half)), px);
-    if (tx0 > tx1) {
-      const float s = tx0;
-      tx0 = tx1;
-      tx1 = s;
-    }
-    float ty0 = __fadd_rn(__fmul_rn(ry, __fsub_rn(ccy, half)), py);
-    float ty1 = __fadd_rn(__fmul_rn(ry, __fadd_rn(ccy, half)), py);
-    if (ty0 > ty1) {
-      const float s = ty0;
-      ty0 = ty1;
-      ty1 = s;
-    }
-    float tz0 = __fadd_rn(__fmul_rn(rz, __fsub_rn(ccz, half)), pz);
-    float tz1 = __fadd_rn(__fmul_rn(rz, __fadd_rn(ccz, half)), pz);
-    if (tz0 > tz1) {
-      const float s = tz0;
-      tz0 = tz1;
-      tz1 = s;
-    }
-    const float tc_min = cl_max(tx0, cl_max(ty0, tz0));
-    const float tc_max = cl_min(tx1, cl_min(ty1, tz1));
-
-    if (!have_node) {
-      if ((uint64_t)node >= num_nodes) {
-        h.flags = SVO_HITFLAG_BOUNDS;
-        h.loops = loops;
-        h.fetches = fetches;
-        return h;
-      }
-      nd = __ldg(nodes + node);
-      have_node = true;
-    }
-    ++fetches;
-    const uint32_t masks = nd.y;
-    if ((masks >> (ci + 8u)) & 1u) {
-      const uint32_t below = __popc((masks >> 8) & ((1u << ci) - 1u));
-      const uint32_t child = (kFlat ? 0u : node) + nd.x + below;
-      if ((masks >> ci) & 1u) {  // leaf
-        h.hit = 1u;
-        h.node = child;
-        h.depth = (uint32_t)(S - scale);
-        h.t = tmin;
-        h.loops = loops;
-        h.fetches = fetches;
-        return h;
-      }
-      const bool lod = kFlat ? (__fmul_rn(tsr, tc_max) > sx2)
-                             : (__fmul_rn(tsr, tc_min) > sx2 || scale == 1);
-      if (lod) {
-        h.hit = 1u;
-        h.node = child;
-        h.depth = (uint32_t)(kFlat ? (S - scale) : (S - scale + 1));
-        h.t = tmin;
-        h.loops = loops;
-        h.fetches = fetches;
-        return h;
-      }
-      // push: the current frame's tMin becomes tc_max (recovered on pop).
-      stack[(S - 1 - scale) * stride] = make_uint2(node, __float_as_uint(tmax));
-      --scale;
-      node = child;
-      tmin = tc_min;
-      tmax = tc_max;
-      ix = (ix << 1) | bx;
-      iy = (iy << 1) | by;
-      iz = (iz << 1) | bz;
-      have_node = false;
-      continue;
-    }
-    tmin = tc_max;  // advance to the next sibling
-  }
-  h.hit = 0u;
-  h.node = 0u;
-  h.depth = 0u;
-  h.t = kFlat ? 0.0f : t_max;
-  h.loops = loops;
-  h.fetches = fetches;
+  if (isfinite(rx) && isfinite(ry) && isfinite(rz))
+    descend<kFlat, true>(nodes, num_nodes, o, dx, dy, dz, rx, px, ry, py, rz, pz, t_min, t_max,
+                         tsr, S, stack, stride, h);
+  else
+    descend<kFlat, false>(nodes, num_nodes, o, dx, dy, dz, rx, px, ry, py, rz, pz, t_min, t_max,
+                          tsr, S, stack, stride, h);
   return h;
 }
 

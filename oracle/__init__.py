@@ -93,6 +93,8 @@ def reference_lib():
         L.ref_sample_rays.restype = None
         L.ref_render.argtypes = [vp, vp, vp, vp, i32]
         L.ref_render.restype = None
+        L.ref_render_rows.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32, vp, i32]
+        L.ref_render_rows.restype = None
         assert L.ref_hit_record_size() == 16
         _ref = L
     return _ref
@@ -160,8 +162,9 @@ def reference_sample_rays(nodes, origins, dirs, t_scale_ratio, threads=None):
     return hits
 
 
-def reference_render(nodes, attribs, params: bytes, threads=None):
-    """renderToBuffer from the reference source: float RGBA [H, W, 4]."""
+def reference_render(nodes, attribs, params: bytes, threads=None, rows=None):
+    """renderToBuffer from the reference source: float RGBA [H, W, 4]
+    (only rows [rows[0], rows[1]) when ``rows`` is given)."""
     L = reference_lib()
     if L is None:
         return None
@@ -170,7 +173,11 @@ def reference_render(nodes, attribs, params: bytes, threads=None):
     w, h = np.frombuffer(params[:8], dtype=np.uint32)
     out = np.zeros((h, w, 4), dtype=np.float32)
     pbuf = np.frombuffer(bytearray(params), dtype=np.uint8)
-    L.ref_render(_ptr(nodes), _ptr(attribs), _ptr(pbuf), _ptr(out), _threads(threads))
+    if rows is None:
+        L.ref_render(_ptr(nodes), _ptr(attribs), _ptr(pbuf), _ptr(out), _threads(threads))
+    else:
+        L.ref_render_rows(_ptr(nodes), _ptr(attribs), _ptr(pbuf), int(rows[0]), int(rows[1]), _ptr(out),
+                          _threads(threads))
     return out
 
 

@@ -334,6 +334,14 @@ Hit cast_flat(const uint32_t* nodes, uint64_t num_nodes, V3 o, V3 d, float tsr, 
         h.fetches = (uint16_t)fetches;
         return h;
       }
+      if (scale == 0) {
+        // a non-leaf child below the octree's depth: only a corrupt pool gets
+        // here, and the reference would index its stack at -1
+        h.flags = kFlagBounds;
+        h.loops = (uint16_t)loops;
+        h.fetches = (uint16_t)fetches;
+        return h;
+      }
       stack[scale].tmin = tc_max;
       --scale;
       stack[scale] = Frame{tc_min, tc_max, child, cc};
