@@ -278,6 +278,63 @@ int svo_mm_render_host(svo_mm* mm, const svo_frame_params* params, const svo_tra
  * (capped rays = the watchdog status word), then clears them. */
 int svo_mm_sync(svo_mm* mm, void* stream, svo_stats* out);
 
+/* ---- batched views: one persistent launch ------------------------------ */
+
+/* A resident octree: device node and attribute pools (e.g. from
+ * svo_mm_get_device_buffers) and how to traverse them. */
+typedef struct svo_octree_desc {
+  const svo_node* d_nodes;
+  const svo_attrib* d_attribs;
+  uint64_t num_nodes;
+  int32_t traversal;  /* SVO_TRAVERSAL_*                                   */
+  int32_t stack_size; /* as in svo_trace_cfg                               */
+} svo_octree_desc;
+
+/* One view of a batch: renderToBuffer's arguments, the octree it looks at
+ * (index into the batch's octree table) and its outputs. */
+typedef struct svo_view_desc {
+  svo_frame_params params;
+  uint32_t octree;
+  uint32_t reserved;
+  uint32_t* d_rgba; /* width*height RGBA8 pixels, byte 0 red           */
+  svo_hit* d_hits;  /* optional, width*height records                   */
+} svo_view_desc;
+
+typedef struct svo_batch_cfg {
+  uint32_t tile_w, tile_h;  /* pixels per warp tile: 8x4, 16x2, 4x8 or 32x1  */
+  uint32_t block_threads;   /* multiple of 32, 64..1024                      */
+  uint32_t blocks_per_sm;   /* persistent blocks per SM, 0 = as many as fit  */
+  uint32_t top_nodes;       /* records of octree 0 staged in shared memory   */
+  uint32_t use_graph;       /* replay a captured CUDA graph                  */
+} svo_batch_cfg;
+
+/* The launch unit of the reference is one frame (renderToBuffer enqueue,
+ * raycast_serialized_opencl.cpp:742-747); a batcher casts a ragged table of
+ * views over one or several octrees in one persistent, work-stealing launch
+ * (32-pixel tiles pulled from a device counter).  A batcher owns the device
+ * descriptor tables (allocated at creation) and is not thread-safe. */
+typedef struct svo_batcher svo_batcher;
+int svo_batcher_create(uint32_t max_views, uint32_t max_octrees, svo_batcher** out);
+void svo_batcher_destroy(svo_batcher* b);
+/* Sets the batch: validates and uploads the descriptors (waits for earlier
+ * work on `stream` first).  The octree pools and outputs must stay valid
+ * while launches of this batch run. */
+int svo_batcher_set(svo_batcher* b, const svo_octree_desc* octrees, uint32_t num_octrees,
+                    const svo_view_desc* views, uint32_t num_views, const svo_batch_cfg* cfg,
+                    void* stream);
+/* Casts every view of the current batch (asynchronous).  d_stats
+ * (optional) accumulates counters.  With cfg.use_graph the counter reset
+ * and the kernel are captured as a CUDA graph on the first launch and
+ * replayed afterwards. */
+int svo_batcher_launch(svo_batcher* b, svo_stats* d_stats, void* stream);
+/* Times each tile shape, block size and top-node staging on the current
+ * batch (`reps` launches each), keeps the fastest as the batch's
+ * configuration and returns it with its time per launch. */
+int svo_batcher_autotune(svo_batcher* b, uint32_t reps, void* stream, svo_batch_cfg* best,
+                         float* best_ms);
+/* Total tiles and rays of the current batch. */
+int svo_batcher_size(svo_batcher* b, uint64_t* tiles, uint64_t* rays);
+
 /* ---- misc -------------------------------------------------------------- */
 const char* svo_version(void);
 /* Last CUDA error string seen by the library on this thread ("" if none). */

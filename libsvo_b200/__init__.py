@@ -104,7 +104,25 @@ class svo_slot_info(ctypes.Structure):
                 ("error", ctypes.c_float)]
 
 
+class svo_octree_desc(ctypes.Structure):
+    _fields_ = [("d_nodes", ctypes.c_void_p), ("d_attribs", ctypes.c_void_p),
+                ("num_nodes", ctypes.c_uint64), ("traversal", ctypes.c_int32),
+                ("stack_size", ctypes.c_int32)]
+
+
+class svo_view_desc(ctypes.Structure):
+    _fields_ = [("params", svo_frame_params), ("octree", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("d_rgba", ctypes.c_void_p), ("d_hits", ctypes.c_void_p)]
+
+
+class svo_batch_cfg(ctypes.Structure):
+    _fields_ = [("tile_w", ctypes.c_uint32), ("tile_h", ctypes.c_uint32),
+                ("block_threads", ctypes.c_uint32), ("blocks_per_sm", ctypes.c_uint32),
+                ("top_nodes", ctypes.c_uint32), ("use_graph", ctypes.c_uint32)]
+
+
 assert ctypes.sizeof(svo_frame_params) == 80
+assert ctypes.sizeof(svo_view_desc) == 104
 
 _vp, _u32, _u64, _i32, _f32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32, ctypes.c_float
 _P = ctypes.POINTER
@@ -147,6 +165,13 @@ _SIGS = {
     "svo_mm_render": ([_vp, _P(svo_frame_params), _P(svo_trace_cfg), _vp, _vp, _vp], ctypes.c_int),
     "svo_mm_render_host": ([_vp, _P(svo_frame_params), _P(svo_trace_cfg), _vp, _vp], ctypes.c_int),
     "svo_mm_sync": ([_vp, _vp, _P(svo_stats)], ctypes.c_int),
+    "svo_batcher_create": ([_u32, _u32, _P(_vp)], ctypes.c_int),
+    "svo_batcher_destroy": ([_vp], None),
+    "svo_batcher_set": ([_vp, _P(svo_octree_desc), _u32, _P(svo_view_desc), _u32, _P(svo_batch_cfg), _vp],
+                        ctypes.c_int),
+    "svo_batcher_launch": ([_vp, _vp, _vp], ctypes.c_int),
+    "svo_batcher_autotune": ([_vp, _u32, _vp, _P(svo_batch_cfg), _P(_f32)], ctypes.c_int),
+    "svo_batcher_size": ([_vp, _P(_u64), _P(_u64)], ctypes.c_int),
 }
 for _name, (_args, _res) in _SIGS.items():
     _fn = getattr(_L, _name)
@@ -515,3 +540,75 @@ def trace_rays(d_nodes, num_nodes: int, d_origins, d_dirs, n: int, t_scale_ratio
     _check(_L.svo_trace_rays(_dptr(d_nodes), num_nodes, _dptr(d_origins), _dptr(d_dirs), n,
                              float(t_scale_ratio), ctypes.byref(cfg), _dptr(d_hits), _dptr(d_stats),
                              _stream_ptr(stream)), "svo_trace_rays")
+
+
+# ---- batched views -------------------------------------------------------------
+def batch_cfg(tile_w=8, tile_h=4, block_threads=256, blocks_per_sm=0, top_nodes=0, use_graph=True):
+    c = svo_batch_cfg()
+    c.tile_w, c.tile_h, c.block_threads = tile_w, tile_h, block_threads
+    c.blocks_per_sm, c.top_nodes, c.use_graph = blocks_per_sm, top_nodes, int(bool(use_graph))
+    return c
+
+
+def octree_desc(d_nodes, d_attribs, num_nodes, traversal=TRAVERSAL_TREELET, stack_size=13):
+    o = svo_octree_desc()
+    o.d_nodes, o.d_attribs, o.num_nodes = _dptr(d_nodes), _dptr(d_attribs), num_nodes
+    o.traversal, o.stack_size = traversal, stack_size
+    return o
+
+
+def octree_of(mm: "TreeletMemoryManagerCuda", stack_size=13) -> svo_octree_desc:
+    n, a, c = mm.getDeviceIncoreBuffer()
+    return octree_desc(n, a, c, TRAVERSAL_TREELET, stack_size)
+
+
+def view_desc(params: svo_frame_params, octree: int, d_rgba, d_hits=None) -> svo_view_desc:
+    v = svo_view_desc()
+    v.params = params
+    v.octree = octree
+    v.d_rgba = _dptr(d_rgba)
+    v.d_hits = _dptr(d_hits)
+    return v
+
+
+class Batcher:
+    """A ragged table of views over resident octrees, cast in one persistent
+    launch (svo_batcher_* in the C ABI)."""
+
+    def __init__(self, max_views=1024, max_octrees=64):
+        h = ctypes.c_void_p()
+        _check(_L.svo_batcher_create(max_views, max_octrees, ctypes.byref(h)), "svo_batcher_create")
+        self._h = h
+
+    def set(self, octrees, views, cfg: svo_batch_cfg | None = None, stream=None):
+        cfg = cfg or batch_cfg()
+        oa = (svo_octree_desc * len(octrees))(*octrees)
+        va = (svo_view_desc * len(views))(*views)
+        _check(_L.svo_batcher_set(self._h, oa, len(octrees), va, len(views), ctypes.byref(cfg),
+                                  _stream_ptr(stream)), "svo_batcher_set")
+
+    def launch(self, d_stats=None, stream=None):
+        _check(_L.svo_batcher_launch(self._h, _dptr(d_stats), _stream_ptr(stream)), "svo_batcher_launch")
+
+    def autotune(self, reps=5, stream=None):
+        best = svo_batch_cfg()
+        ms = _f32()
+        _check(_L.svo_batcher_autotune(self._h, reps, _stream_ptr(stream), ctypes.byref(best),
+                                       ctypes.byref(ms)), "svo_batcher_autotune")
+        return best, ms.value
+
+    def size(self):
+        t, r = _u64(), _u64()
+        _check(_L.svo_batcher_size(self._h, ctypes.byref(t), ctypes.byref(r)), "svo_batcher_size")
+        return t.value, r.value
+
+    def close(self):
+        if self._h and self._h.value:
+            _L.svo_batcher_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,148 @@
+// batch.cu -- many views of uneven size over one or several resident octrees
+// in one persistent launch.
+//
+// The reference renders one frame per kernel enqueue
+// (raycast_serialized_opencl.cpp:729-747).  Here the launch unit is a ragged
+// table of views: every view is cut into tiles of 32 pixels (tile_w x
+// tile_h), the tiles of all views are numbered one after another, and a
+// persistent grid of warps pulls tile numbers from a global counter until
+// the table is exhausted.  A warp finds its view by binary search over the
+// views' first tile numbers, casts its 32 rays with the same traversal as the
+// per-frame kernel, and writes RGBA8 (and optional hit records) into that
+// view's output.  Blocks may stage the top records of octree 0 in shared
+// memory.  Everything the launch reads lives in device descriptor tables, so
+// the counter reset plus the launch are captured once as a CUDA graph and
+// replayed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+
+#include "batch.h"
+#include "errors.h"
+#include "shade.cuh"
+#include "traverse.cuh"
+
+namespace svo {
+
+namespace {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+template <int TW>
+__device__ __forceinline__ void trace_tile_pixel(const BatchView& v, const BatchOctree& oct,
+                                                 uint32_t x, uint32_t y, const uint2* top,
+                                                 uint32_t top_count, uint2* stack, int stride,
+                                                 svo_stats* stats) {
+  float o[3], dx, dy, dz;
+  pixel_ray(v.params, x, y, o, dx, dy, dz);
+  RayHit h;
+  if (oct.traversal == SVO_TRAVERSAL_FLAT)
+    h = cast_ray<true>(GlobalFetch{oct.nodes}, oct.num_nodes, o, dx, dy, dz,
+                       v.params.t_scale_ratio, oct.stack_size, stack, stride);
+  else if (top_count)
+    h = cast_ray<false>(StagedFetch{oct.nodes, top, top_count}, oct.num_nodes, o, dx, dy, dz,
+                        v.params.t_scale_ratio, oct.stack_size, stack, stride);
+  else
+    h = cast_ray<false>(GlobalFetch{oct.nodes}, oct.num_nodes, o, dx, dy, dz,
+                        v.params.t_scale_ratio, oct.stack_size, stack, stride);
+  const uint64_t pix = (uint64_t)y * v.params.width + x;
+  v.rgba[pix] = shade(v.params.mode, h, oct.attribs, oct.num_nodes, oct.stack_size);
+  if (v.hits != nullptr) store_hit(v.hits, pix, h);
+  count_stats(stats, h);
+}
+
+template <int TW, int TH>
+__global__ void batch_kernel(const BatchView* __restrict__ views, uint32_t num_views,
+                             const BatchOctree* __restrict__ octrees, uint64_t total_tiles,
+                             unsigned long long* __restrict__ counter, svo_stats* stats, int max_s,
+                             uint32_t top_nodes) {
+  static_assert(TW * TH == 32, "a tile is one warp of rays");
+  extern __shared__ uint2 smem[];
+  uint2* stack = smem + threadIdx.x;
+  const int stride = blockDim.x;
+  uint2* top = smem + (size_t)max_s * blockDim.x;
+  uint32_t top_count = 0;
+  if (top_nodes) {
+    const BatchOctree o0 = octrees[0];
+    top_count = (uint32_t)min((uint64_t)top_nodes, o0.num_nodes);
+    for (uint32_t i = threadIdx.x; i < top_count; i += blockDim.x) top[i] = __ldg(o0.nodes + i);
+    __syncthreads();
+  }
+  const uint32_t lane = threadIdx.x & 31u;
+  for (;;) {
+    unsigned long long tile = 0;
+    if (lane == 0) tile = atomicAdd(counter, 1ull);
+    tile = __shfl_sync(kFull, tile, 0);
+    if (tile >= total_tiles) return;
+    // the view holding this tile: last view whose first tile is <= tile
+    uint32_t lo = 0, hi = num_views - 1;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (views[mid].tile_begin <= tile)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const BatchView& v = views[lo];
+    const uint64_t local = tile - v.tile_begin;
+    const uint32_t ty = (uint32_t)(local / v.tiles_x), tx = (uint32_t)(local % v.tiles_x);
+    const uint32_t x = tx * TW + lane % TW, y = ty * TH + lane / TW;
+    if (x < v.params.width && y < v.params.height) {
+      const BatchOctree& oct = octrees[v.octree];
+      trace_tile_pixel<TW>(v, oct, x, y, top, v.octree == 0 ? top_count : 0u, stack, stride, stats);
+    }
+    __syncwarp();
+  }
+}
+
+typedef void (*BatchKernelFn)(const BatchView*, uint32_t, const BatchOctree*, uint64_t,
+                              unsigned long long*, svo_stats*, int, uint32_t);
+
+BatchKernelFn kernel_for(uint32_t tw, uint32_t th) {
+  if (tw == 8 && th == 4) return batch_kernel<8, 4>;
+  if (tw == 16 && th == 2) return batch_kernel<16, 2>;
+  if (tw == 4 && th == 8) return batch_kernel<4, 8>;
+  if (tw == 32 && th == 1) return batch_kernel<32, 1>;
+  return nullptr;
+}
+
+}  // namespace
+
+bool batch_tile_supported(uint32_t tw, uint32_t th) { return kernel_for(tw, th) != nullptr; }
+
+size_t batch_smem_bytes(int max_s, uint32_t threads, uint32_t top_nodes) {
+  return ((size_t)max_s * threads + top_nodes) * sizeof(uint2);
+}
+
+int launch_batch(const BatchLaunch& L, cudaStream_t stream) {
+  BatchKernelFn fn = kernel_for(L.tile_w, L.tile_h);
+  if (!fn) return SVO_ERR_NOTSUP;
+  const size_t smem = batch_smem_bytes(L.max_s, L.threads, L.top_nodes);
+  if (smem > 48u * 1024u) {
+    SVO_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  }
+  fn<<<L.blocks, L.threads, smem, stream>>>(L.views, L.num_views, L.octrees, L.total_tiles,
+                                             L.counter, L.stats, L.max_s, L.top_nodes);
+  return cuda_status(cudaGetLastError());
+}
+
+int batch_grid(uint32_t tile_w, uint32_t tile_h, int max_s, uint32_t threads, uint32_t top_nodes,
+               uint32_t blocks_per_sm, uint32_t* blocks) {
+  BatchKernelFn fn = kernel_for(tile_w, tile_h);
+  if (!fn) return SVO_ERR_NOTSUP;
+  const size_t smem = batch_smem_bytes(max_s, threads, top_nodes);
+  if (smem > 48u * 1024u) {
+    SVO_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  }
+  int dev = 0, sms = 0, fit = 0;
+  SVO_CUDA_TRY(cudaGetDevice(&dev));
+  SVO_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  SVO_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, fn, (int)threads, smem));
+  if (fit <= 0) return SVO_ERR_RANGE;
+  const uint32_t per_sm = blocks_per_sm ? std::min<uint32_t>(blocks_per_sm, (uint32_t)fit) : (uint32_t)fit;
+  *blocks = per_sm * (uint32_t)sms;
+  return SVO_OK;
+}
+
+}  // namespace svo

@@ -83,6 +83,22 @@ __device__ __forceinline__ bool root_slab(const float o[3], const float d[3], fl
   return true;
 }
 
+// Node-record fetch policies.  GlobalFetch reads through the read-only
+// cache; StagedFetch serves the first `count` records (the top levels of a
+// breadth-first treelet pool) from a shared-memory copy.
+struct GlobalFetch {
+  const uint2* __restrict__ nodes;
+  __device__ __forceinline__ uint2 operator()(uint32_t i) const { return __ldg(nodes + i); }
+};
+struct StagedFetch {
+  const uint2* __restrict__ nodes;
+  const uint2* top;
+  uint32_t count;
+  __device__ __forceinline__ uint2 operator()(uint32_t i) const {
+    return i < count ? top[i] : __ldg(nodes + i);
+  }
+};
+
 // The descent loop.  kFlat selects the CpuRaycasterSingleRay3 rules; S is
 // the stack size (treelet) or the octree depth (flat).  `stack` points at
 // this thread's column of the shared-memory stack, `stride` words apart.
@@ -102,8 +118,8 @@ __device__ __forceinline__ bool root_slab(const float o[3], const float d[3], fl
 // pipe instead of the compare/select pipe.  Rays with an infinite or NaN
 // reciprocal (a direction component of exactly zero) take kSigned = false,
 // the literal compare and swap.
-template <bool kFlat, bool kSigned>
-__device__ __forceinline__ void descend(const uint2* __restrict__ nodes, uint64_t num_nodes,
+template <bool kFlat, bool kSigned, class Fetch>
+__device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
                                         const float o[3], float dx, float dy, float dz, float rx,
                                         float px, float ry, float py, float rz, float pz,
                                         float t_min, float t_max, float tsr, int S, uint2* stack,
@@ -121,7 +137,7 @@ __device__ __forceinline__ void descend(const uint2* __restrict__ nodes, uint64_
   float cx = 0.0f, cy = 0.0f, cz = 0.0f;
   float sx2 = 0.5f, half = 0.25f;
   bool in_pool = num_nodes > 0u;
-  uint2 nd = in_pool ? __ldg(nodes) : make_uint2(0u, 0u);
+  uint2 nd = in_pool ? fetch(0u) : make_uint2(0u, 0u);
   uint32_t loops = 0u, fetches = 0u;
 
   while (scale < S) {
@@ -151,7 +167,7 @@ __device__ __forceinline__ void descend(const uint2* __restrict__ nodes, uint64_
         node = e.x;
         tmax = __uint_as_float(e.y);
         in_pool = (uint64_t)node < num_nodes;
-        if (in_pool) nd = __ldg(nodes + node);
+        if (in_pool) nd = fetch(node);
         ix >>= 1;
         iy >>= 1;
         iz >>= 1;
@@ -245,7 +261,7 @@ __device__ __forceinline__ void descend(const uint2* __restrict__ nodes, uint64_
       --scale;
       node = child;
       in_pool = (uint64_t)node < num_nodes;
-      if (in_pool) nd = __ldg(nodes + node);
+      if (in_pool) nd = fetch(node);
       tmin = tc_min;
       tmax = tc_max;
       ix = (ix << 1) | bx;
@@ -269,8 +285,8 @@ __device__ __forceinline__ void descend(const uint2* __restrict__ nodes, uint64_
 }
 
 // One ray: root box test, direction clamp, then the descent.
-template <bool kFlat>
-__device__ __forceinline__ RayHit cast_ray(const uint2* __restrict__ nodes, uint64_t num_nodes,
+template <bool kFlat, class Fetch>
+__device__ __forceinline__ RayHit cast_ray(const Fetch& fetch, uint64_t num_nodes,
                                            const float o[3], float dx, float dy, float dz,
                                            float tsr, int S, uint2* stack, int stride) {
   RayHit h;
@@ -307,10 +323,10 @@ __device__ __forceinline__ RayHit cast_ray(const uint2* __restrict__ nodes, uint
   const float ry = __frcp_rn(dy), py = __fmul_rn(-o[1], ry);
   const float rz = __frcp_rn(dz), pz = __fmul_rn(-o[2], rz);
   if (isfinite(rx) && isfinite(ry) && isfinite(rz))
-    descend<kFlat, true>(nodes, num_nodes, o, dx, dy, dz, rx, px, ry, py, rz, pz, t_min, t_max,
+    descend<kFlat, true>(fetch, num_nodes, o, dx, dy, dz, rx, px, ry, py, rz, pz, t_min, t_max,
                          tsr, S, stack, stride, h);
   else
-    descend<kFlat, false>(nodes, num_nodes, o, dx, dy, dz, rx, px, ry, py, rz, pz, t_min, t_max,
+    descend<kFlat, false>(fetch, num_nodes, o, dx, dy, dz, rx, px, ry, py, rz, pz, t_min, t_max,
                           tsr, S, stack, stride, h);
   return h;
 }

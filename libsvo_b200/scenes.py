@@ -14,6 +14,12 @@ configurations name:
                    2.5.  The configuration names no field of view; 25 degrees
                    (vertical) makes the sphere fill the frame height, so most
                    rays enter the octree.
+* ``terrain``   -- 1024 x 1024 height-field grid (2,093,058 triangles), heights
+                   from 6-octave fBm in [-0.45, -0.15] (0.3 of the extent),
+                   depth-12 octree cut into 6-level treelets; 64 square views
+                   with sides drawn log-uniformly from 256 to 2048 pixels,
+                   eyes above the terrain looking at seeded points on it,
+                   60 degree fov.
 """
 from __future__ import annotations
 
@@ -63,3 +69,21 @@ def icosphere(subdivisions=6, depth=11, treelet_levels=6, seed=1, width=1920, he
                     description=f"icosphere {subdivisions}x subdivided ({t.shape[0]} triangles), 3-octave "
                                 f"noise 0.05, depth {depth}, {treelet_levels}-level treelets, {width}x{height}, "
                                 f"orbit radius {radius}, fov {fov_deg}")
+
+
+def terrain(grid=1024, depth=12, treelet_levels=6, seed=1, views=64, min_side=256, max_side=2048,
+            fov_deg=60.0) -> Workload:
+    v, t = terrain_mesh(grid, octaves=6, base=-0.45, height=0.3, frequency=2.0, seed=seed)
+    scene = Scene.from_mesh(v, t, depth, treelet_levels=treelet_levels)
+    rng = np.random.default_rng(seed + 1000)
+    cams = []
+    for _ in range(views):
+        side = int(round(math.exp(rng.uniform(math.log(min_side), math.log(max_side)))))
+        eye = (rng.uniform(-0.45, 0.45), rng.uniform(-0.05, 0.35), rng.uniform(-0.45, 0.45))
+        target = (rng.uniform(-0.35, 0.35), -0.3, rng.uniform(-0.35, 0.35))
+        up = (0.0, 1.0, 0.0)
+        cams.append(Camera(eye, target, side, side, fov_deg, up))
+    return Workload(f"terrain_g{grid}_d{depth}_{views}views", scene, cams,
+                    description=f"terrain {grid}x{grid} grid ({t.shape[0]} triangles), 6-octave fBm, "
+                                f"depth {depth}, {treelet_levels}-level treelets, {views} views "
+                                f"{min_side}^2..{max_side}^2 log-uniform, fov {fov_deg}")
