@@ -335,6 +335,23 @@ int svo_batcher_autotune(svo_batcher* b, uint32_t reps, void* stream, svo_batch_
 /* Total tiles and rays of the current batch. */
 int svo_batcher_size(svo_batcher* b, uint64_t* tiles, uint64_t* rays);
 
+/* The batched cast for callers that may not allocate device memory (no
+ * counterpart in the reference).  A host that owns and budgets all of HBM
+ * through its own allocator, or a latency-critical loop where cudaMalloc /
+ * cudaFree could synchronise the device, passes its octree pools and output
+ * buffers and nothing is allocated: the descriptor tables and the tile
+ * counter live in a fixed 29,440-byte device array inside the library, held
+ * by every GPU that loads it until the process exits.  At most 256 views and
+ * 16 octrees per call (SVO_ERR_RANGE otherwise); tile 8x4, 16x2, 4x8 or 32x1;
+ * 256-thread persistent blocks.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) with that device current;
+ * make that first call before any stream capture.  All calls share the one
+ * array, which keeps the last call's contents; each call rewrites it and
+ * zeroes its counter, and calls whose work overlaps on the GPU race. */
+int svo_render_batch_static(const svo_octree_desc* octrees, uint32_t num_octrees,
+                            const svo_view_desc* views, uint32_t num_views, uint32_t tile_w,
+                            uint32_t tile_h, svo_stats* d_stats, void* stream);
+
 /* ---- misc -------------------------------------------------------------- */
 const char* svo_version(void);
 /* Last CUDA error string seen by the library on this thread ("" if none). */

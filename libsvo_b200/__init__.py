@@ -172,6 +172,8 @@ _SIGS = {
     "svo_batcher_launch": ([_vp, _vp, _vp], ctypes.c_int),
     "svo_batcher_autotune": ([_vp, _u32, _vp, _P(svo_batch_cfg), _P(_f32)], ctypes.c_int),
     "svo_batcher_size": ([_vp, _P(_u64), _P(_u64)], ctypes.c_int),
+    "svo_render_batch_static": ([_P(svo_octree_desc), _u32, _P(svo_view_desc), _u32, _u32, _u32, _vp, _vp],
+                                ctypes.c_int),
 }
 for _name, (_args, _res) in _SIGS.items():
     _fn = getattr(_L, _name)
@@ -612,3 +614,14 @@ class Batcher:
             self.close()
         except Exception:
             pass
+
+
+def render_batch_static(octrees, views, tile=(8, 4), d_stats=None, stream=None):
+    """The batched cast without allocation (svo_render_batch_static): for
+    callers whose host owns all device memory or must not stall on
+    cudaMalloc.  At most 256 views and 16 octrees; calls that overlap on the
+    GPU share one scratch array and race."""
+    oa = (svo_octree_desc * len(octrees))(*octrees)
+    va = (svo_view_desc * len(views))(*views)
+    _check(_L.svo_render_batch_static(oa, len(octrees), va, len(views), tile[0], tile[1],
+                                      _dptr(d_stats), _stream_ptr(stream)), "svo_render_batch_static")
