@@ -11,14 +11,15 @@ from __future__ import annotations
 
 import ctypes
 import math
-import struct
+import os
 from dataclasses import dataclass
 from pathlib import Path
 
 import numpy as np
 
 _PKG = Path(__file__).resolve().parent
-LIB_PATH = _PKG / "_lib" / "libsvo_b200.so"
+# LIBSVO_B200_LIB selects another build of the same library (same C ABI)
+LIB_PATH = Path(os.environ.get("LIBSVO_B200_LIB", str(_PKG / "_lib" / "libsvo_b200.so")))
 
 if not LIB_PATH.is_file():
     raise ImportError(

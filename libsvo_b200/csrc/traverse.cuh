@@ -19,8 +19,9 @@
 //     push it was set to the pushed child's tcMax, which is the child frame's
 //     tMax and never changes afterwards; so on a pop tMin := popped tMax;
 //   - node centres are exact dyadic numbers (-0.5 + (2i+1) 2^-(k+1) for a
-//     depth-k node with lattice coordinate i), so they are rebuilt exactly
-//     from integer coordinates instead of being stored.
+//     depth-k node with lattice coordinate i): a child's centre is its
+//     parent's +- half the child size, so a pop recovers the parent's centre
+//     exactly from the child's and the low bit of the lattice coordinate.
 // The stack lives in shared memory, one 8-byte word per level per thread,
 // laid out [level][thread] so a warp's accesses are contiguous.
 #pragma once
@@ -168,13 +169,13 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
         tmax = __uint_as_float(e.y);
         in_pool = (uint64_t)node < num_nodes;
         if (in_pool) nd = fetch(node);
+        // parent centre = child centre -+ the child's sx2 (exact)
+        cx = __fadd_rn(cx, (ix & 1u) ? -sx2 : sx2);
+        cy = __fadd_rn(cy, (iy & 1u) ? -sx2 : sx2);
+        cz = __fadd_rn(cz, (iz & 1u) ? -sx2 : sx2);
         ix >>= 1;
         iy >>= 1;
         iz >>= 1;
-        const int k = S - 1 - scale;
-        cx = cell_center(ix, k);
-        cy = cell_center(iy, k);
-        cz = cell_center(iz, k);
         sx2 = __fmul_rn(sx2, 2.0f);
         half = __fmul_rn(sx2, 0.5f);
       }
