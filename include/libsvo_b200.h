@@ -352,6 +352,76 @@ int svo_render_batch_static(const svo_octree_desc* octrees, uint32_t num_octrees
                             const svo_view_desc* views, uint32_t num_views, uint32_t tile_w,
                             uint32_t tile_h, svo_stats* d_stats, void* stream);
 
+/* ---- serving: a request loop over resident octrees --------------------- */
+
+/* The reference pages treelets for one octree per frame and renders one
+ * frame per kernel (TreeletMemoryManager::updateClientSideIncoreBuffer,
+ * src/TreeletMemoryManager.cpp:393-548; raycast_serialized_opencl.cpp:
+ * 680-747).  A server accepts cast requests at any time from any thread:
+ * a dispatcher thread admits them against an HBM budget (octree pools) and
+ * an in-flight ray budget, pages the treelets of their octrees into one
+ * pre-allocated device pool through pinned asynchronous copies on a side
+ * stream (evicting the least recently used idle octree when full), and
+ * launches everything admitted as one batch on the next free stream, so work
+ * that arrives while other batches run overlaps with them on the device. */
+#define SVO_SERVE_BATCHED 0 /* batched launches on `streams` streams       */
+#define SVO_SERVE_PLAIN 1   /* one per-frame kernel per request, one stream */
+
+typedef struct svo_server_cfg {
+  uint64_t hbm_budget_bytes;  /* device pool for octree node+attribute pools */
+  uint64_t max_inflight_rays; /* admission: rays launched, not yet finished  */
+  uint32_t streams;           /* concurrent launches, 1..16                  */
+  uint32_t max_batch_views;   /* requests per batched launch                 */
+  uint32_t mode;              /* SVO_SERVE_*                                 */
+  uint32_t tile_w, tile_h;    /* batch tile shape (0 = 8x4)                   */
+  uint32_t block_threads;     /* batch block size (0 = 256)                  */
+} svo_server_cfg;
+
+typedef struct svo_request {
+  uint32_t octree; /* id from svo_server_add_octree                       */
+  uint32_t reserved;
+  svo_frame_params params;
+  uint32_t* d_rgba; /* width*height RGBA8 output, device, owned by caller */
+} svo_request;
+
+typedef struct svo_request_result {
+  int32_t status;  /* SVO_OK, SVO_ERR_CANCELED, or the error that ended it */
+  uint32_t batch;  /* launch sequence number                               */
+  double submit_s; /* server clock, seconds since svo_server_create        */
+  double launch_s;
+  double done_s;   /* stamped by a callback when the launch finished       */
+} svo_request_result;
+
+typedef struct svo_server_stats {
+  uint64_t requests_done, rays_done, batches;
+  uint64_t octree_loads, octree_evictions, treelets_paged_in, bytes_uploaded;
+  uint64_t resident_bytes;
+  uint32_t resident_octrees, reserved;
+} svo_server_stats;
+
+typedef struct svo_server svo_server;
+/* Allocates the device pool (hbm_budget_bytes) and starts the dispatcher. */
+int svo_server_create(const svo_server_cfg* cfg, svo_server** out);
+/* Cancels requests not yet launched, waits for running ones, frees all. */
+void svo_server_destroy(svo_server* s);
+/* Registers an octree (copied) with the given stack size; not resident
+ * until a request needs it. */
+int svo_server_add_octree(svo_server* s, const svo_scene* scene, int32_t stack_size, uint32_t* id);
+int svo_server_submit(svo_server* s, const svo_request* req, uint64_t* ticket);
+/* Bounded wait: SVO_ERR_TIMEOUT after timeout_ms. */
+int svo_server_wait(svo_server* s, uint64_t ticket, uint32_t timeout_ms, svo_request_result* out);
+/* SVO_ERR_BUSY while the request is pending or running. */
+int svo_server_poll(svo_server* s, uint64_t ticket, svo_request_result* out);
+/* Cancels a request not yet launched (SVO_ERR_BUSY if it is running). */
+int svo_server_cancel(svo_server* s, uint64_t ticket);
+/* Forgets a finished request's record. */
+int svo_server_release(svo_server* s, uint64_t ticket);
+int svo_server_stats_get(svo_server* s, svo_server_stats* out);
+/* Load generator: submits reqs[i] at arrival_s[i] seconds after the call,
+ * then waits (each wait bounded by timeout_ms) and fills results[i]. */
+int svo_server_replay(svo_server* s, const svo_request* reqs, const double* arrival_s, uint32_t n,
+                      uint32_t timeout_ms, svo_request_result* results);
+
 /* ---- misc -------------------------------------------------------------- */
 const char* svo_version(void);
 /* Last CUDA error string seen by the library on this thread ("" if none). */

@@ -626,3 +626,161 @@ def render_batch_static(octrees, views, tile=(8, 4), d_stats=None, stream=None):
     va = (svo_view_desc * len(views))(*views)
     _check(_L.svo_render_batch_static(oa, len(octrees), va, len(views), tile[0], tile[1],
                                       _dptr(d_stats), _stream_ptr(stream)), "svo_render_batch_static")
+
+
+# ---- serving -------------------------------------------------------------------
+SERVE_BATCHED = 0
+SERVE_PLAIN = 1
+
+
+class svo_server_cfg(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_uint64), ("max_inflight_rays", ctypes.c_uint64),
+                ("streams", ctypes.c_uint32), ("max_batch_views", ctypes.c_uint32),
+                ("mode", ctypes.c_uint32), ("tile_w", ctypes.c_uint32), ("tile_h", ctypes.c_uint32),
+                ("block_threads", ctypes.c_uint32)]
+
+
+class svo_request(ctypes.Structure):
+    _fields_ = [("octree", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("params", svo_frame_params), ("d_rgba", ctypes.c_void_p)]
+
+
+class svo_request_result(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("batch", ctypes.c_uint32), ("submit_s", ctypes.c_double),
+                ("launch_s", ctypes.c_double), ("done_s", ctypes.c_double)]
+
+
+class svo_server_stats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in ("requests_done", "rays_done", "batches", "octree_loads",
+                                                "octree_evictions", "treelets_paged_in",
+                                                "bytes_uploaded", "resident_bytes")] + \
+               [("resident_octrees", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+for _name, (_args, _res) in {
+    "svo_server_create": ([_P(svo_server_cfg), _P(_vp)], ctypes.c_int),
+    "svo_server_destroy": ([_vp], None),
+    "svo_server_add_octree": ([_vp, _vp, _i32, _P(_u32)], ctypes.c_int),
+    "svo_server_submit": ([_vp, _P(svo_request), _P(_u64)], ctypes.c_int),
+    "svo_server_wait": ([_vp, _u64, _u32, _P(svo_request_result)], ctypes.c_int),
+    "svo_server_poll": ([_vp, _u64, _P(svo_request_result)], ctypes.c_int),
+    "svo_server_cancel": ([_vp, _u64], ctypes.c_int),
+    "svo_server_release": ([_vp, _u64], ctypes.c_int),
+    "svo_server_stats_get": ([_vp, _P(svo_server_stats)], ctypes.c_int),
+    "svo_server_replay": ([_vp, _P(svo_request), _P(ctypes.c_double), _u32, _u32, _P(svo_request_result)],
+                          ctypes.c_int),
+}.items():
+    _fn = getattr(_L, _name)
+    _fn.argtypes = _args
+    _fn.restype = _res
+
+
+def server_cfg(hbm_budget_bytes, max_inflight_rays=64 << 20, streams=4, max_batch_views=256,
+               mode=SERVE_BATCHED, tile=(8, 4), block_threads=256) -> svo_server_cfg:
+    c = svo_server_cfg()
+    c.hbm_budget_bytes, c.max_inflight_rays = int(hbm_budget_bytes), int(max_inflight_rays)
+    c.streams, c.max_batch_views, c.mode = streams, max_batch_views, mode
+    c.tile_w, c.tile_h, c.block_threads = tile[0], tile[1], block_threads
+    return c
+
+
+def request(octree: int, params: svo_frame_params, d_rgba) -> svo_request:
+    r = svo_request()
+    r.octree, r.params, r.d_rgba = octree, params, _dptr(d_rgba)
+    return r
+
+
+class Server:
+    """Request loop over resident octrees (svo_server_* in the C ABI)."""
+
+    def __init__(self, cfg: svo_server_cfg):
+        h = ctypes.c_void_p()
+        _check(_L.svo_server_create(ctypes.byref(cfg), ctypes.byref(h)), "svo_server_create")
+        self._h = h
+
+    def add_octree(self, scene: Scene, stack_size=13) -> int:
+        i = _u32()
+        _check(_L.svo_server_add_octree(self._h, scene._h, stack_size, ctypes.byref(i)),
+               "svo_server_add_octree")
+        return i.value
+
+    def submit(self, req: svo_request) -> int:
+        t = _u64()
+        _check(_L.svo_server_submit(self._h, ctypes.byref(req), ctypes.byref(t)), "svo_server_submit")
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms=10000) -> svo_request_result:
+        r = svo_request_result()
+        _check(_L.svo_server_wait(self._h, ticket, timeout_ms, ctypes.byref(r)), "svo_server_wait")
+        return r
+
+    def poll(self, ticket: int):
+        r = svo_request_result()
+        rc = _L.svo_server_poll(self._h, ticket, ctypes.byref(r))
+        return (r if rc == SVO_OK else None), rc
+
+    def cancel(self, ticket: int) -> int:
+        return _L.svo_server_cancel(self._h, ticket)
+
+    def release(self, ticket: int) -> int:
+        return _L.svo_server_release(self._h, ticket)
+
+    def stats(self) -> svo_server_stats:
+        s = svo_server_stats()
+        _check(_L.svo_server_stats_get(self._h, ctypes.byref(s)), "svo_server_stats_get")
+        return s
+
+    def replay(self, reqs, arrival_s, timeout_ms=60000):
+        n = len(reqs)
+        ra = (svo_request * n)(*reqs)
+        ta = (ctypes.c_double * n)(*[float(a) for a in arrival_s])
+        out = (svo_request_result * n)()
+        _check(_L.svo_server_replay(self._h, ra, ta, n, timeout_ms, out), "svo_server_replay")
+        return list(out)
+
+    def close(self):
+        if self._h and self._h.value:
+            _L.svo_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---- teardown ------------------------------------------------------------------
+# Handles still open when the interpreter exits are closed here, before the
+# CUDA runtime linked into the library is torn down: a server's dispatcher
+# thread must not issue CUDA calls after that.
+import atexit as _atexit  # noqa: E402
+import weakref as _weakref  # noqa: E402
+
+_live = _weakref.WeakSet()
+
+
+def _track(obj):
+    _live.add(obj)
+    return obj
+
+
+def _close_all():
+    objs = list(_live)
+    for o in sorted(objs, key=lambda o: 0 if isinstance(o, Server) else 1):
+        try:
+            o.close()
+        except Exception:
+            pass
+
+
+_atexit.register(_close_all)
+
+for _cls in (Scene, TreeletMemoryManagerCuda, Batcher, Server):
+    _orig_init = _cls.__init__
+
+    def _init(self, *a, __orig=_orig_init, **k):
+        __orig(self, *a, **k)
+        _track(self)
+
+    _cls.__init__ = _init

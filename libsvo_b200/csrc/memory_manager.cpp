@@ -227,8 +227,10 @@ std::vector<std::pair<uint32_t, uint32_t>> TreeletMemoryManager::upload_ranges()
 
 TreeletMemoryManagerCuda::~TreeletMemoryManagerCuda() {
   if (copy_stream_) cudaStreamSynchronize(copy_stream_);
-  cudaFree(d_nodes_);
-  cudaFree(d_attribs_);
+  if (owns_device_) {
+    cudaFree(d_nodes_);
+    cudaFree(d_attribs_);
+  }
   cudaFree(d_stats_);
   cudaFree(d_rgba_);
   for (int i = 0; i < 2; ++i) {
@@ -239,15 +241,37 @@ TreeletMemoryManagerCuda::~TreeletMemoryManagerCuda() {
   if (copy_stream_) cudaStreamDestroy(copy_stream_);
 }
 
-int TreeletMemoryManagerCuda::init_device_buffer() {
-  if (d_nodes_) return SVO_OK;
-  const uint64_t n = incore_nodes();
+int TreeletMemoryManagerCuda::init_transfer() {
+  if (copy_stream_) return SVO_OK;
   SVO_CUDA_TRY(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
   SVO_CUDA_TRY(cudaEventCreateWithFlags(&upload_done_, cudaEventDisableTiming));
   for (int i = 0; i < 2; ++i) {
     SVO_CUDA_TRY(cudaEventCreateWithFlags(&stage_evt_[i], cudaEventDisableTiming));
     SVO_CUDA_TRY(cudaMallocHost(&stage_[i], kStageBytes));
   }
+  SVO_CUDA_TRY(cudaMalloc(&d_stats_, sizeof(svo_stats)));
+  SVO_CUDA_TRY(cudaMemsetAsync(d_stats_, 0, sizeof(svo_stats), copy_stream_));
+  return SVO_OK;
+}
+
+// whole-buffer upload, as clCreateBuffer(COPY_HOST_PTR) does
+// (TreeletMemoryManagerCl.cpp:106-112)
+int TreeletMemoryManagerCuda::upload_all() {
+  const uint64_t n = incore_nodes();
+  int rc = stage_copy(d_nodes_, incore_, n * sizeof(svo_node));
+  if (rc == SVO_OK) rc = stage_copy(d_attribs_, incore_attr_, n * sizeof(svo_attrib));
+  if (rc != SVO_OK) return rc;
+  SVO_CUDA_TRY(cudaEventRecord(upload_done_, copy_stream_));
+  upload_pending_ = true;
+  upload_.clear();
+  return SVO_OK;
+}
+
+int TreeletMemoryManagerCuda::init_device_buffer() {
+  if (d_nodes_) return SVO_OK;
+  int rc = init_transfer();
+  if (rc != SVO_OK) return rc;
+  const uint64_t n = incore_nodes();
   if (cudaMalloc(&d_nodes_, n * sizeof(svo_node)) != cudaSuccess ||
       cudaMalloc(&d_attribs_, n * sizeof(svo_attrib)) != cudaSuccess) {
     cudaGetLastError();
@@ -257,16 +281,29 @@ int TreeletMemoryManagerCuda::init_device_buffer() {
     d_attribs_ = nullptr;
     return SVO_ERR_NOMEM;
   }
-  SVO_CUDA_TRY(cudaMalloc(&d_stats_, sizeof(svo_stats)));
-  SVO_CUDA_TRY(cudaMemsetAsync(d_stats_, 0, sizeof(svo_stats), copy_stream_));
+  owns_device_ = true;
   device_bytes_ = n * (sizeof(svo_node) + sizeof(svo_attrib));
-  // whole-buffer upload, as clCreateBuffer(COPY_HOST_PTR) does
-  // (TreeletMemoryManagerCl.cpp:106-112)
-  int rc = stage_copy(d_nodes_, incore_, n * sizeof(svo_node));
-  if (rc == SVO_OK) rc = stage_copy(d_attribs_, incore_attr_, n * sizeof(svo_attrib));
+  return upload_all();
+}
+
+int TreeletMemoryManagerCuda::attach_device_buffers(svo_node* d_nodes, svo_attrib* d_attribs) {
+  if (d_nodes_ || !d_nodes || !d_attribs) return SVO_ERR_INVALID;
+  int rc = init_transfer();
   if (rc != SVO_OK) return rc;
-  SVO_CUDA_TRY(cudaEventRecord(upload_done_, copy_stream_));
-  upload_pending_ = true;
+  d_nodes_ = d_nodes;
+  d_attribs_ = d_attribs;
+  owns_device_ = false;
+  device_bytes_ = incore_nodes() * (sizeof(svo_node) + sizeof(svo_attrib));
+  return upload_all();
+}
+
+int TreeletMemoryManagerCuda::detach_device_buffers() {
+  if (!d_nodes_ || owns_device_) return SVO_ERR_INVALID;
+  SVO_CUDA_TRY(cudaStreamSynchronize(copy_stream_));
+  d_nodes_ = nullptr;
+  d_attribs_ = nullptr;
+  device_bytes_ = 0;
+  upload_pending_ = false;
   return SVO_OK;
 }
 

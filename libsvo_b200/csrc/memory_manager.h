@@ -87,6 +87,11 @@ class TreeletMemoryManagerCuda : public TreeletMemoryManager {
   ~TreeletMemoryManagerCuda() override;
 
   int init_device_buffer();                         // initClBuffer
+  // Uses caller-owned device buffers of incore_nodes() records each instead
+  // of allocating, and uploads the whole incore buffer into them.
+  int attach_device_buffers(svo_node* d_nodes, svo_attrib* d_attribs);
+  // Forgets attached buffers (after waiting for uploads into them).
+  int detach_device_buffers();
   int update_device_memory(uint32_t* copy_calls);   // updateDeviceMemory
   int reset_incore_buffer() override;
 
@@ -104,6 +109,8 @@ class TreeletMemoryManagerCuda : public TreeletMemoryManager {
 
  private:
   int stage_copy(void* dst, const void* src, uint64_t bytes);
+  int init_transfer();
+  int upload_all();
 
   cudaStream_t render_stream_ = nullptr;
   cudaStream_t copy_stream_ = nullptr;
@@ -111,6 +118,7 @@ class TreeletMemoryManagerCuda : public TreeletMemoryManager {
   bool upload_pending_ = false;
   svo_node* d_nodes_ = nullptr;
   svo_attrib* d_attribs_ = nullptr;
+  bool owns_device_ = false;
   svo_stats* d_stats_ = nullptr;
   uint64_t device_bytes_ = 0;
   static constexpr uint64_t kStageBytes = 32ull << 20;  // per half of the ring

@@ -1,0 +1,604 @@
+// server.cpp -- request loop over resident octrees (svo_server_* in the C ABI).
+//
+// The reference pages treelets of one octree per frame, driven by its
+// analysis pass, and renders one frame per kernel (src/TreeletMemoryManager.cpp:
+// 393-548, raycast_serialized_opencl.cpp:680-747).  The server turns that
+// into a request loop: clients submit cast requests (an octree and a camera)
+// at any time; a dispatcher thread admits them against an HBM budget and an
+// in-flight ray budget, pages the treelets of their octrees into one
+// pre-allocated device pool (the octree's TreeletMemoryManagerCuda uploads
+// its slots through its pinned staging ring on its side stream, and the
+// launch waits on the upload event), and launches every admitted request
+// together as one batch on the next free stream.  Requests that arrive while
+// batches run are launched in further batches on other streams, so their
+// work overlaps on the device (continuous batching).  Octrees no batch uses
+// are evicted least recently used first when the pool is full.  A host
+// callback on each batch's stream timestamps completion.
+//
+// In SVO_SERVE_PLAIN mode the same loop launches the per-frame kernel once
+// per request on a single stream instead: the plain baseline.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/libsvo_b200.h"
+#include "errors.h"
+#include "memory_manager.h"
+#include "render.h"
+#include "scene.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+// First-fit allocator over one device allocation; offsets aligned to 256 B.
+class DevicePool {
+ public:
+  int init(uint64_t bytes) {
+    size_ = bytes & ~255ull;
+    if (size_ == 0) return SVO_ERR_RANGE;
+    SVO_CUDA_TRY(cudaMalloc(&base_, size_));
+    free_.clear();
+    free_[0] = size_;
+    return SVO_OK;
+  }
+  ~DevicePool() { cudaFree(base_); }
+  bool alloc(uint64_t bytes, uint64_t* off) {
+    bytes = (bytes + 255) & ~255ull;
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second < bytes) continue;
+      *off = it->first;
+      const uint64_t rest = it->second - bytes, start = it->first + bytes;
+      free_.erase(it);
+      if (rest) free_[start] = rest;
+      return true;
+    }
+    return false;
+  }
+  void release(uint64_t off, uint64_t bytes) {
+    bytes = (bytes + 255) & ~255ull;
+    auto it = free_.emplace(off, bytes).first;
+    auto next = std::next(it);
+    if (next != free_.end() && it->first + it->second == next->first) {
+      it->second += next->second;
+      free_.erase(next);
+    }
+    if (it != free_.begin()) {
+      auto prev = std::prev(it);
+      if (prev->first + prev->second == it->first) {
+        prev->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+  char* base() const { return static_cast<char*>(base_); }
+  uint64_t size() const { return size_; }
+
+ private:
+  void* base_ = nullptr;
+  uint64_t size_ = 0;
+  std::map<uint64_t, uint64_t> free_;
+};
+
+struct ServedOctree {
+  std::unique_ptr<svo::TreeletMemoryManagerCuda> mm;
+  int32_t stack_size = 13;
+  uint64_t node_bytes = 0;  // per pool (nodes, then attributes)
+  bool resident = false;
+  uint64_t pool_off = 0;
+  uint32_t refs = 0;  // batches in flight that read it
+  uint64_t last_use = 0;
+};
+
+struct Request {
+  svo_request r{};
+  svo_request_result res{};
+  bool done = false;
+};
+
+struct Launch;
+
+}  // namespace
+
+struct svo_server {
+  svo_server_cfg cfg{};
+  Clock::time_point t0;
+  DevicePool pool;
+  std::vector<ServedOctree> octrees;
+
+  std::mutex mu;  // pending, requests, results, octree table
+  std::condition_variable cv_user;
+  std::condition_variable cv_dispatch;
+  std::deque<uint64_t> pending;
+  std::unordered_map<uint64_t, Request> requests;
+  uint64_t next_ticket = 1;
+  bool stop = false;
+  int fatal = SVO_OK;
+
+  struct Slot {
+    cudaStream_t stream = nullptr;
+    svo_batcher* batcher = nullptr;
+    bool busy = false;
+    std::vector<uint64_t> tickets;
+    std::vector<uint32_t> octrees;  // octree ids pinned by this launch
+    uint64_t rays = 0;
+    double done_s = 0.0;            // written by the stream callback
+    svo_server* owner = nullptr;
+    uint32_t index = 0;
+  };
+  std::vector<Slot> slots;
+  std::mutex cmu;  // completion queue (the only lock stream callbacks take)
+  std::deque<uint32_t> completed;
+  std::atomic<uint32_t> completions{0};
+  // Host callbacks launched and callbacks past their last access to this
+  // object; the server is freed only once both agree.
+  std::atomic<uint64_t> callbacks_launched{0};
+  std::atomic<uint64_t> callbacks_exited{0};
+
+  uint64_t inflight_rays = 0;
+  bool blocked = false;  // admission stopped on a limit; cleared by completions
+  uint64_t use_clock = 0;
+  uint32_t batch_seq = 0;
+  svo_server_stats stats{};
+  std::thread dispatcher;
+
+  double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+};
+
+namespace {
+
+void CUDART_CB on_slot_done(void* p) {
+  auto* slot = static_cast<svo_server::Slot*>(p);
+  svo_server* s = slot->owner;
+  slot->done_s = s->now();
+  {
+    std::lock_guard<std::mutex> lk(s->cmu);
+    s->completed.push_back(slot->index);
+    s->completions.fetch_add(1);
+  }
+  s->cv_dispatch.notify_one();
+  s->callbacks_exited.fetch_add(1, std::memory_order_release);  // last access to *s
+}
+
+// Makes octree `id` resident, evicting idle octrees if the pool is full.
+// Called by the dispatcher with `mu` held.
+int ensure_resident(svo_server* s, uint32_t id) {
+  ServedOctree& o = s->octrees[id];
+  o.last_use = ++s->use_clock;
+  if (o.resident) return SVO_OK;
+  const uint64_t need = 2 * ((o.node_bytes + 255) & ~255ull);
+  uint64_t off = 0;
+  while (!s->pool.alloc(need, &off)) {
+    int victim = -1;
+    for (uint32_t i = 0; i < s->octrees.size(); ++i) {
+      const ServedOctree& c = s->octrees[i];
+      if (i == id || !c.resident || c.refs) continue;
+      if (victim < 0 || c.last_use < s->octrees[victim].last_use) victim = (int)i;
+    }
+    if (victim < 0) return need > s->pool.size() ? SVO_ERR_RANGE : SVO_ERR_BUSY;
+    ServedOctree& v = s->octrees[victim];
+    int rc = v.mm->detach_device_buffers();
+    if (rc != SVO_OK) return rc;
+    s->pool.release(v.pool_off, 2 * ((v.node_bytes + 255) & ~255ull));
+    v.resident = false;
+    s->stats.octree_evictions++;
+    s->stats.resident_octrees--;
+    s->stats.resident_bytes -= 2 * v.node_bytes;
+  }
+  char* base = s->pool.base() + off;
+  const uint64_t attr_off = (o.node_bytes + 255) & ~255ull;
+  const int rc = o.mm->attach_device_buffers(reinterpret_cast<svo_node*>(base),
+                                            reinterpret_cast<svo_attrib*>(base + attr_off));
+  if (rc != SVO_OK) {
+    s->pool.release(off, need);
+    return rc;
+  }
+  o.pool_off = off;
+  o.resident = true;
+  s->stats.octree_loads++;
+  s->stats.treelets_paged_in += o.mm->num_treelets();
+  s->stats.bytes_uploaded += 2 * o.node_bytes;
+  s->stats.resident_octrees++;
+  s->stats.resident_bytes += 2 * o.node_bytes;
+  return SVO_OK;
+}
+
+void finish_slot(svo_server* s, svo_server::Slot& slot) {
+  // called with mu held
+  for (uint64_t t : slot.tickets) {
+    auto it = s->requests.find(t);
+    if (it == s->requests.end()) continue;
+    it->second.res.done_s = slot.done_s;
+    it->second.res.status = SVO_OK;
+    it->second.done = true;
+    s->stats.requests_done++;
+  }
+  for (uint32_t id : slot.octrees) s->octrees[id].refs--;
+  s->inflight_rays -= slot.rays;
+  s->stats.rays_done += slot.rays;
+  slot.tickets.clear();
+  slot.octrees.clear();
+  slot.rays = 0;
+  slot.busy = false;
+}
+
+// Launches the requests in `slot.tickets` (octrees already resident and pinned).
+int launch_slot(svo_server* s, svo_server::Slot& slot) {
+  const bool plain = s->cfg.mode == SVO_SERVE_PLAIN;
+  std::vector<svo_octree_desc> descs;
+  std::vector<uint32_t> remap(s->octrees.size(), UINT32_MAX);
+  std::vector<svo_view_desc> views;
+  for (uint32_t id : slot.octrees) {
+    ServedOctree& o = s->octrees[id];
+    int rc = o.mm->wait_uploads(slot.stream);
+    if (rc != SVO_OK) return rc;
+    remap[id] = (uint32_t)descs.size();
+    descs.push_back(svo_octree_desc{o.mm->device_nodes(), o.mm->device_attribs(),
+                                    o.mm->incore_nodes(), SVO_TRAVERSAL_TREELET, o.stack_size});
+  }
+  const double t_launch = s->now();
+  for (uint64_t t : slot.tickets) {
+    Request& q = s->requests[t];
+    q.res.launch_s = t_launch;
+    q.res.batch = s->batch_seq;
+    svo_view_desc v{};
+    v.params = q.r.params;
+    v.octree = remap[q.r.octree];
+    v.d_rgba = q.r.d_rgba;
+    v.d_hits = nullptr;
+    views.push_back(v);
+  }
+  s->batch_seq++;
+  s->stats.batches++;
+  if (plain) {
+    for (const svo_view_desc& v : views) {
+      const svo_octree_desc& d = descs[v.octree];
+      const svo_trace_cfg tc{SVO_TRAVERSAL_TREELET, d.stack_size};
+      const int rc = svo::launch_render(d.d_nodes, d.d_attribs, d.num_nodes, v.params, tc, v.d_rgba,
+                                        nullptr, nullptr, slot.stream);
+      if (rc != SVO_OK) return rc;
+    }
+  } else {
+    const svo_batch_cfg bc{s->cfg.tile_w, s->cfg.tile_h, s->cfg.block_threads, 0, 0, 0};
+    int rc = svo_batcher_set(slot.batcher, descs.data(), (uint32_t)descs.size(), views.data(),
+                             (uint32_t)views.size(), &bc, slot.stream);
+    if (rc != SVO_OK) return rc;
+    rc = svo_batcher_launch(slot.batcher, nullptr, slot.stream);
+    if (rc != SVO_OK) return rc;
+  }
+  SVO_CUDA_TRY(cudaLaunchHostFunc(slot.stream, on_slot_done, &slot));
+  s->callbacks_launched.fetch_add(1);
+  return SVO_OK;
+}
+
+void dispatch_loop(svo_server* s) {
+  std::unique_lock<std::mutex> lk(s->mu);
+  for (;;) {
+    s->cv_dispatch.wait_for(lk, std::chrono::microseconds(200), [&] {
+      if (s->completions.load() > 0) return true;
+      bool busy = false, idle = false;
+      for (auto& sl : s->slots) (sl.busy ? busy : idle) = true;
+      if (s->stop) return !busy;  // stopping: wake for completions or to exit
+      return !s->pending.empty() && !s->blocked && idle;
+    });
+    // completions
+    std::deque<uint32_t> done;
+    {
+      std::lock_guard<std::mutex> ck(s->cmu);
+      done.swap(s->completed);
+      s->completions.fetch_sub((uint32_t)done.size());
+    }
+    if (!done.empty()) {
+      for (uint32_t i : done) finish_slot(s, s->slots[i]);
+      s->blocked = false;
+      s->cv_user.notify_all();
+    }
+    bool busy_any = false;
+    for (auto& sl : s->slots) busy_any |= sl.busy;
+    if (s->stop && s->pending.empty() && !busy_any) return;
+    if (s->fatal != SVO_OK) continue;
+    // admit and launch while a stream is free
+    for (;;) {
+      if (s->pending.empty()) break;
+      svo_server::Slot* slot = nullptr;
+      for (auto& sl : s->slots)
+        if (!sl.busy) {
+          slot = &sl;
+          break;
+        }
+      if (!slot) break;
+      const uint32_t max_views = s->cfg.mode == SVO_SERVE_PLAIN ? 1u : s->cfg.max_batch_views;
+      // Residency-aware admission, in arrival order within each pass:
+      //  1. requests whose octree is resident (no paging needed);
+      //  2. otherwise the oldest request: its octree is paged in (evicting
+      //     idle octrees least recently used first), and pass 1 runs again
+      //     so every pending request for that octree rides on the same load.
+      // A request waiting longer than kMaxWait goes straight to step 2, so
+      // no request starves behind a stream of requests on resident octrees.
+      constexpr double kMaxWait = 0.05;
+      auto admit = [&](std::deque<uint64_t>::iterator it) {
+        const uint64_t t = *it;
+        Request& q = s->requests[t];
+        ServedOctree& o = s->octrees[q.r.octree];
+        if (std::find(slot->octrees.begin(), slot->octrees.end(), q.r.octree) == slot->octrees.end()) {
+          slot->octrees.push_back(q.r.octree);
+          o.refs++;
+        }
+        slot->tickets.push_back(t);
+        slot->rays += (uint64_t)q.r.params.width * q.r.params.height;
+        return s->pending.erase(it);
+      };
+      auto fits = [&](const Request& q) {
+        const uint64_t rays = (uint64_t)q.r.params.width * q.r.params.height;
+        if (slot->tickets.size() >= max_views) return false;
+        if (s->inflight_rays + slot->rays == 0) return true;  // always admit one
+        return s->inflight_rays + slot->rays + rays <= s->cfg.max_inflight_rays;
+      };
+      auto admit_resident = [&] {
+        for (auto it = s->pending.begin(); it != s->pending.end();) {
+          const Request& q = s->requests[*it];
+          if (!fits(q)) break;
+          if (s->octrees[q.r.octree].resident) {
+            s->octrees[q.r.octree].last_use = ++s->use_clock;
+            it = admit(it);
+          } else {
+            ++it;
+          }
+        }
+      };
+      const bool starving =
+          !s->pending.empty() && s->now() - s->requests[s->pending.front()].res.submit_s > kMaxWait;
+      if (!starving) admit_resident();
+      while (slot->tickets.empty() && !s->pending.empty()) {
+        Request& q = s->requests[s->pending.front()];
+        if (!fits(q)) break;
+        const int rc = ensure_resident(s, q.r.octree);
+        if (rc == SVO_ERR_BUSY) break;  // the pool is held by running batches: retry later
+        if (rc != SVO_OK) {  // cannot ever fit, or a CUDA error
+          s->pending.pop_front();
+          q.res.status = rc;
+          q.done = true;
+          s->cv_user.notify_all();
+          continue;
+        }
+        admit(s->pending.begin());
+        admit_resident();
+      }
+      if (slot->tickets.empty()) {
+        s->blocked = !s->pending.empty();  // wait for a completion before retrying
+        break;
+      }
+      slot->busy = true;
+      s->inflight_rays += slot->rays;
+      const int rc = launch_slot(s, *slot);
+      if (rc != SVO_OK) {
+        s->fatal = rc;
+        for (uint64_t t : slot->tickets) {
+          s->requests[t].res.status = rc;
+          s->requests[t].done = true;
+        }
+        for (uint32_t id : slot->octrees) s->octrees[id].refs--;
+        s->inflight_rays -= slot->rays;
+        slot->tickets.clear();
+        slot->octrees.clear();
+        slot->rays = 0;
+        slot->busy = false;
+        s->cv_user.notify_all();
+        break;
+      }
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int svo_server_create(const svo_server_cfg* cfg, svo_server** out) {
+  if (!cfg || !out) return SVO_ERR_INVALID;
+  *out = nullptr;
+  if (cfg->streams == 0 || cfg->streams > 16 || cfg->max_batch_views == 0 ||
+      cfg->max_batch_views > 4096 || cfg->max_inflight_rays == 0)
+    return SVO_ERR_RANGE;
+  if (cfg->mode != SVO_SERVE_BATCHED && cfg->mode != SVO_SERVE_PLAIN) return SVO_ERR_NOTSUP;
+  auto* s = new (std::nothrow) svo_server;
+  if (!s) return SVO_ERR_NOMEM;
+  s->cfg = *cfg;
+  if (s->cfg.tile_w == 0) s->cfg.tile_w = 8, s->cfg.tile_h = 4;
+  if (s->cfg.block_threads == 0) s->cfg.block_threads = 256;
+  s->t0 = Clock::now();
+  int rc = s->pool.init(cfg->hbm_budget_bytes);
+  // Plain mode queues one per-frame kernel per request back to back on a
+  // single stream (its slots share that stream); batched mode gives every
+  // slot its own stream and batcher so batches overlap.
+  s->slots.resize(cfg->streams);
+  for (uint32_t i = 0; i < cfg->streams && rc == SVO_OK; ++i) {
+    auto& sl = s->slots[i];
+    sl.owner = s;
+    sl.index = i;
+    if (cfg->mode == SVO_SERVE_PLAIN && i > 0) {
+      sl.stream = s->slots[0].stream;
+      continue;
+    }
+    rc = svo::cuda_status(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
+    if (rc == SVO_OK && cfg->mode == SVO_SERVE_BATCHED)
+      rc = svo_batcher_create(cfg->max_batch_views, 64, &sl.batcher);
+  }
+  if (rc != SVO_OK) {
+    svo_server_destroy(s);
+    return rc;
+  }
+  s->dispatcher = std::thread(dispatch_loop, s);
+  *out = s;
+  return SVO_OK;
+}
+
+void svo_server_destroy(svo_server* s) {
+  if (!s) return;
+  if (s->dispatcher.joinable()) {
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->stop = true;
+      // requests never launched end as cancelled
+      for (uint64_t t : s->pending) {
+        s->requests[t].res.status = SVO_ERR_CANCELED;
+        s->requests[t].done = true;
+      }
+      s->pending.clear();
+    }
+    s->cv_dispatch.notify_one();
+    s->dispatcher.join();
+  }
+  // plain mode: all slots share slot 0's stream, destroyed once at the end
+  for (auto& sl : s->slots)
+    if (sl.stream) cudaStreamSynchronize(sl.stream);
+  for (uint32_t i = 0; i < s->slots.size(); ++i) {
+    auto& sl = s->slots[i];
+    if (sl.batcher) svo_batcher_destroy(sl.batcher);
+    const bool shared = s->cfg.mode == SVO_SERVE_PLAIN && i > 0;
+    if (sl.stream && !shared) cudaStreamDestroy(sl.stream);
+  }
+  // A callback may still be inside its notify when its completion has been
+  // processed: wait (bounded) until every callback is past its last access.
+  // If one never gets there, the object is leaked rather than freed under it.
+  const auto deadline = Clock::now() + std::chrono::seconds(10);
+  while (s->callbacks_exited.load(std::memory_order_acquire) != s->callbacks_launched.load()) {
+    if (Clock::now() > deadline) return;
+    std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+  delete s;
+}
+
+int svo_server_add_octree(svo_server* s, const svo_scene* scene, int32_t stack_size, uint32_t* id) {
+  if (!s || !scene || !id || scene->treelets.empty()) return SVO_ERR_INVALID;
+  if (stack_size < 2 || stack_size > 24) return SVO_ERR_RANGE;
+  try {
+    ServedOctree o;
+    o.mm.reset(new svo::TreeletMemoryManagerCuda(nullptr));
+    svo_scene copy = *scene;
+    const uint64_t incore = (uint64_t)scene->treelet_bytes * scene->treelets.size();
+    int rc = o.mm->init(std::move(copy), incore);
+    if (rc != SVO_OK) return rc;
+    uint32_t n = 0;
+    rc = o.mm->insert_all(&n);
+    if (rc != SVO_OK) return rc;
+    o.stack_size = stack_size;
+    o.node_bytes = o.mm->incore_nodes() * sizeof(svo_node);
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->octrees.size() >= 64) return SVO_ERR_RANGE;
+    s->octrees.push_back(std::move(o));
+    *id = (uint32_t)s->octrees.size() - 1;
+  } catch (const std::bad_alloc&) {
+    return SVO_ERR_NOMEM;
+  }
+  return SVO_OK;
+}
+
+int svo_server_submit(svo_server* s, const svo_request* req, uint64_t* ticket) {
+  const double submitted = s ? s->now() : 0.0;  // before waiting for the lock
+  if (!s || !req || !ticket || !req->d_rgba) return SVO_ERR_INVALID;
+  const int32_t m = req->params.mode;
+  if (!(m == 0 || m == 1 || m == 3 || m == 4 || m == 5)) return SVO_ERR_NOTSUP;
+  if (req->params.width == 0 || req->params.height == 0) return SVO_ERR_INVALID;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (req->octree >= s->octrees.size() || s->stop) return SVO_ERR_INVALID;
+    const uint64_t t = s->next_ticket++;
+    Request& q = s->requests[t];
+    q.r = *req;
+    q.res.status = SVO_ERR_BUSY;
+    q.res.submit_s = submitted;
+    s->pending.push_back(t);
+    s->blocked = false;
+    *ticket = t;
+  }
+  s->cv_dispatch.notify_one();
+  return SVO_OK;
+}
+
+int svo_server_wait(svo_server* s, uint64_t ticket, uint32_t timeout_ms, svo_request_result* out) {
+  if (!s) return SVO_ERR_INVALID;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->requests.find(ticket);
+  if (it == s->requests.end()) return SVO_ERR_INVALID;
+  const bool ok = s->cv_user.wait_for(lk, std::chrono::milliseconds(timeout_ms),
+                                      [&] { return s->requests[ticket].done; });
+  if (!ok) return SVO_ERR_TIMEOUT;
+  if (out) *out = s->requests[ticket].res;
+  return SVO_OK;
+}
+
+int svo_server_poll(svo_server* s, uint64_t ticket, svo_request_result* out) {
+  const int rc = svo_server_wait(s, ticket, 0, out);
+  return rc == SVO_ERR_TIMEOUT ? SVO_ERR_BUSY : rc;
+}
+
+int svo_server_cancel(svo_server* s, uint64_t ticket) {
+  if (!s) return SVO_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->requests.find(ticket);
+  if (it == s->requests.end()) return SVO_ERR_INVALID;
+  auto p = std::find(s->pending.begin(), s->pending.end(), ticket);
+  if (p == s->pending.end()) return it->second.done ? SVO_OK : SVO_ERR_BUSY;  // running
+  s->pending.erase(p);
+  it->second.res.status = SVO_ERR_CANCELED;
+  it->second.done = true;
+  s->cv_user.notify_all();
+  return SVO_OK;
+}
+
+int svo_server_release(svo_server* s, uint64_t ticket) {
+  if (!s) return SVO_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->requests.find(ticket);
+  if (it == s->requests.end()) return SVO_ERR_INVALID;
+  if (!it->second.done) return SVO_ERR_BUSY;
+  s->requests.erase(it);
+  return SVO_OK;
+}
+
+int svo_server_stats_get(svo_server* s, svo_server_stats* out) {
+  if (!s || !out) return SVO_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(s->mu);
+  *out = s->stats;
+  return SVO_OK;
+}
+
+int svo_server_replay(svo_server* s, const svo_request* reqs, const double* arrival_s, uint32_t n,
+                      uint32_t timeout_ms, svo_request_result* results) {
+  if (!s || (n && (!reqs || !arrival_s || !results))) return SVO_ERR_INVALID;
+  std::vector<uint64_t> tickets(n, 0);
+  const auto start = Clock::now();
+  for (uint32_t i = 0; i < n; ++i) {
+    const auto due = start + std::chrono::duration_cast<Clock::duration>(
+                                 std::chrono::duration<double>(arrival_s[i]));
+    const auto early = due - std::chrono::microseconds(100);
+    if (Clock::now() < early) std::this_thread::sleep_until(early);
+    while (Clock::now() < due) {
+    }
+    const int rc = svo_server_submit(s, &reqs[i], &tickets[i]);
+    if (rc != SVO_OK) return rc;
+  }
+  int first = SVO_OK;
+  for (uint32_t i = 0; i < n; ++i) {
+    const int rc = svo_server_wait(s, tickets[i], timeout_ms, &results[i]);
+    if (rc != SVO_OK) {
+      results[i].status = rc;
+      if (first == SVO_OK) first = rc;
+    } else {
+      svo_server_release(s, tickets[i]);
+    }
+  }
+  return first;
+}
+
+}  // extern "C"

@@ -87,3 +87,60 @@ def terrain(grid=1024, depth=12, treelet_levels=6, seed=1, views=64, min_side=25
                     description=f"terrain {grid}x{grid} grid ({t.shape[0]} triangles), 6-octave fBm, "
                                 f"depth {depth}, {treelet_levels}-level treelets, {views} views "
                                 f"{min_side}^2..{max_side}^2 log-uniform, fov {fov_deg}")
+
+
+@dataclass
+class ServingWorkload:
+    name: str
+    scenes: list          # Scene per octree
+    stack_sizes: list
+    description: str = ""
+
+
+# (kind, size, depth, treelet levels, seed, radius): displaced icospheres and
+# fBm terrains of depths 9..13.  The depth-13 octree is a smaller sphere
+# (radius 0.15) so that its host build stays in seconds.
+SERVING_OCTREES = [
+    ("icosphere", 5, 9, 4, 11, 0.4), ("terrain", 257, 9, 4, 12, None),
+    ("icosphere", 5, 10, 5, 13, 0.4), ("terrain", 513, 10, 5, 14, None),
+    ("icosphere", 6, 11, 6, 15, 0.4), ("terrain", 1024, 11, 6, 16, None),
+    ("icosphere", 6, 12, 6, 17, 0.3), ("icosphere", 6, 13, 6, 18, 0.15),
+]
+
+
+def serving(octrees=SERVING_OCTREES) -> ServingWorkload:
+    scenes = []
+    for kind, size, depth, levels, seed, radius in octrees:
+        if kind == "icosphere":
+            v, t = icosphere_mesh(size, radius=radius, octaves=3, amplitude=0.05 * radius / 0.4,
+                                  frequency=2.0, seed=seed)
+        else:
+            v, t = terrain_mesh(size, octaves=6, base=-0.45, height=0.3, frequency=2.0, seed=seed)
+        scenes.append(Scene.from_mesh(v, t, depth, treelet_levels=levels))
+    depths = [o[2] for o in octrees]
+    return ServingWorkload("serving_8_octrees", scenes, [13] * len(scenes),
+                           description=f"{len(scenes)} octrees (icospheres and terrains, depths "
+                                       f"{min(depths)}..{max(depths)}), requests 64x64..1920x1080 "
+                                       f"log-uniform, Poisson arrivals")
+
+
+def serving_requests(n, num_octrees, seed=0, min_wh=(64, 64), max_wh=(1920, 1080)):
+    """Seeded request mix: (octree, Camera) pairs; each axis of the resolution
+    interpolates log-linearly between 64x64 and 1920x1080 with one uniform
+    draw, cameras on an orbit around the octree."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        o = int(rng.integers(0, num_octrees))
+        u = rng.uniform()
+        w = int(round(min_wh[0] * (max_wh[0] / min_wh[0]) ** u))
+        h = int(round(min_wh[1] * (max_wh[1] / min_wh[1]) ** u))
+        cam = orbit_pose(float(rng.uniform(1.2, 2.5)), float(rng.uniform(0, 360)),
+                         float(rng.uniform(-40, 40)), w, h, fov_deg=float(rng.uniform(25, 60)))
+        out.append((o, cam))
+    return out
+
+
+def poisson_arrivals(n, rate_per_s, seed=0):
+    rng = np.random.default_rng(seed + 7)
+    return np.cumsum(rng.exponential(1.0 / rate_per_s, size=n))

@@ -1,0 +1,132 @@
+"""Serving: requests of uneven size over several octrees under an HBM budget.
+
+Each request's pixels must be the same whether it is rendered alone (the
+per-frame kernel on a fully resident octree) or served in the mix (batched
+with others, while octrees are paged in and evicted), bit for bit."""
+import numpy as np
+import pytest
+
+import libsvo_b200 as L
+from libsvo_b200 import scenes as S
+
+pytestmark = pytest.mark.gpu
+
+SMALL = [("icosphere", 3, 7, 3, 1, 0.4), ("terrain", 65, 7, 3, 2, None),
+         ("icosphere", 4, 8, 4, 3, 0.35), ("terrain", 129, 8, 4, 4, None)]
+
+
+@pytest.fixture(scope="module")
+def workload(cuda):
+    return S.serving(SMALL)
+
+
+def alone(scene, cam, cuda):
+    import torch
+
+    info = scene.info
+    mm = L.TreeletMemoryManagerCuda(scene, info.treelet_bytes * info.num_treelets)
+    mm.insertAll()
+    mm.initDeviceBuffer()
+    p = cam.frame_params()
+    out = torch.empty((p.height, p.width), dtype=torch.int32, device=cuda)
+    mm.render(p, out)
+    torch.cuda.synchronize()
+    mm.close()
+    return out.cpu().numpy()
+
+
+def footprint(scene):
+    i = scene.info
+    return 16 * i.treelet_bytes // 8 * i.num_treelets
+
+
+@pytest.mark.parametrize("mode", [L.SERVE_BATCHED, L.SERVE_PLAIN])
+def test_results_same_alone_and_in_the_mix(workload, cuda, mode):
+    import torch
+
+    reqs = S.serving_requests(40, len(workload.scenes), seed=5, max_wh=(320, 200))
+    # budget for about two of the four octrees: octrees page in and out
+    budget = int(1.1 * (footprint(workload.scenes[2]) + footprint(workload.scenes[3])))
+    srv = L.Server(L.server_cfg(budget, streams=3, max_batch_views=8, mode=mode))
+    ids = [srv.add_octree(s) for s in workload.scenes]
+    outs, rq = [], []
+    for o, cam in reqs:
+        p = cam.frame_params()
+        t = torch.full((p.height, p.width), -1, dtype=torch.int32, device=cuda)
+        outs.append(t)
+        rq.append(L.request(ids[o], p, t))
+    arrivals = S.poisson_arrivals(len(rq), 2000.0, seed=1)
+    res = srv.replay(rq, arrivals, timeout_ms=30000)
+    assert all(r.status == L.SVO_OK for r in res)
+    assert all(r.submit_s <= r.launch_s <= r.done_s for r in res)
+    st = srv.stats()
+    assert st.requests_done == len(rq)
+    # the budget holds about two octrees: some had to be evicted to serve the rest
+    assert st.octree_evictions > 0
+    assert st.octree_loads >= len({o for o, _ in reqs})
+    torch.cuda.synchronize()
+    for (o, cam), t in zip(reqs, outs):
+        assert np.array_equal(t.cpu().numpy(), alone(workload.scenes[o], cam, cuda))
+    srv.close()
+
+
+def test_batches_overlap_and_coalesce(workload, cuda):
+    import torch
+
+    reqs = S.serving_requests(60, len(workload.scenes), seed=9, max_wh=(256, 160))
+    total = sum(footprint(s) for s in workload.scenes)
+    srv = L.Server(L.server_cfg(2 * total, streams=4, max_batch_views=16))
+    ids = [srv.add_octree(s) for s in workload.scenes]
+    outs = [torch.empty((c.height, c.width), dtype=torch.int32, device=cuda) for _, c in reqs]
+    rq = [L.request(ids[o], c.frame_params(), t) for (o, c), t in zip(reqs, outs)]
+    res = srv.replay(rq, np.zeros(len(rq)), timeout_ms=30000)  # all at once
+    assert all(r.status == L.SVO_OK for r in res)
+    batches = {r.batch for r in res}
+    assert len(batches) < len(rq)  # requests were batched together
+    st = srv.stats()
+    assert st.octree_evictions == 0 and st.octree_loads == len(set(o for o, _ in reqs))
+    srv.close()
+
+
+def test_cancel_wait_timeout_and_errors(workload, cuda):
+    import torch
+
+    total = sum(footprint(s) for s in workload.scenes)
+    srv = L.Server(L.server_cfg(total, streams=1, max_batch_views=1, max_inflight_rays=1))
+    oid = srv.add_octree(workload.scenes[0])
+    cam = L.orbit_camera(1, 128, 128)
+    out = torch.empty((128, 128), dtype=torch.int32, device=cuda)
+    tickets = [srv.submit(L.request(oid, cam.frame_params(), out)) for _ in range(20)]
+    # with one ray in flight at most, later requests are still pending
+    assert srv.cancel(tickets[-1]) == L.SVO_OK
+    r = srv.wait(tickets[-1])
+    assert r.status == L.SVO_ERR_CANCELED
+    for t in tickets[:-1]:
+        assert srv.wait(t).status == L.SVO_OK
+    with pytest.raises(L.SvoError) as e:
+        srv.submit(L.request(99, cam.frame_params(), out))
+    assert e.value.code == L.SVO_ERR_INVALID
+    srv.close()
+    # an octree larger than the whole budget fails its requests instead of hanging
+    tiny = L.Server(L.server_cfg(1 << 20, streams=1))
+    big = tiny.add_octree(workload.scenes[3])
+    t = tiny.submit(L.request(big, cam.frame_params(), out))
+    assert tiny.wait(t, timeout_ms=5000).status == L.SVO_ERR_RANGE
+    tiny.close()
+
+
+def test_repeated_create_serve_destroy(workload, cuda):
+    """Teardown right after the last completion, many times over: the server
+    must outlive its stream callbacks."""
+    import torch
+
+    total = sum(footprint(s) for s in workload.scenes)
+    cams = [L.orbit_camera(k, 48 + 8 * k, 40, radius=1.6) for k in range(12)]
+    outs = [torch.empty((c.height, c.width), dtype=torch.int32, device=cuda) for c in cams]
+    for cycle in range(15):
+        srv = L.Server(L.server_cfg(total, streams=4, max_batch_views=3))
+        oid = srv.add_octree(workload.scenes[cycle % len(workload.scenes)])
+        res = srv.replay([L.request(oid, c.frame_params(), t) for c, t in zip(cams, outs)],
+                         np.zeros(len(cams)), timeout_ms=20000)
+        assert all(r.status == L.SVO_OK for r in res)
+        srv.close()
