@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="icosphere")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the batched-views and served-requests measurements")
     return ap.parse_args()
 
 
@@ -217,6 +219,111 @@ def run_reference(args, wl):
     print(json.dumps(line), flush=True)
 
 
+def _event_ms(torch, fn, reps):
+    fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def batched_leg(dev, reps=10):
+    """64 terrain views of uneven size: the same views as
+    64 per-frame launches on one stream, and as one autotuned, graph-replayed
+    persistent launch."""
+    import torch
+
+    import libsvo_b200 as L
+    from libsvo_b200 import scenes
+
+    t0 = time.perf_counter()
+    wl = scenes.terrain()
+    info = wl.scene.info
+    build_s = time.perf_counter() - t0
+    mm = L.TreeletMemoryManagerCuda(wl.scene, info.treelet_bytes * info.num_treelets)
+    mm.insertAll()
+    mm.initDeviceBuffer()
+    ps = [c.frame_params() for c in wl.cameras]
+    outs = [torch.empty((p.height, p.width), dtype=torch.int32, device=dev) for p in ps]
+    s = torch.cuda.current_stream()
+
+    def per_view():
+        for p, o in zip(ps, outs):
+            mm.render(p, o, stream=s)
+
+    ms_plain = _event_ms(torch, per_view, reps)
+    b = L.Batcher()
+    b.set([L.octree_of(mm)], [L.view_desc(p, 0, o) for p, o in zip(ps, outs)], L.batch_cfg(), stream=s)
+    best, _ = b.autotune(reps=3, stream=s)
+    ms_batch = _event_ms(torch, lambda: b.launch(stream=s), reps)
+    rays = wl.rays_per_step
+    b.close()
+    mm.close()
+    return {"workload": wl.name, "description": wl.description, "rays_per_step": rays,
+            "scene_build_s": round(build_s, 2), "per_view_launches_mrays_s": rays / ms_plain / 1e3,
+            "batched_mrays_s": rays / ms_batch / 1e3, "speedup": ms_plain / ms_batch,
+            "batched_ms": ms_batch, "per_view_ms": ms_plain,
+            "autotuned": {"tile": [best.tile_w, best.tile_h], "block_threads": best.block_threads,
+                          "top_nodes": best.top_nodes, "graph": True}}
+
+
+def served_leg(dev, n=400, rates=(4000, 16000)):
+    """8 octrees served to a Poisson stream of requests
+    from 64x64 to 1920x1080: batched server vs the plain per-frame kernel in the
+    same request loop, all octrees resident; then the batched server with a
+    budget of half the octrees' footprint, so octrees page in and out."""
+    import numpy as np
+    import torch
+
+    import libsvo_b200 as L
+    from libsvo_b200 import scenes as S
+
+    t0 = time.perf_counter()
+    wl = S.serving()
+    build_s = time.perf_counter() - t0
+    footprint = sum(16 * s.info.treelet_bytes // 8 * s.info.num_treelets for s in wl.scenes)
+    reqs = S.serving_requests(n, len(wl.scenes), seed=3)
+    outs = [torch.empty((c.height, c.width), dtype=torch.int32, device=dev) for _, c in reqs]
+    rays = sum(c.width * c.height for _, c in reqs)
+
+    def run(mode, budget, rate_list):
+        srv = L.Server(L.server_cfg(budget, streams=4, max_batch_views=256, mode=mode))
+        ids = [srv.add_octree(s) for s in wl.scenes]
+        rq = [L.request(ids[o], c.frame_params(), t) for (o, c), t in zip(reqs, outs)]
+        srv.replay(rq[:64], np.zeros(64), timeout_ms=120000)  # first loads
+        res = {}
+        for rate in rate_list:
+            arr = S.poisson_arrivals(n, rate, seed=11) if rate else np.zeros(n)
+            r = srv.replay(rq, arr, timeout_ms=120000)
+            lat = np.array([x.done_s - x.submit_s for x in r]) * 1e3
+            span = max(x.done_s for x in r) - min(x.submit_s for x in r)
+            res[str(rate) if rate else "burst"] = {
+                "mrays_s": rays / span / 1e6, "p50_ms": float(np.percentile(lat, 50)),
+                "p99_ms": float(np.percentile(lat, 99)), "launches": len({x.batch for x in r})}
+        st = srv.stats()
+        res["paging"] = {"octree_loads": st.octree_loads, "evictions": st.octree_evictions,
+                         "treelets_paged_in": st.treelets_paged_in, "gb_uploaded": st.bytes_uploaded / 1e9}
+        srv.close()
+        return res
+
+    all_rates = list(rates) + [0]
+    batched = run(L.SERVE_BATCHED, 2 * footprint, all_rates)
+    plain = run(L.SERVE_PLAIN, 2 * footprint, all_rates)
+    paging = run(L.SERVE_BATCHED, footprint // 2, [rates[-1]])
+    return {"workload": wl.name, "description": wl.description, "requests": n, "rays": rays,
+            "scene_build_s": round(build_s, 2), "octree_footprint_gb": footprint / 1e9,
+            "budget_note": "the stand-in octrees total far less than the configuration's 40 GB cap; "
+                           "the paging run caps the pool at half their footprint",
+            "batched": batched, "plain": plain,
+            "speedup_vs_plain": {k: batched[k]["mrays_s"] / plain[k]["mrays_s"]
+                                 for k in batched if k != "paging"},
+            "paging_half_budget": paging}
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -331,7 +438,7 @@ def main():
         peak, peak_kind = load_peaks()
         achieved = algo_bytes / (ms * 1e-3) / 1e9
         traffic = None
-        tp = ROOT / "profiles" / "dram_traffic.json"
+        tp = ROOT / "profiles" / "render_frame_kernel_dram_traffic.json"
         if tp.is_file():
             traffic = json.loads(tp.read_text()).get(wl.name)
         line = {
@@ -362,6 +469,13 @@ def main():
         if not args.no_cpu_baseline and world == 1:
             nodes, attribs = mm.getIncoreBuffer()
             line["cpu_baseline"] = cpu_reference_frames(wl, nodes, attribs)
+        mm.close()
+        if world == 1 and not args.no_extra:
+            for key, leg in (("batched", batched_leg), ("served", served_leg)):
+                try:
+                    line[key] = leg(dev)
+                except Exception as e:  # a failing extra leg must not lose the primary line
+                    line[key] = {"error": f"{type(e).__name__}: {e}"}
         print(json.dumps(line), flush=True)
     mm.close()
     if world > 1:
