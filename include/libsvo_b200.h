@@ -278,6 +278,45 @@ int svo_mm_render_host(svo_mm* mm, const svo_frame_params* params, const svo_tra
  * (capped rays = the watchdog status word), then clears them. */
 int svo_mm_sync(svo_mm* mm, void* stream, svo_stats* out);
 
+/* ---- analysis pass: visibility-driven paging --------------------------- */
+
+/* FeedBackDataElement (opencl/treeletRenderer_rgba.cl:761-766). */
+typedef struct svo_feedback {
+  int32_t node_id;         /* incore index of the node the ray stopped at, 0 = none */
+  float error;             /* leaf: scale_exp2 - tScaleRatio*tcMin; LOD stop: 1/0  */
+  int32_t sub_treelet_gid; /* leaf's sub-treelet gid when not resident, else 0     */
+  float t_min;             /* tcMin of that node; 9999999 when nothing was hit     */
+} svo_feedback;
+
+/* renderToFeedbackBuffer (opencl/treeletRenderer_rgba.cl:960-1011): one
+ * analysis ray per pixel of `params` (sampleAnalyse, :773-953), one record
+ * per pixel into d_feedback; d_rgba (optional) receives the kernel's debug
+ * colour as RGBA8. */
+int svo_feedback_render(const svo_node* d_nodes, uint64_t num_nodes, const svo_frame_params* params,
+                        int32_t stack_size, svo_feedback* d_feedback, uint32_t* d_rgba,
+                        void* stream);
+/* RenderPassAnalyse::performAnalysePass's processing of the records
+ * (src/RenderPassAnalyse.cpp:218-356): newly visible treelets (at most
+ * max_new; 0 = the reference's 12 MB worth) and visible resident treelets
+ * with their ancestors, as gid/error arrays, largest error first; pass them
+ * to svo_mm_update_client_side.  SVO_ERR_RANGE with empty lists on records
+ * the reference rejects.  Capacities smaller than the lists give
+ * SVO_ERR_RANGE with the needed counts in *num_new / *num_old. */
+int svo_mm_analyse_feedback(svo_mm* mm, const svo_feedback* h_feedback, uint64_t n, uint32_t max_new,
+                            int32_t* new_gids, float* new_errors, uint32_t new_capacity,
+                            uint32_t* num_new, int32_t* old_gids, float* old_errors,
+                            uint32_t old_capacity, uint32_t* num_old);
+/* One dynamic-loading step of the reference's frame loop
+ * (raycast_serialized_opencl.cpp:684-716): the analysis pass over the
+ * frame's view at (width/divisor, height/divisor) with the far plane's
+ * origin offset by (jitter_x, jitter_y) * divisor / 2 frame pixels (the
+ * reference's "rumble", RenderPassAnalyse.cpp:176-184; jitter in [-1, 1]),
+ * records read back, analysed, treelets inserted (evicting by visibility)
+ * and uploaded.  Blocks until the records are on the host. */
+int svo_mm_analysis_step(svo_mm* mm, const svo_frame_params* frame, uint32_t divisor,
+                         float jitter_x, float jitter_y, int32_t stack_size, void* stream,
+                         uint32_t* num_new, uint32_t* num_old);
+
 /* ---- batched views: one persistent launch ------------------------------ */
 
 /* A resident octree: device node and attribute pools (e.g. from

@@ -750,6 +750,63 @@ class Server:
             pass
 
 
+# ---- analysis pass ---------------------------------------------------------------
+class svo_feedback(ctypes.Structure):
+    _fields_ = [("node_id", ctypes.c_int32), ("error", ctypes.c_float), ("sub_treelet_gid", ctypes.c_int32),
+                ("t_min", ctypes.c_float)]
+
+
+FEEDBACK_DTYPE = np.dtype([("node_id", "<i4"), ("error", "<f4"), ("sub_treelet_gid", "<i4"), ("t_min", "<f4")])
+
+for _name, (_args, _res) in {
+    "svo_feedback_render": ([_vp, _u64, _P(svo_frame_params), _i32, _vp, _vp, _vp], ctypes.c_int),
+    "svo_mm_analyse_feedback": ([_vp, _vp, _u64, _u32, _vp, _vp, _u32, _P(_u32), _vp, _vp, _u32, _P(_u32)],
+                                ctypes.c_int),
+    "svo_mm_analysis_step": ([_vp, _P(svo_frame_params), _u32, _f32, _f32, _i32, _vp, _P(_u32), _P(_u32)],
+                             ctypes.c_int),
+}.items():
+    _fn = getattr(_L, _name)
+    _fn.argtypes = _args
+    _fn.restype = _res
+
+
+def feedback_render(d_nodes, num_nodes, params: svo_frame_params, d_feedback, d_rgba=None, stack_size=13,
+                    stream=None):
+    """renderToFeedbackBuffer over a device node pool (one record per pixel)."""
+    _check(_L.svo_feedback_render(_dptr(d_nodes), num_nodes, ctypes.byref(params), stack_size,
+                                  _dptr(d_feedback), _dptr(d_rgba), _stream_ptr(stream)), "svo_feedback_render")
+
+
+def _analyse_feedback(self, records: np.ndarray, max_new: int = 0):
+    """performAnalysePass's processing: ([(gid, error)] new, [(gid, error)] old)."""
+    rec = np.ascontiguousarray(records).view(np.uint8).reshape(-1)
+    n = rec.size // 16
+    nn, no = _u32(), _u32()
+    rc = _L.svo_mm_analyse_feedback(self._h, _np_ptr(rec), n, max_new, None, None, 0, ctypes.byref(nn),
+                                    None, None, 0, ctypes.byref(no))
+    _check(rc, "svo_mm_analyse_feedback")
+    ng = np.zeros(nn.value, np.int32); ne = np.zeros(nn.value, np.float32)
+    og = np.zeros(no.value, np.int32); oe = np.zeros(no.value, np.float32)
+    _check(_L.svo_mm_analyse_feedback(self._h, _np_ptr(rec), n, max_new, _np_ptr(ng), _np_ptr(ne), nn.value,
+                                      ctypes.byref(nn), _np_ptr(og), _np_ptr(oe), no.value, ctypes.byref(no)),
+           "svo_mm_analyse_feedback")
+    return list(zip(ng.tolist(), ne.tolist())), list(zip(og.tolist(), oe.tolist()))
+
+
+def _perform_analyse_pass(self, frame: svo_frame_params, divisor=8, jitter=(0.0, 0.0), stack_size=13,
+                          stream=None):
+    """One dynamic-loading step (analysis pass, insert, upload): (new, old) counts."""
+    nn, no = _u32(), _u32()
+    _check(_L.svo_mm_analysis_step(self._h, ctypes.byref(frame), divisor, float(jitter[0]), float(jitter[1]),
+                                   stack_size, _stream_ptr(stream), ctypes.byref(nn), ctypes.byref(no)),
+           "svo_mm_analysis_step")
+    return nn.value, no.value
+
+
+TreeletMemoryManagerCuda.analyseFeedback = _analyse_feedback
+TreeletMemoryManagerCuda.performAnalysePass = _perform_analyse_pass
+
+
 # ---- teardown ------------------------------------------------------------------
 # Handles still open when the interpreter exits are closed here, before the
 # CUDA runtime linked into the library is torn down: a server's dispatcher

@@ -5,9 +5,11 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "../../include/libsvo_b200.h"
 #include "errors.h"
+#include "feedback.h"
 #include "memory_manager.h"
 #include "render.h"
 #include "scene.h"
@@ -401,6 +403,92 @@ int svo_mm_sync(svo_mm* mm, void* stream, svo_stats* out) {
   SVO_CUDA_TRY(cudaMemset(mm->impl.device_stats(), 0, sizeof(svo_stats)));
   if (out) *out = st;
   return SVO_OK;
+}
+
+// ---- analysis pass ----------------------------------------------------------
+
+int svo_feedback_render(const svo_node* d_nodes, uint64_t num_nodes, const svo_frame_params* params,
+                        int32_t stack_size, svo_feedback* d_feedback, uint32_t* d_rgba,
+                        void* stream) {
+  if (!d_nodes || !params || !d_feedback || num_nodes == 0 || num_nodes > 0x100000000ull)
+    return SVO_ERR_INVALID;
+  if (stack_size < 2 || stack_size > 24) return SVO_ERR_RANGE;
+  return svo::launch_feedback(d_nodes, num_nodes, *params, stack_size, d_feedback, d_rgba,
+                              (cudaStream_t)stream);
+}
+
+int svo_mm_analyse_feedback(svo_mm* mm, const svo_feedback* h_feedback, uint64_t n, uint32_t max_new,
+                            int32_t* new_gids, float* new_errors, uint32_t new_capacity,
+                            uint32_t* num_new, int32_t* old_gids, float* old_errors,
+                            uint32_t old_capacity, uint32_t* num_old) {
+  if (!mm || (n && !h_feedback)) return SVO_ERR_INVALID;
+  return guarded([&] {
+    std::vector<std::pair<int32_t, float>> nw, old;
+    const uint32_t cap = max_new ? max_new : mm->impl.default_max_new_treelets();
+    const int rc = mm->impl.analyse_feedback(h_feedback, n, cap, nw, old);
+    if (num_new) *num_new = (uint32_t)nw.size();
+    if (num_old) *num_old = (uint32_t)old.size();
+    if (rc != SVO_OK) return rc;
+    if ((new_gids || new_errors) && nw.size() > new_capacity) return SVO_ERR_RANGE;
+    if ((old_gids || old_errors) && old.size() > old_capacity) return SVO_ERR_RANGE;
+    for (size_t i = 0; i < nw.size(); ++i) {
+      if (new_gids) new_gids[i] = nw[i].first;
+      if (new_errors) new_errors[i] = nw[i].second;
+    }
+    for (size_t i = 0; i < old.size(); ++i) {
+      if (old_gids) old_gids[i] = old[i].first;
+      if (old_errors) old_errors[i] = old[i].second;
+    }
+    return SVO_OK;
+  });
+}
+
+int svo_mm_analysis_step(svo_mm* mm, const svo_frame_params* frame, uint32_t divisor,
+                         float jitter_x, float jitter_y, int32_t stack_size, void* stream,
+                         uint32_t* num_new, uint32_t* num_old) {
+  if (!mm || !frame || divisor == 0 || !mm->impl.device_ready()) return SVO_ERR_INVALID;
+  if (stack_size < 2 || stack_size > 24) return SVO_ERR_RANGE;
+  return guarded([&] {
+    cudaStream_t s = stream ? (cudaStream_t)stream : mm->impl.render_stream();
+    // analysis buffer and its one-pixel far-plane vectors
+    // (RenderPassAnalyse.cpp:168-193): same frustum, coarser pixels
+    svo_frame_params a = *frame;
+    a.width = std::max(1u, frame->width / divisor);
+    a.height = std::max(1u, frame->height / divisor);
+    const double sx = (double)frame->width / a.width, sy = (double)frame->height / a.height;
+    for (int k = 0; k < 3; ++k) {
+      a.pixel_far_h[k] = (float)(frame->pixel_far_h[k] * sx);
+      a.pixel_far_v[k] = (float)(frame->pixel_far_v[k] * sy);
+      a.far_lower_left[k] = (float)(frame->far_lower_left[k] +
+                                    jitter_x * (double)divisor * frame->pixel_far_h[k] * 0.5 +
+                                    jitter_y * (double)divisor * frame->pixel_far_v[k] * 0.5);
+    }
+    const uint64_t n = (uint64_t)a.width * a.height;
+    svo_feedback* d_fb = nullptr;
+    int rc = mm->impl.feedback_scratch(n, &d_fb);
+    if (rc != SVO_OK) return rc;
+    rc = mm->impl.wait_uploads(s);
+    if (rc != SVO_OK) return rc;
+    rc = svo::launch_feedback(mm->impl.device_nodes(), mm->impl.incore_nodes(), a, stack_size, d_fb,
+                              nullptr, s);
+    if (rc != SVO_OK) return rc;
+    std::vector<svo_feedback> h(n);
+    SVO_CUDA_TRY(cudaMemcpyAsync(h.data(), d_fb, n * sizeof(svo_feedback), cudaMemcpyDeviceToHost, s));
+    SVO_CUDA_TRY(cudaStreamSynchronize(s));
+    std::vector<std::pair<int32_t, float>> nw, old;
+    rc = mm->impl.analyse_feedback(h.data(), n, mm->impl.default_max_new_treelets(), nw, old);
+    if (num_new) *num_new = (uint32_t)nw.size();
+    if (num_old) *num_old = (uint32_t)old.size();
+    if (rc != SVO_OK) return rc;
+    std::vector<int32_t> ng(nw.size()), og(old.size());
+    std::vector<float> ne(nw.size());
+    for (size_t i = 0; i < nw.size(); ++i) ng[i] = nw[i].first, ne[i] = nw[i].second;
+    for (size_t i = 0; i < old.size(); ++i) og[i] = old[i].first;
+    rc = mm->impl.update_client_side(ng.data(), ne.data(), (uint32_t)ng.size(), og.data(),
+                                     (uint32_t)og.size());
+    const int up = mm->impl.update_device_memory(nullptr);
+    return rc != SVO_OK ? rc : up;
+  });
 }
 
 }  // extern "C"

@@ -233,6 +233,7 @@ TreeletMemoryManagerCuda::~TreeletMemoryManagerCuda() {
   }
   cudaFree(d_stats_);
   cudaFree(d_rgba_);
+  cudaFree(d_feedback_);
   for (int i = 0; i < 2; ++i) {
     if (stage_evt_[i]) cudaEventDestroy(stage_evt_[i]);
     if (stage_[i]) cudaFreeHost(stage_[i]);
@@ -367,6 +368,18 @@ int TreeletMemoryManagerCuda::rgba_scratch(uint64_t pixels, uint32_t** out) {
     d_rgba_pixels_ = pixels;
   }
   *out = d_rgba_;
+  return SVO_OK;
+}
+
+int TreeletMemoryManagerCuda::feedback_scratch(uint64_t records, svo_feedback** out) {
+  if (records > d_feedback_records_) {
+    cudaFree(d_feedback_);
+    d_feedback_ = nullptr;
+    d_feedback_records_ = 0;
+    SVO_CUDA_TRY(cudaMalloc(&d_feedback_, records * sizeof(svo_feedback)));
+    d_feedback_records_ = records;
+  }
+  *out = d_feedback_;
   return SVO_OK;
 }
 

@@ -59,6 +59,17 @@ class TreeletMemoryManager {
   const svo_attrib* host_attribs() const { return incore_attr_; }
   const svo_scene& scene() const { return scene_; }
 
+  // performAnalysePass's processing of the feedback records
+  // (src/RenderPassAnalyse.cpp:218-356): newly visible treelets (cut to
+  // max_new) and visible resident treelets, each as (gid, error), largest
+  // error first.  SVO_ERR_RANGE (and empty lists) on records the reference
+  // rejects.
+  int analyse_feedback(const svo_feedback* fb, uint64_t n, uint32_t max_new,
+                       std::vector<std::pair<int32_t, float>>& out_new,
+                       std::vector<std::pair<int32_t, float>>& out_old) const;
+  // 12 MB worth of treelets (RenderPassAnalyse.cpp:340).
+  uint32_t default_max_new_treelets() const;
+
   // Slot ranges the reference's updateDeviceMemory would copy
   // (TreeletMemoryManagerCl.cpp:177-236), as (first slot, slot count).
   std::vector<std::pair<uint32_t, uint32_t>> upload_ranges() const;
@@ -106,6 +117,8 @@ class TreeletMemoryManagerCuda : public TreeletMemoryManager {
   int wait_uploads(cudaStream_t stream);
   // Device RGBA scratch for host-output renders (grown on demand).
   int rgba_scratch(uint64_t pixels, uint32_t** out);
+  // Device feedback-record scratch for analysis passes (grown on demand).
+  int feedback_scratch(uint64_t records, svo_feedback** out);
 
  private:
   int stage_copy(void* dst, const void* src, uint64_t bytes);
@@ -127,6 +140,8 @@ class TreeletMemoryManagerCuda : public TreeletMemoryManager {
   int stage_next_ = 0;
   uint32_t* d_rgba_ = nullptr;
   uint64_t d_rgba_pixels_ = 0;
+  svo_feedback* d_feedback_ = nullptr;
+  uint64_t d_feedback_records_ = 0;
 };
 
 }  // namespace svo

@@ -41,6 +41,11 @@ struct RayHit {
   uint32_t flags;
   uint32_t loops;
   uint32_t fetches;  // loop iterations that read the parent node
+  // set on a leaf or LOD stop, for the analysis pass: the hit child's entry
+  // distance, the child size, and whether the child was a leaf
+  float tc_min;
+  float sx2;
+  uint32_t leaf;
 };
 
 __device__ __forceinline__ float cl_max(float a, float b) { return (a < b) ? b : a; }
@@ -249,6 +254,9 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
         h.t = tmin;
         h.loops = loops;
         h.fetches = fetches;
+        h.tc_min = tc_min;
+        h.sx2 = sx2;
+        h.leaf = leaf ? 1u : 0u;
         return;
       }
       if (kFlat && scale == 0) {  // non-leaf below the octree's depth: corrupt pool
@@ -298,6 +306,9 @@ __device__ __forceinline__ RayHit cast_ray(const Fetch& fetch, uint64_t num_node
   h.flags = 0u;
   h.loops = 0u;
   h.fetches = 0u;
+  h.tc_min = 0.0f;
+  h.sx2 = 0.0f;
+  h.leaf = 0u;
 
   float t_min, t_max;
   {

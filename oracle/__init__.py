@@ -75,6 +75,8 @@ def lib():
         L.oracle_cast_rays.restype = u64
         L.oracle_pixel_rays.argtypes = [vp, vp, vp]
         L.oracle_pixel_rays.restype = None
+        L.oracle_feedback.argtypes = [vp, u64, vp, i32, vp, vp, i32]
+        L.oracle_feedback.restype = None
         assert L.oracle_hit_record_size() == 16
         _lib = L
     return _lib
@@ -95,6 +97,8 @@ def reference_lib():
         L.ref_render.restype = None
         L.ref_render_rows.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32, vp, i32]
         L.ref_render_rows.restype = None
+        L.ref_feedback.argtypes = [vp, vp, vp, vp, i32]
+        L.ref_feedback.restype = None
         assert L.ref_hit_record_size() == 16
         _ref = L
     return _ref
@@ -186,3 +190,31 @@ def to_rgba8(rgbaf: np.ndarray) -> np.ndarray:
     c = np.clip(rgbaf.astype(np.float32), np.float32(0), np.float32(1))
     b = np.floor(c * np.float32(255.0) + np.float32(0.5)).astype(np.uint32)
     return b[..., 0] | (b[..., 1] << 8) | (b[..., 2] << 16) | (b[..., 3] << 24)
+
+
+FEEDBACK_DTYPE = np.dtype([("node_id", "<i4"), ("error", "<f4"), ("sub_treelet_gid", "<i4"), ("t_min", "<f4")])
+
+
+def feedback(nodes, params: bytes, stack_size: int = 13, threads=None):
+    """renderToFeedbackBuffer on the CPU: (records [H, W], debug rgbaf [H, W, 4])."""
+    nodes = np.ascontiguousarray(nodes, dtype=np.uint32)
+    w, h = np.frombuffer(params[:8], dtype=np.uint32)
+    rec = np.zeros((h, w), dtype=FEEDBACK_DTYPE)
+    rgbaf = np.zeros((h, w, 4), dtype=np.float32)
+    pbuf = np.frombuffer(bytearray(params), dtype=np.uint8)
+    lib().oracle_feedback(_ptr(nodes), nodes.shape[0], _ptr(pbuf), int(stack_size), _ptr(rec), _ptr(rgbaf),
+                          _threads(threads))
+    return rec, rgbaf
+
+
+def reference_feedback(nodes, params: bytes, threads=None):
+    L = reference_lib()
+    if L is None:
+        return None
+    nodes = np.ascontiguousarray(nodes, dtype=np.uint32)
+    w, h = np.frombuffer(params[:8], dtype=np.uint32)
+    rec = np.zeros((h, w), dtype=FEEDBACK_DTYPE)
+    rgbaf = np.zeros((h, w, 4), dtype=np.float32)
+    pbuf = np.frombuffer(bytearray(params), dtype=np.uint8)
+    L.ref_feedback(_ptr(nodes), _ptr(pbuf), _ptr(rec), _ptr(rgbaf), _threads(threads))
+    return rec, rgbaf

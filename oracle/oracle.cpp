@@ -359,6 +359,94 @@ Hit cast_flat(const uint32_t* nodes, uint64_t num_nodes, V3 o, V3 d, float tsr, 
   return h;
 }
 
+// sampleAnalyse (opencl/treeletRenderer_rgba.cl:773-953): the analysis ray.
+// Same descent as sample(); it reports {node, error, sub-treelet gid, tcMin}
+// at a leaf or LOD stop and nothing on a miss or when the watchdog fires.
+struct Feedback {
+  int32_t node_id;
+  float error;
+  int32_t sub_treelet_gid;
+  float t_min;
+};
+static_assert(sizeof(Feedback) == 16, "FeedBackDataElement is 16 bytes");
+
+Feedback analyse_ray(const uint32_t* nodes, uint64_t num_nodes, V3 o, V3 d, float tsr, int S) {
+  Feedback e{0, 0.0f, 0, 9999999.0f};
+  float t_min, t_max;
+  if (!root_slab(o, d, t_min, t_max)) return e;
+  const int scale_max = S;
+  int scale = scale_max - 1;
+  const float min_normal = 0.0001f;
+  const float eps = 0.00001f;
+  Frame stack[32];
+  stack[scale] = Frame{t_min, t_max, 0u, V3{0.0f, 0.0f, 0.0f}};
+  if (std::fabs(d.x) < min_normal) d.x = min_normal * cl_sign(d.x);
+  if (std::fabs(d.y) < min_normal) d.y = min_normal * cl_sign(d.y);
+  if (std::fabs(d.z) < min_normal) d.z = min_normal * cl_sign(d.z);
+  const float rx = 1.0f / d.x, px = -o.x * rx;
+  const float ry = 1.0f / d.y, py = -o.y * ry;
+  const float rz = 1.0f / d.z, pz = -o.z * rz;
+  uint32_t loops = 0;
+  const uint32_t max_loops = (uint32_t)((scale_max + 1) * (scale_max + 1) * 5);
+  while (scale < scale_max) {
+    ++loops;
+    if (loops == max_loops) break;
+    Frame& p = stack[scale];
+    const float sx2 = pow2i(scale - scale_max);
+    const float half = sx2 * 0.5f;
+    if (p.tmax < 0.0f) {
+      ++scale;
+      continue;
+    }
+    if (!(std::fabs(p.tmin - p.tmax) > eps)) {
+      ++scale;
+      continue;
+    }
+    const float te = p.tmin + eps;
+    const float ex = (o.x + te * d.x) - p.center.x;
+    const float ey = (o.y + te * d.y) - p.center.y;
+    const float ez = (o.z + te * d.z) - p.center.z;
+    const uint32_t ci = 4u * (ex > 0.0f) + 2u * (ey > 0.0f) + (ez > 0.0f);
+    const V3 cc{(-0.5f + (float)((ci & 4u) != 0)) * sx2 + p.center.x,
+                (-0.5f + (float)((ci & 2u) != 0)) * sx2 + p.center.y,
+                (-0.5f + (float)((ci & 1u) != 0)) * sx2 + p.center.z};
+    float tx0 = rx * (cc.x - half) + px, tx1 = rx * (cc.x + half) + px;
+    if (tx0 > tx1) std::swap(tx0, tx1);
+    float ty0 = ry * (cc.y - half) + py, ty1 = ry * (cc.y + half) + py;
+    if (ty0 > ty1) std::swap(ty0, ty1);
+    float tz0 = rz * (cc.z - half) + pz, tz1 = rz * (cc.z + half) + pz;
+    if (tz0 > tz1) std::swap(tz0, tz1);
+    const float tc_min = cl_max(tx0, cl_max(ty0, tz0));
+    const float tc_max = cl_min(tx1, cl_min(ty1, tz1));
+    if (p.node >= num_nodes) return e;
+    const uint32_t fc = nodes[2 * (uint64_t)p.node];
+    const uint32_t masks = nodes[2 * (uint64_t)p.node + 1];
+    if (valid_bit(masks, ci)) {
+      const uint32_t child = p.node + nth_child(masks, fc, ci);
+      if (leaf_bit(masks, ci)) {
+        e.node_id = (int32_t)child;
+        e.error = sx2 - tsr * tc_min;
+        e.sub_treelet_gid = child < num_nodes ? (int32_t)nodes[2 * (uint64_t)child] : 0;
+        e.t_min = tc_min;
+        return e;
+      }
+      if (tsr * tc_min > sx2 || scale_max - scale == scale_max - 1) {
+        e.node_id = (int32_t)child;
+        e.error = (tsr * tc_min > sx2) ? 1.0f : 0.0f;
+        e.sub_treelet_gid = 0;
+        e.t_min = tc_min;
+        return e;
+      }
+      p.tmin = tc_max;
+      --scale;
+      stack[scale] = Frame{tc_min, tc_max, child, cc};
+      continue;
+    }
+    p.tmin = tc_max;
+  }
+  return e;
+}
+
 struct FrameParams {
   uint32_t width, height;
   float t_scale_ratio;
@@ -552,6 +640,37 @@ void oracle_pixel_rays(const void* params, float* origins, float* dirs) {
       dirs[3 * i + 1] = d.y;
       dirs[3 * i + 2] = d.z;
     }
+}
+
+// renderToFeedbackBuffer (opencl/treeletRenderer_rgba.cl:960-1011) over a
+// whole analysis buffer: one 16-byte record per pixel and (optional) the
+// debug colour per pixel as floats.
+void oracle_feedback(const uint32_t* nodes, uint64_t num_nodes, const void* params, int S,
+                     void* records, float* rgbaf, int threads) {
+  const FrameParams& fp = *(const FrameParams*)params;
+  Feedback* out = (Feedback*)records;
+  parallel_lines(fp.height, 4, threads, [&](uint32_t y) {
+    for (uint32_t x = 0; x < fp.width; ++x) {
+      V3 o, d;
+      pixel_ray(fp, x, y, o, d);
+      const Feedback e = analyse_ray(nodes, num_nodes, o, d, fp.t_scale_ratio, S);
+      const uint64_t pix = (uint64_t)y * fp.width + x;
+      out[pix] = e;
+      if (rgbaf) {
+        float* c = rgbaf + 4 * pix;
+        if (e.node_id != 0) {
+          c[0] = (float)e.sub_treelet_gid;
+          c[1] = 0.0f;
+          c[2] = e.error;
+        } else {
+          c[0] = 0.2f;
+          c[1] = 0.3f;
+          c[2] = 0.2f;
+        }
+        c[3] = 1.0f;
+      }
+    }
+  });
 }
 
 int oracle_hit_record_size(void) { return (int)sizeof(Hit); }

@@ -24,7 +24,7 @@ from rays import edge_rays, paged_menger_manager, random_octree_pool  # noqa: E4
 HERE = Path(__file__).resolve().parent
 
 
-def fixture(name, nodes, attribs, frames, rays, tsrs):
+def fixture(name, nodes, attribs, frames, rays, tsrs, feedback_frames=()):
     oracle.build_reference()
     assert oracle.reference_lib() is not None, "reference build missing"
     out = {"nodes": nodes, "attribs": attribs}
@@ -38,6 +38,11 @@ def fixture(name, nodes, attribs, frames, rays, tsrs):
         out[f"tsr_{j}"] = np.float32(tsr)
         for k in ("node", "t", "depth", "hit", "loops"):
             out[f"hits_{j}_{k}"] = h[k]
+    for k, p in enumerate(feedback_frames):
+        out[f"fb_params_{k}"] = np.frombuffer(bytes(p), dtype=np.uint8)
+        rec, img = oracle.reference_feedback(nodes, bytes(p))
+        out[f"fb_rec_{k}"] = rec.view(np.uint8)
+        out[f"fb_img_{k}"] = img
     np.savez_compressed(HERE / f"{name}.npz", **out)
     print(name, sum(v.nbytes for v in out.values() if hasattr(v, "nbytes")), "bytes raw")
 
@@ -59,6 +64,16 @@ def main():
     n, a = mm.getIncoreBuffer()
     frames = [L.orbit_camera(7, 64, 64, radius=1.4).frame_params(t_scale_ratio=0.0)]
     fixture("menger_paged", n, a, frames, edge_rays(n_random=2000, seed=3), [0.0])
+
+    # analysis pass over a partially resident pool (sub-treelet gids appear)
+    from test_oracle_pinning import partially_resident_menger
+
+    _, mm, _ = partially_resident_menger()
+    n, a = mm.getIncoreBuffer()
+    cam = L.orbit_camera(3, 48, 40, radius=1.3)
+    fixture("menger_partial", n, a, [cam.frame_params(t_scale_ratio=0.0)],
+            edge_rays(n_random=1000, seed=4), [0.0],
+            feedback_frames=[cam.frame_params(t_scale_ratio=0.0), cam.frame_params()])
 
 
 if __name__ == "__main__":

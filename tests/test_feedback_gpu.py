@@ -1,0 +1,84 @@
+"""Analysis pass on the GPU: the feedback kernel against the oracle bit for
+bit, and visibility-driven paging converging to the fully resident image."""
+import numpy as np
+import pytest
+
+import libsvo_b200 as L
+import oracle
+from test_oracle_pinning import partially_resident_menger
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_feedback_kernel_matches_oracle(cuda, seed):
+    import torch
+
+    _, mm, _ = partially_resident_menger()
+    mm.initDeviceBuffer()
+    d_nodes, _, n = mm.getDeviceIncoreBuffer()
+    nodes, _ = mm.getIncoreBuffer()
+    for tsr in (0.0, None):
+        p = L.orbit_camera(seed, 150, 100, radius=(1.2, 2.0)).frame_params(t_scale_ratio=tsr)
+        fb = torch.empty(p.width * p.height * 16, dtype=torch.uint8, device=cuda)
+        img = torch.empty((p.height, p.width), dtype=torch.int32, device=cuda)
+        L.feedback_render(d_nodes, n, p, fb, img)
+        torch.cuda.synchronize()
+        rec, rgbaf = oracle.feedback(nodes, bytes(p))
+        got = fb.cpu().numpy().view(oracle.FEEDBACK_DTYPE).reshape(p.height, p.width)
+        assert np.array_equal(got.view(np.uint8), rec.view(np.uint8))
+        assert np.array_equal(img.cpu().numpy().view(np.uint32), oracle.to_rgba8(rgbaf))
+    mm.close()
+
+
+def render(mm, p, cuda):
+    import torch
+
+    rgba = torch.empty((p.height, p.width), dtype=torch.int32, device=cuda)
+    hits = torch.empty(p.width * p.height * 16, dtype=torch.uint8, device=cuda)
+    mm.render(p, rgba, hits)
+    torch.cuda.synchronize()
+    return rgba.cpu().numpy(), hits.cpu().numpy().view(L.HIT_DTYPE)
+
+
+@pytest.mark.parametrize("scene_kind", ["menger", "icosphere"])
+def test_paging_by_analysis_converges_to_full_residency(cuda, scene_kind):
+    if scene_kind == "menger":
+        scene = L.Scene.menger(level=4, depth=7, seed=3, treelet_levels=3)
+        cam = L.orbit_camera(5, 160, 120, radius=1.5)
+    else:
+        v, t = L.icosphere(4, seed=2)
+        scene = L.Scene.from_mesh(v, t, 8, treelet_levels=3)
+        cam = L.orbit_camera(6, 160, 120, radius=1.6)
+    info = scene.info
+    p = cam.frame_params(t_scale_ratio=0.0)
+    full = L.TreeletMemoryManagerCuda(scene, info.treelet_bytes * info.num_treelets)
+    full.insertAll()
+    full.initDeviceBuffer()
+    want_rgba, want_hits = render(full, p, cuda)
+    full.close()
+
+    mm = L.TreeletMemoryManagerCuda(scene, info.treelet_bytes * info.num_treelets)
+    mm.initDeviceBuffer()  # only the root treelet is resident
+    steps, loaded = 0, 0
+    while steps < 60:
+        new, old = mm.performAnalysePass(p, divisor=1)
+        steps += 1
+        loaded += new
+        if new == 0:
+            break
+    assert new == 0 and 0 < loaded < info.num_treelets
+    got_rgba, got_hits = render(mm, p, cuda)
+    assert np.array_equal(got_rgba, want_rgba)
+    for k in ("hit", "depth", "loops"):
+        assert np.array_equal(got_hits[k], want_hits[k])
+    assert np.array_equal(got_hits["t"].view(np.uint32), want_hits["t"].view(np.uint32))
+    # the reference's defaults: 1/8 resolution with jittered far plane
+    mm.resetIncoreBuffer()
+    rng = np.random.default_rng(1)
+    total = 0
+    for _ in range(8):
+        new, _ = mm.performAnalysePass(p, divisor=8, jitter=tuple(rng.uniform(-1, 1, 2)))
+        total += new
+    assert total > 0
+    mm.close()

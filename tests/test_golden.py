@@ -17,7 +17,7 @@ FIXTURES = sorted(GOLDEN.glob("*.npz"))
 
 
 def test_fixtures_present():
-    assert len(FIXTURES) >= 3
+    assert len(FIXTURES) >= 4
 
 
 @pytest.mark.parametrize("path", FIXTURES, ids=[p.stem for p in FIXTURES])
@@ -44,3 +44,9 @@ def test_oracle_reproduces_reference_outputs(path):
         assert np.array_equal(h["t"].view(np.uint32), z[f"hits_{j}_t"].view(np.uint32))
         j += 1
     assert j > 0
+    k = 0
+    while f"fb_params_{k}" in z:
+        rec, img = oracle.feedback(nodes, z[f"fb_params_{k}"].tobytes())
+        assert np.array_equal(rec.view(np.uint8).reshape(-1), z[f"fb_rec_{k}"].reshape(-1)), f"feedback {k}"
+        assert np.array_equal(img.view(np.uint32), z[f"fb_img_{k}"].view(np.uint32))
+        k += 1

@@ -109,3 +109,31 @@ def test_unorm8_conversion_is_exact_for_packed_bytes():
     c = b * np.float32(0.003921569)
     back = np.floor(c * np.float32(255.0) + np.float32(0.5))
     assert np.array_equal(back, b)
+
+
+def partially_resident_menger():
+    """Root and a few top treelets resident: leaves with non-resident
+    sub-treelets appear in the pool."""
+    scene = L.Scene.menger(level=4, depth=7, seed=3, treelet_levels=3)
+    ntl = scene.info.num_treelets
+    parents = np.array([scene.treelet(g)["parent_gid"] for g in range(ntl)])
+    mm = L.TreeletMemoryManagerCuda(scene, scene.info.treelet_bytes * ntl)
+    top = [g for g in range(1, ntl) if parents[g] == 0]
+    for g in top[::2]:
+        assert mm.insertTreeletIntoIncoreBuffer(g)
+    return scene, mm, parents
+
+
+@ref_needed
+@pytest.mark.parametrize("seed", [1, 2, 3, 4])
+def test_feedback_pass(seed):
+    _, mm, _ = partially_resident_menger()
+    nodes, _ = mm.getIncoreBuffer()
+    for tsr in (0.0, None):
+        p = bytes(L.orbit_camera(seed, 120, 80, radius=(1.2, 2.0)).frame_params(t_scale_ratio=tsr))
+        rec, img = oracle.feedback(nodes, p)
+        ref_rec, ref_img = oracle.reference_feedback(nodes, p)
+        assert np.array_equal(rec.view(np.uint8), ref_rec.view(np.uint8))
+        assert np.array_equal(img.view(np.uint32), ref_img.view(np.uint32))
+        if tsr == 0.0:
+            assert (rec["sub_treelet_gid"] > 0).any()
