@@ -66,7 +66,10 @@ typedef struct svo_frame_params {
   uint32_t height;          /* frameBufferSize.y                         */
   float t_scale_ratio;      /* frameBufferSize.z (LOD footprint per t)   */
   int32_t mode;             /* otherParams.x: 0 colour, 1 normal,
-                               3 octree depth, 4 pixel depth, 5 loops    */
+                               2 loops as wavelength colour, 3 octree
+                               depth, 4 pixel depth, 5 loops, 6 Phong,
+                               7 LOD quality (2, 6, 7: svo_render and
+                               svo_mm_render only; 6, 7: treelet only)   */
   float pixel_far_h[4];     /* pixelFarVectorH                           */
   float pixel_far_v[4];     /* pixelFarVectorV                           */
   float far_lower_left[4];  /* far_lower_left                            */
@@ -274,6 +277,33 @@ int svo_mm_render(svo_mm* mm, const svo_frame_params* params, const svo_trace_cf
  * image read back. */
 int svo_mm_render_host(svo_mm* mm, const svo_frame_params* params, const svo_trace_cfg* cfg,
                        uint32_t* h_rgba, void* stream);
+/* Shadow rays: one per primary hit, toward a directional light. */
+typedef struct svo_shadow_cfg {
+  float light_direction[3]; /* unit vector toward the light, used as given  */
+  float t_scale_ratio;      /* tScaleRatio of the shadow rays (0.001)      */
+  float normal_offset;      /* origin = hit node centre + normal * offset
+                               (0.01)                                      */
+  uint32_t reserved;        /* 0                                           */
+} svo_shadow_cfg;
+
+/* Primary ray plus one shadow ray per hit, shaded as
+ * shade_diffuse_color_shadow (opencl/fillFrameBuffer_rgba.cl:494-529; the
+ * live renderer's shade_phong has its shadow ray compiled out, :475-484) with
+ * the live renderer's attribute index (= node index): the shadow ray is
+ * sample() (opencl/treeletRenderer_rgba.cl:201-382) from nodeCenter +
+ * normal * offset.  params->mode is ignored; treelet traversal only.  Writes
+ * RGBA8 to d_rgba and, when not NULL, the primary and the shadow hit record
+ * per pixel (zeros where no shadow ray was cast). */
+int svo_render_shadow(const svo_node* d_nodes, const svo_attrib* d_attribs, uint64_t num_nodes,
+                      const svo_frame_params* params, const svo_trace_cfg* cfg,
+                      const svo_shadow_cfg* shadow, uint32_t* d_rgba, svo_hit* d_hits,
+                      svo_hit* d_shadow_hits, svo_stats* d_stats, void* stream);
+/* svo_render_shadow over the manager's incore buffer, after its pending
+ * uploads; counters accumulate in the manager. */
+int svo_mm_render_shadow(svo_mm* mm, const svo_frame_params* params, const svo_trace_cfg* cfg,
+                         const svo_shadow_cfg* shadow, uint32_t* d_rgba, svo_hit* d_hits,
+                         svo_hit* d_shadow_hits, void* stream);
+
 /* Waits for `stream` and returns the manager's accumulated counters
  * (capped rays = the watchdog status word), then clears them. */
 int svo_mm_sync(svo_mm* mm, void* stream, svo_stats* out);

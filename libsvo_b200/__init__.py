@@ -122,8 +122,14 @@ class svo_batch_cfg(ctypes.Structure):
                 ("top_nodes", ctypes.c_uint32), ("use_graph", ctypes.c_uint32)]
 
 
+class svo_shadow_cfg(ctypes.Structure):
+    _fields_ = [("light_direction", ctypes.c_float * 3), ("t_scale_ratio", ctypes.c_float),
+                ("normal_offset", ctypes.c_float), ("reserved", ctypes.c_uint32)]
+
+
 assert ctypes.sizeof(svo_frame_params) == 80
 assert ctypes.sizeof(svo_view_desc) == 104
+assert ctypes.sizeof(svo_shadow_cfg) == 24
 
 _vp, _u32, _u64, _i32, _f32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32, ctypes.c_float
 _P = ctypes.POINTER
@@ -166,6 +172,10 @@ _SIGS = {
     "svo_mm_render": ([_vp, _P(svo_frame_params), _P(svo_trace_cfg), _vp, _vp, _vp], ctypes.c_int),
     "svo_mm_render_host": ([_vp, _P(svo_frame_params), _P(svo_trace_cfg), _vp, _vp], ctypes.c_int),
     "svo_mm_sync": ([_vp, _vp, _P(svo_stats)], ctypes.c_int),
+    "svo_render_shadow": ([_vp, _vp, _u64, _P(svo_frame_params), _P(svo_trace_cfg), _P(svo_shadow_cfg), _vp, _vp,
+                           _vp, _vp, _vp], ctypes.c_int),
+    "svo_mm_render_shadow": ([_vp, _P(svo_frame_params), _P(svo_trace_cfg), _P(svo_shadow_cfg), _vp, _vp, _vp,
+                              _vp], ctypes.c_int),
     "svo_batcher_create": ([_u32, _u32, _P(_vp)], ctypes.c_int),
     "svo_batcher_destroy": ([_vp], None),
     "svo_batcher_set": ([_vp, _P(svo_octree_desc), _u32, _P(svo_view_desc), _u32, _P(svo_batch_cfg), _vp],
@@ -511,6 +521,15 @@ class TreeletMemoryManagerCuda:
                                      _stream_ptr(stream)), "svo_mm_render_host")
         return out
 
+    def render_shadow(self, params: svo_frame_params, rgba, shadow: svo_shadow_cfg | None = None,
+                      hits=None, shadow_hits=None, cfg: svo_trace_cfg | None = None, stream=None):
+        """Primary plus one shadow ray per hit over the incore buffer."""
+        cfg = cfg or trace_cfg()
+        shadow = shadow or shadow_cfg()
+        _check(_L.svo_mm_render_shadow(self._h, ctypes.byref(params), ctypes.byref(cfg), ctypes.byref(shadow),
+                                       _dptr(rgba), _dptr(hits), _dptr(shadow_hits), _stream_ptr(stream)),
+               "svo_mm_render_shadow")
+
     def sync(self, stream=None) -> svo_stats:
         s = svo_stats()
         _check(_L.svo_mm_sync(self._h, _stream_ptr(stream), ctypes.byref(s)), "svo_mm_sync")
@@ -535,6 +554,50 @@ def render(d_nodes, d_attribs, num_nodes: int, params: svo_frame_params, d_rgba,
     _check(_L.svo_render(_dptr(d_nodes), _dptr(d_attribs), num_nodes, ctypes.byref(params),
                          ctypes.byref(cfg), _dptr(d_rgba), _dptr(d_hits), _dptr(d_stats),
                          _stream_ptr(stream)), "svo_render")
+
+
+def default_light() -> np.ndarray:
+    """shade_diffuse_color_shadow's light (opencl/fillFrameBuffer_rgba.cl:506):
+    normalize(-0.5, 1.0, 0.6), with normalize = v / sqrt((x*x + y*y) + z*z) in FP32."""
+    v = np.array([-0.5, 1.0, 0.6], dtype=np.float32)
+    n = np.sqrt((v[0] * v[0] + v[1] * v[1]) + v[2] * v[2], dtype=np.float32)
+    return (v / n).astype(np.float32)
+
+
+def seeded_light(seed: int) -> np.ndarray:
+    """A directional light from a seed: a uniform direction on the upper
+    hemisphere (y >= 0.2), normalised in FP32 like default_light()."""
+    rng = np.random.default_rng(seed)
+    while True:
+        v = rng.normal(size=3).astype(np.float32)
+        v[1] = abs(v[1])
+        n = np.sqrt((v[0] * v[0] + v[1] * v[1]) + v[2] * v[2], dtype=np.float32)
+        if n > 1e-3 and v[1] / n >= 0.2:
+            return (v / n).astype(np.float32)
+
+
+def shadow_cfg(light=None, t_scale_ratio=0.001, normal_offset=0.01) -> svo_shadow_cfg:
+    """Shadow-ray settings; the defaults are shade_diffuse_color_shadow's
+    (light normalize(-0.5, 1, 0.6), tScaleRatio 0.001, normal offset 0.01)."""
+    c = svo_shadow_cfg()
+    light = default_light() if light is None else np.asarray(light, dtype=np.float32)
+    for i in range(3):
+        c.light_direction[i] = float(light[i])
+    c.t_scale_ratio, c.normal_offset, c.reserved = t_scale_ratio, normal_offset, 0
+    return c
+
+
+def render_shadow(d_nodes, d_attribs, num_nodes: int, params: svo_frame_params, d_rgba,
+                  shadow: svo_shadow_cfg | None = None, d_hits=None, d_shadow_hits=None,
+                  cfg: svo_trace_cfg | None = None, d_stats=None, stream=None):
+    """Primary ray plus one shadow ray per hit (shade_diffuse_color_shadow)
+    over a node pool already in device memory."""
+    cfg = cfg or trace_cfg()
+    shadow = shadow or shadow_cfg()
+    _check(_L.svo_render_shadow(_dptr(d_nodes), _dptr(d_attribs), num_nodes, ctypes.byref(params),
+                                ctypes.byref(cfg), ctypes.byref(shadow), _dptr(d_rgba), _dptr(d_hits),
+                                _dptr(d_shadow_hits), _dptr(d_stats), _stream_ptr(stream)),
+           "svo_render_shadow")
 
 
 def trace_rays(d_nodes, num_nodes: int, d_origins, d_dirs, n: int, t_scale_ratio: float,

@@ -52,6 +52,14 @@ int check_mode(int32_t mode) {
   return (mode == 0 || mode == 1 || mode == 3 || mode == 4 || mode == 5) ? SVO_OK : SVO_ERR_NOTSUP;
 }
 
+// The per-frame kernel also shades modes 2, 6 and 7; 6 and 7 need the node
+// centre and quality that only the treelet traversal reports.
+int check_frame_mode(int32_t mode, int32_t traversal) {
+  if (mode == 2) return SVO_OK;
+  if (mode == 6 || mode == 7) return traversal == SVO_TRAVERSAL_TREELET ? SVO_OK : SVO_ERR_NOTSUP;
+  return check_mode(mode);
+}
+
 int build_scene(uint32_t depth, std::vector<uint64_t>& codes, std::vector<svo_attrib>& attribs,
                 uint32_t treelet_levels, uint32_t treelet_bytes, svo_scene** out) {
   svo::Octree tree;
@@ -349,11 +357,28 @@ int svo_render(const svo_node* d_nodes, const svo_attrib* d_attribs, uint64_t nu
     return SVO_ERR_INVALID;
   int rc = check_cfg(cfg);
   if (rc != SVO_OK) return rc;
-  rc = check_mode(params->mode);
+  rc = check_frame_mode(params->mode, cfg->traversal);
   if (rc != SVO_OK) return rc;
-  if ((params->mode == 0 || params->mode == 1) && !d_attribs) return SVO_ERR_INVALID;
+  if ((params->mode == 0 || params->mode == 1 || params->mode == 6) && !d_attribs)
+    return SVO_ERR_INVALID;
   return svo::launch_render(d_nodes, d_attribs, num_nodes, *params, *cfg, d_rgba, d_hits, d_stats,
                             (cudaStream_t)stream);
+}
+
+int svo_render_shadow(const svo_node* d_nodes, const svo_attrib* d_attribs, uint64_t num_nodes,
+                      const svo_frame_params* params, const svo_trace_cfg* cfg,
+                      const svo_shadow_cfg* shadow, uint32_t* d_rgba, svo_hit* d_hits,
+                      svo_hit* d_shadow_hits, svo_stats* d_stats, void* stream) {
+  if (!params || !shadow || !d_nodes || !d_attribs || !d_rgba || num_nodes == 0 ||
+      num_nodes > 0x100000000ull)
+    return SVO_ERR_INVALID;
+  const int rc = check_cfg(cfg);
+  if (rc != SVO_OK) return rc;
+  if (cfg->traversal != SVO_TRAVERSAL_TREELET) return SVO_ERR_NOTSUP;
+  if (shadow->reserved != 0u) return SVO_ERR_INVALID;
+  return svo::launch_render_shadow(d_nodes, d_attribs, num_nodes, *params, *shadow,
+                                   cfg->stack_size, d_rgba, d_hits, d_shadow_hits, d_stats,
+                                   (cudaStream_t)stream);
 }
 
 int svo_trace_rays(const svo_node* d_nodes, uint64_t num_nodes, const float* d_origins,
@@ -376,6 +401,18 @@ int svo_mm_render(svo_mm* mm, const svo_frame_params* params, const svo_trace_cf
   if (rc != SVO_OK) return rc;
   return svo_render(mm->impl.device_nodes(), mm->impl.device_attribs(), mm->impl.incore_nodes(),
                     params, cfg, d_rgba, d_hits, mm->impl.device_stats(), s);
+}
+
+int svo_mm_render_shadow(svo_mm* mm, const svo_frame_params* params, const svo_trace_cfg* cfg,
+                         const svo_shadow_cfg* shadow, uint32_t* d_rgba, svo_hit* d_hits,
+                         svo_hit* d_shadow_hits, void* stream) {
+  if (!mm || !mm->impl.device_ready()) return SVO_ERR_INVALID;
+  cudaStream_t s = stream ? (cudaStream_t)stream : mm->impl.render_stream();
+  int rc = mm->impl.wait_uploads(s);
+  if (rc != SVO_OK) return rc;
+  return svo_render_shadow(mm->impl.device_nodes(), mm->impl.device_attribs(),
+                           mm->impl.incore_nodes(), params, cfg, shadow, d_rgba, d_hits,
+                           d_shadow_hits, mm->impl.device_stats(), s);
 }
 
 int svo_mm_render_host(svo_mm* mm, const svo_frame_params* params, const svo_trace_cfg* cfg,

@@ -19,7 +19,9 @@ constexpr int kBlockW = 16;
 constexpr int kBlockH = 16;
 constexpr int kThreads = kBlockW * kBlockH;
 
-template <bool kFlat>
+// kExt: view modes 2, 6 and 7 (shade_ext); the other modes compile without
+// the extra exit state.
+template <bool kFlat, bool kExt>
 __global__ void __launch_bounds__(kThreads) render_frame_kernel(
     const uint2* __restrict__ nodes, const uint2* __restrict__ attribs, uint64_t num_nodes,
     const svo_frame_params p, int S, uint32_t* __restrict__ rgba, svo_hit* __restrict__ hits,
@@ -36,8 +38,66 @@ __global__ void __launch_bounds__(kThreads) render_frame_kernel(
   const RayHit h = cast_ray<kFlat>(GlobalFetch{nodes}, num_nodes, o, dx, dy, dz, p.t_scale_ratio,
                                    S, stack_smem + t, kThreads);
   const uint64_t pix = (uint64_t)y * p.width + x;
-  rgba[pix] = shade(p.mode, h, attribs, num_nodes, S);
+  rgba[pix] = kExt ? shade_ext(p.mode, h, attribs, num_nodes, S, p.t_scale_ratio, dx, dy, dz)
+                   : shade(p.mode, h, attribs, num_nodes, S);
   if (hits != nullptr) store_hit(hits, pix, h);
+  count_stats(stats, h);
+}
+
+// Primary ray plus one shadow ray per hit, shaded as shade_diffuse_color_shadow
+// (opencl/fillFrameBuffer_rgba.cl:494-529) with the live renderer's attribute
+// addressing (attribute index = node index, :388-404):
+//   n = getNormal, c = getColor, nDotL = max(0, dot(n, L)),
+//   shadow = sample(nodeCenter + n * offset, L, tsr_shadow) ? 1 : 0,
+//   colour = c * nDotL * (1 - shadow) + c * 0.2, alpha 1; misses, and hits
+//   outside the pool, (0.2, 0.3, 0.2).
+// The shadow ray reuses the primary ray's stack columns.
+__global__ void __launch_bounds__(kThreads) render_shadow_kernel(
+    const uint2* __restrict__ nodes, const uint2* __restrict__ attribs, uint64_t num_nodes,
+    const svo_frame_params p, const svo_shadow_cfg sc, int S, uint32_t* __restrict__ rgba,
+    svo_hit* __restrict__ hits, svo_hit* __restrict__ shadow_hits,
+    svo_stats* __restrict__ stats) {
+  extern __shared__ uint2 stack_smem[];
+  const int t = threadIdx.x;
+  const int warp = t >> 5, lane = t & 31;
+  const uint32_t x = blockIdx.x * kBlockW + (warp & 1) * 8 + (lane & 7);
+  const uint32_t y = blockIdx.y * kBlockH + (warp >> 1) * 4 + (lane >> 3);
+  if (x >= p.width || y >= p.height) return;
+  float o[3], dx, dy, dz;
+  pixel_ray(p, x, y, o, dx, dy, dz);
+  const RayHit h = cast_ray<false>(GlobalFetch{nodes}, num_nodes, o, dx, dy, dz, p.t_scale_ratio,
+                                   S, stack_smem + t, kThreads);
+  const uint64_t pix = (uint64_t)y * p.width + x;
+  uint32_t out = pack_rgba8(0.2f, 0.3f, 0.2f, 1.0f);
+  RayHit sh;
+  sh.node = 0u;
+  sh.t = 0.0f;
+  sh.depth = sh.hit = sh.flags = sh.loops = sh.fetches = 0u;
+  if (h.hit && (uint64_t)h.node < num_nodes) {
+    {
+      const uint2 a = __ldg(attribs + h.node);
+      float nx, ny, nz, c[4];
+      unpack_normal(a.x, nx, ny, nz);
+      unpack_color(a.y, c);
+      const float lx = sc.light_direction[0], ly = sc.light_direction[1],
+                  lz = sc.light_direction[2];
+      const float ndl = cl_max(0.0f, dot3(nx, ny, nz, lx, ly, lz));
+      const float so[3] = {__fadd_rn(h.cx, __fmul_rn(nx, sc.normal_offset)),
+                           __fadd_rn(h.cy, __fmul_rn(ny, sc.normal_offset)),
+                           __fadd_rn(h.cz, __fmul_rn(nz, sc.normal_offset))};
+      sh = cast_ray<false>(GlobalFetch{nodes}, num_nodes, so, lx, ly, lz, sc.t_scale_ratio, S,
+                           stack_smem + t, kThreads);
+      const float lit = __fsub_rn(1.0f, sh.hit ? 1.0f : 0.0f);
+      float r[3];
+      for (int i = 0; i < 3; ++i)
+        r[i] = __fadd_rn(__fmul_rn(__fmul_rn(c[i], ndl), lit), __fmul_rn(c[i], 0.2f));
+      out = pack_rgba8(r[0], r[1], r[2], 1.0f);
+      count_stats(stats, sh);
+    }
+  }
+  rgba[pix] = out;
+  if (hits != nullptr) store_hit(hits, pix, h);
+  if (shadow_hits != nullptr) store_hit(shadow_hits, pix, sh);
   count_stats(stats, h);
 }
 
@@ -69,12 +129,34 @@ int launch_render(const svo_node* nodes, const svo_attrib* attribs, uint64_t num
   const size_t smem = render_smem_bytes(S);
   const uint2* n2 = reinterpret_cast<const uint2*>(nodes);
   const uint2* a2 = reinterpret_cast<const uint2*>(attribs);
-  if (cfg.traversal == SVO_TRAVERSAL_FLAT)
-    render_frame_kernel<true><<<grid, kThreads, smem, stream>>>(n2, a2, num_nodes, p, S, rgba,
-                                                                hits, stats);
-  else
-    render_frame_kernel<false><<<grid, kThreads, smem, stream>>>(n2, a2, num_nodes, p, S, rgba,
-                                                                 hits, stats);
+  const bool ext = p.mode == 2 || p.mode == 6 || p.mode == 7;
+  if (cfg.traversal == SVO_TRAVERSAL_FLAT) {
+    if (ext)
+      render_frame_kernel<true, true><<<grid, kThreads, smem, stream>>>(n2, a2, num_nodes, p, S,
+                                                                        rgba, hits, stats);
+    else
+      render_frame_kernel<true, false><<<grid, kThreads, smem, stream>>>(n2, a2, num_nodes, p, S,
+                                                                         rgba, hits, stats);
+  } else {
+    if (ext)
+      render_frame_kernel<false, true><<<grid, kThreads, smem, stream>>>(n2, a2, num_nodes, p, S,
+                                                                         rgba, hits, stats);
+    else
+      render_frame_kernel<false, false><<<grid, kThreads, smem, stream>>>(n2, a2, num_nodes, p, S,
+                                                                          rgba, hits, stats);
+  }
+  return cudaGetLastError() == cudaSuccess ? SVO_OK : SVO_ERR_CUDA;
+}
+
+int launch_render_shadow(const svo_node* nodes, const svo_attrib* attribs, uint64_t num_nodes,
+                         const svo_frame_params& p, const svo_shadow_cfg& sc, int S,
+                         uint32_t* rgba, svo_hit* hits, svo_hit* shadow_hits, svo_stats* stats,
+                         cudaStream_t stream) {
+  if (p.width == 0 || p.height == 0) return SVO_OK;
+  const dim3 grid((p.width + kBlockW - 1) / kBlockW, (p.height + kBlockH - 1) / kBlockH);
+  render_shadow_kernel<<<grid, kThreads, render_smem_bytes(S), stream>>>(
+      reinterpret_cast<const uint2*>(nodes), reinterpret_cast<const uint2*>(attribs), num_nodes, p,
+      sc, S, rgba, hits, shadow_hits, stats);
   return cudaGetLastError() == cudaSuccess ? SVO_OK : SVO_ERR_CUDA;
 }
 

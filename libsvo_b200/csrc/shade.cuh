@@ -8,8 +8,9 @@
 
 namespace svo {
 
+// float -> unsigned 8-bit normalised: round(clamp(c, 0, 1) * 255), NaN -> 0.
 __device__ __forceinline__ uint32_t to_unorm8(float c) {
-  c = c < 0.0f ? 0.0f : (c > 1.0f ? 1.0f : c);
+  c = c > 0.0f ? (c < 1.0f ? c : 1.0f) : 0.0f;
   return __float2uint_rz(__fadd_rn(__fmul_rn(c, 255.0f), 0.5f));
 }
 
@@ -54,6 +55,138 @@ __device__ __forceinline__ uint32_t shade(int mode, const RayHit& h,
     default:
       return pack_rgba8(0.0f, 0.0f, 0.0f, 1.0f);
   }
+}
+
+// OpenCL dot() and normalize() pinned to (x*x + y*y) + z*z and v / sqrt(dot).
+__device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz) {
+  return __fadd_rn(__fadd_rn(__fmul_rn(ax, bx), __fmul_rn(ay, by)), __fmul_rn(az, bz));
+}
+__device__ __forceinline__ void normalize3(float& x, float& y, float& z) {
+  const float l = __fsqrt_rn(dot3(x, y, z, x, y, z));
+  x = __fdiv_rn(x, l);
+  y = __fdiv_rn(y, l);
+  z = __fdiv_rn(z, l);
+}
+
+// getNormal / getColor (opencl/treeletRenderer_rgba.cl:388-404).
+__device__ __forceinline__ void unpack_normal(uint32_t v, float& x, float& y, float& z) {
+  const float k = 0.003921569f;
+  x = __fmul_rn(__fsub_rn(__fmul_rn((float)(v >> 24), k), 0.5f), 2.0f);
+  y = __fmul_rn(__fsub_rn(__fmul_rn((float)((v >> 16) & 255u), k), 0.5f), 2.0f);
+  z = __fmul_rn(__fsub_rn(__fmul_rn((float)((v >> 8) & 255u), k), 0.5f), 2.0f);
+}
+__device__ __forceinline__ void unpack_color(uint32_t v, float c[4]) {
+  const float k = 0.003921569f;
+  c[0] = __fmul_rn((float)(v >> 24), k);
+  c[1] = __fmul_rn((float)((v >> 16) & 255u), k);
+  c[2] = __fmul_rn((float)((v >> 8) & 255u), k);
+  c[3] = __fmul_rn((float)(v & 255u), k);
+}
+
+// smoothstep(0, 1, x) with t = clamp(x, 0, 1) and t * t * (3 - 2t) in that order.
+__device__ __forceinline__ float smoothstep01(float x) {
+  const float t = x < 0.0f ? 0.0f : (x > 1.0f ? 1.0f : x);
+  return __fmul_rn(__fmul_rn(t, t), __fsub_rn(3.0f, __fmul_rn(2.0f, t)));
+}
+
+// Adjust (opencl/treeletRenderer_rgba.cl:518-528).  Gamma is the double
+// literal 0.80, so the power and the scaling by 255 run in double.
+__device__ __forceinline__ float wl_adjust(float color, float factor) {
+  if (color == 0.0f) return 0.0f;
+  const int res = (int)round(255.0 * pow((double)__fmul_rn(color, factor), 0.80));
+  return (float)(res < 0 ? 0 : (res > 255 ? 255 : res));
+}
+
+// DataPointToColor(value, 0, vmax) (opencl/treeletRenderer_rgba.cl:532-603):
+// the value mapped to a visible wavelength, then to RGB.
+__device__ __forceinline__ void wavelength_color(float value, float vmax, float rgb[3]) {
+  const float w = __fadd_rn(__fmul_rn(__fdiv_rn(__fsub_rn(value, 0.0f), __fsub_rn(vmax, 0.0f)), 400.0f),
+                            380.0f);
+  float r, g, b, f;
+  if (380.0f <= w && w <= 440.0f) {
+    r = __fdiv_rn(-__fsub_rn(w, 440.0f), 60.0f);
+    g = 0.0f;
+    b = 1.0f;
+  } else if (440.0f < w && w <= 490.0f) {
+    r = 0.0f;
+    g = __fdiv_rn(__fsub_rn(w, 440.0f), 50.0f);
+    b = 1.0f;
+  } else if (490.0f < w && w <= 510.0f) {
+    r = 0.0f;
+    g = 1.0f;
+    b = __fdiv_rn(-__fsub_rn(w, 510.0f), 20.0f);
+  } else if (510.0f < w && w <= 580.0f) {
+    r = __fdiv_rn(__fsub_rn(w, 510.0f), 70.0f);
+    g = 1.0f;
+    b = 0.0f;
+  } else if (580.0f < w && w <= 645.0f) {
+    r = 1.0f;
+    g = __fdiv_rn(-__fsub_rn(w, 645.0f), 65.0f);
+    b = 0.0f;
+  } else if (645.0f < w && w <= 780.0f) {
+    r = 1.0f;
+    g = 0.0f;
+    b = 0.0f;
+  } else {
+    r = g = b = 0.0f;
+  }
+  if (380.0f <= w && w <= 420.0f)
+    f = __fadd_rn(0.3f, __fdiv_rn(__fmul_rn(0.7f, __fsub_rn(w, 380.0f)), 40.0f));
+  else if (420.0f < w && w <= 701.0f)
+    f = 1.0f;
+  else if (701.0f < w && w <= 780.0f)
+    f = __fadd_rn(0.3f, __fdiv_rn(__fmul_rn(0.7f, __fsub_rn(780.0f, w)), 79.0f));
+  else
+    f = 0.0f;
+  const float fac = __fdiv_rn(1.0f, 255.0f);
+  rgb[0] = __fmul_rn(wl_adjust(r, f), fac);
+  rgb[1] = __fmul_rn(wl_adjust(g, f), fac);
+  rgb[2] = __fmul_rn(wl_adjust(b, f), fac);
+}
+
+// The view modes that need more than the hit record: 2 (iteration count as a
+// wavelength colour), 6 (shade_phong, :451-504, whose shadow ray is compiled
+// out in the reference) and 7 (LOD quality, :715-733).  d is the unclamped
+// primary direction.  Modes 6 and 7 use the node centre and the quality that
+// only the treelet traversal reports.
+__device__ __forceinline__ uint32_t shade_ext(int mode, const RayHit& h,
+                                              const uint2* __restrict__ attribs,
+                                              uint64_t num_nodes, int S, float tsr, float dx,
+                                              float dy, float dz) {
+  if (mode == 2) {
+    float rgb[3];
+    wavelength_color((float)h.loops, (float)(S * 30), rgb);
+    return pack_rgba8(rgb[0], rgb[1], rgb[2], 1.0f);
+  }
+  if (mode == 7) {
+    if (!h.hit) return pack_rgba8(0.6f, 0.3f, 0.3f, 1.0f);
+    const float q = h.leaf ? __fsub_rn(h.sx2, __fmul_rn(tsr, h.tc_min)) : 0.0f;
+    const float v = __fsqrt_rn(__fsqrt_rn(q));
+    return pack_rgba8(v, v, v, 1.0f);
+  }
+  // mode 6
+  if (!h.hit) return pack_rgba8(0.4f, 0.6f, 0.4f, 1.0f);
+  if ((uint64_t)h.node >= num_nodes) return pack_rgba8(0.0f, 0.0f, 0.0f, 1.0f);
+  const uint2 a = __ldg(attribs + h.node);
+  float nx, ny, nz, c[4];
+  unpack_normal(a.x, nx, ny, nz);
+  normalize3(nx, ny, nz);
+  unpack_color(a.y, c);
+  float lx = __fsub_rn(-120.0f, h.cx), ly = __fsub_rn(0.0f, h.cy), lz = __fsub_rn(0.0f, h.cz);
+  normalize3(lx, ly, lz);
+  const float ndl = cl_max(0.0f, dot3(nx, ny, nz, lx, ly, lz));
+  float rfx = __fsub_rn(__fmul_rn(__fmul_rn(2.0f, nx), ndl), lx);
+  float rfy = __fsub_rn(__fmul_rn(__fmul_rn(2.0f, ny), ndl), ly);
+  float rfz = __fsub_rn(__fmul_rn(__fmul_rn(2.0f, nz), ndl), lz);
+  normalize3(rfx, rfy, rfz);
+  const float rdv = cl_max(0.0f, dot3(rfx, rfy, rfz, -dx, -dy, -dz));
+  const float spec = __fmul_rn(cl_max(0.0f, powf(rdv, 10.0f)), ndl > 0.0f ? 1.0f : 0.0f);
+  // shadow = 1 - 0: color * 0.5 + (color * nDotL * 1 + specular * 1 * 0.2) * 0.5
+  const float s = __fmul_rn(spec, 0.2f);
+  float o[3];
+  for (int i = 0; i < 3; ++i)
+    o[i] = smoothstep01(__fadd_rn(__fmul_rn(c[i], 0.5f), __fmul_rn(__fadd_rn(__fmul_rn(c[i], ndl), s), 0.5f)));
+  return pack_rgba8(o[0], o[1], o[2], 1.0f);
 }
 
 __device__ __forceinline__ void store_hit(svo_hit* hits, uint64_t i, const RayHit& h) {

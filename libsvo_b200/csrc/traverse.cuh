@@ -41,11 +41,16 @@ struct RayHit {
   uint32_t flags;
   uint32_t loops;
   uint32_t fetches;  // loop iterations that read the parent node
-  // set on a leaf or LOD stop, for the analysis pass: the hit child's entry
-  // distance, the child size, and whether the child was a leaf
+  // set on a leaf or LOD stop, for the analysis pass and the quality view:
+  // the hit child's entry distance, the child size, and whether the child was
+  // a leaf (the watchdog stop sets tMin, the current size and leaf = 1, so
+  // that quality = sx2 - tScaleRatio * tc_min holds for both)
   float tc_min;
   float sx2;
   uint32_t leaf;
+  // SampleResult.nodeCenter: the hit child's centre, or the current node's
+  // when the watchdog ends the ray (shadow rays start there)
+  float cx, cy, cz;
 };
 
 __device__ __forceinline__ float cl_max(float a, float b) { return (a < b) ? b : a; }
@@ -157,6 +162,13 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
         h.node = node;
         h.depth = (uint32_t)(S - scale);
         h.t = tmin;
+        h.cx = cx;
+        h.cy = cy;
+        h.cz = cz;
+        // quality = scale_exp2 - tScaleRatio * tMin, as for a leaf
+        h.tc_min = tmin;
+        h.sx2 = sx2;
+        h.leaf = 1u;
       }
       return;
     }
@@ -257,6 +269,9 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
         h.tc_min = tc_min;
         h.sx2 = sx2;
         h.leaf = leaf ? 1u : 0u;
+        h.cx = __fadd_rn(fbx != 0.0f ? half : -half, cx);
+        h.cy = __fadd_rn(fby != 0.0f ? half : -half, cy);
+        h.cz = __fadd_rn(fbz != 0.0f ? half : -half, cz);
         return;
       }
       if (kFlat && scale == 0) {  // non-leaf below the octree's depth: corrupt pool
@@ -309,6 +324,9 @@ __device__ __forceinline__ RayHit cast_ray(const Fetch& fetch, uint64_t num_node
   h.tc_min = 0.0f;
   h.sx2 = 0.0f;
   h.leaf = 0u;
+  h.cx = 0.0f;
+  h.cy = 0.0f;
+  h.cz = 0.0f;
 
   float t_min, t_max;
   {

@@ -77,6 +77,8 @@ def lib():
         L.oracle_pixel_rays.restype = None
         L.oracle_feedback.argtypes = [vp, u64, vp, i32, vp, vp, i32]
         L.oracle_feedback.restype = None
+        L.oracle_render_shadow.argtypes = [vp, vp, u64, vp, i32, vp, f32, f32, vp, vp, vp, vp, i32]
+        L.oracle_render_shadow.restype = u64
         assert L.oracle_hit_record_size() == 16
         _lib = L
     return _lib
@@ -99,6 +101,8 @@ def reference_lib():
         L.ref_render_rows.restype = None
         L.ref_feedback.argtypes = [vp, vp, vp, vp, i32]
         L.ref_feedback.restype = None
+        L.ref_render_shadow.argtypes = [vp, vp, vp, vp, f32, f32, vp, vp, i32]
+        L.ref_render_shadow.restype = None
         assert L.ref_hit_record_size() == 16
         _ref = L
     return _ref
@@ -186,8 +190,10 @@ def reference_render(nodes, attribs, params: bytes, threads=None, rows=None):
 
 
 def to_rgba8(rgbaf: np.ndarray) -> np.ndarray:
-    """float RGBA -> packed RGBA8 (byte 0 red), round(clamp(c, 0, 1) * 255) in FP32."""
-    c = np.clip(rgbaf.astype(np.float32), np.float32(0), np.float32(1))
+    """float RGBA -> packed RGBA8 (byte 0 red), round(clamp(c, 0, 1) * 255) in
+    FP32, NaN -> 0."""
+    c = rgbaf.astype(np.float32)
+    c = np.clip(np.where(np.isnan(c), np.float32(0), c), np.float32(0), np.float32(1))
     b = np.floor(c * np.float32(255.0) + np.float32(0.5)).astype(np.uint32)
     return b[..., 0] | (b[..., 1] << 8) | (b[..., 2] << 16) | (b[..., 3] << 24)
 
@@ -218,3 +224,51 @@ def reference_feedback(nodes, params: bytes, threads=None):
     pbuf = np.frombuffer(bytearray(params), dtype=np.uint8)
     L.ref_feedback(_ptr(nodes), _ptr(pbuf), _ptr(rec), _ptr(rgbaf), _threads(threads))
     return rec, rgbaf
+
+
+# Light direction of shade_diffuse_color_shadow (opencl/fillFrameBuffer_rgba.cl:
+# 506): normalize(-0.5, 1.0, 0.6) with normalize = v / sqrt((x*x + y*y) + z*z).
+def default_light():
+    v = np.array([-0.5, 1.0, 0.6], dtype=np.float32)
+    l = np.sqrt((v[0] * v[0] + v[1] * v[1]) + v[2] * v[2], dtype=np.float32)
+    return (v / l).astype(np.float32)
+
+
+def render_shadow(nodes, attribs, params: bytes, light, shadow_tsr: float = 0.001,
+                  offset: float = 0.01, stack_size: int = 13,
+                  want_rgbaf: bool = False, threads=None):
+    """Primary plus shadow rays on the CPU.  Returns (rgba8 [H, W], hits [H, W],
+    shadow_hits [H, W], node_fetches, rgbaf or None)."""
+    nodes = np.ascontiguousarray(nodes, dtype=np.uint32)
+    attribs = np.ascontiguousarray(attribs, dtype=np.uint32)
+    light = np.ascontiguousarray(light, dtype=np.float32)
+    w, h = np.frombuffer(params[:8], dtype=np.uint32)
+    pbuf = np.frombuffer(bytearray(params), dtype=np.uint8)
+    rgba = np.zeros((h, w), dtype=np.uint32)
+    hits = np.zeros((h, w), dtype=HIT_DTYPE)
+    shits = np.zeros((h, w), dtype=HIT_DTYPE)
+    rgbaf = np.zeros((h, w, 4), dtype=np.float32) if want_rgbaf else None
+    fetches = lib().oracle_render_shadow(
+        _ptr(nodes), _ptr(attribs), nodes.shape[0], _ptr(pbuf), int(stack_size), _ptr(light),
+        float(shadow_tsr), float(offset), _ptr(rgba),
+        _ptr(rgbaf) if want_rgbaf else None, _ptr(hits), _ptr(shits), _threads(threads))
+    return rgba, hits, shits, int(fetches), rgbaf
+
+
+def reference_render_shadow(nodes, attribs, params: bytes, light, shadow_tsr: float = 0.001,
+                            offset: float = 0.01, threads=None):
+    """The shadow shading over the reference's own sample(): (rgbaf [H, W, 4],
+    shadow_hits [H, W])."""
+    L = reference_lib()
+    if L is None:
+        return None
+    nodes = np.ascontiguousarray(nodes, dtype=np.uint32)
+    attribs = np.ascontiguousarray(attribs, dtype=np.uint32)
+    light = np.ascontiguousarray(light, dtype=np.float32)
+    w, h = np.frombuffer(params[:8], dtype=np.uint32)
+    out = np.zeros((h, w, 4), dtype=np.float32)
+    shits = np.zeros((h, w), dtype=HIT_DTYPE)
+    pbuf = np.frombuffer(bytearray(params), dtype=np.uint8)
+    L.ref_render_shadow(_ptr(nodes), _ptr(attribs), _ptr(pbuf), _ptr(light), float(shadow_tsr),
+                        float(offset), _ptr(out), _ptr(shits), _threads(threads))
+    return out, shits

@@ -111,11 +111,17 @@ struct RayCount {
   uint64_t fetches = 0;
 };
 
+// The rest of SampleResult on a hit: nodeCenter and quality.
+struct Exit {
+  V3 center{0.0f, 0.0f, 0.0f};
+  float quality = 0.0f;
+};
+
 // sample() (opencl/treeletRenderer_rgba.cl:201-382), stack size `S`
 // (MAX_STACK_SIZE, 13 in the reference) and maximum descent depth S-1
-// (MAX_SVO_RAYCAST_DEPTH).
+// (MAX_SVO_RAYCAST_DEPTH).  `out` (optional) receives nodeCenter and quality.
 Hit cast_treelet(const uint32_t* nodes, uint64_t num_nodes, V3 o, V3 d, float tsr, int S,
-                 RayCount& rc) {
+                 RayCount& rc, Exit* out = nullptr) {
   Hit h{};
   float t_min, t_max;
   if (!root_slab(o, d, t_min, t_max)) {
@@ -153,6 +159,7 @@ Hit cast_treelet(const uint32_t* nodes, uint64_t num_nodes, V3 o, V3 d, float ts
       h.loops = (uint16_t)loops;
       h.fetches = (uint16_t)fetches;
       h.flags = kFlagCapped;
+      if (out) *out = Exit{p.center, sx2 - tsr * p.tmin};
       return h;
     }
     if (p.tmax < 0.0f) {
@@ -198,6 +205,7 @@ Hit cast_treelet(const uint32_t* nodes, uint64_t num_nodes, V3 o, V3 d, float ts
         h.t = p.tmin;
         h.loops = (uint16_t)loops;
         h.fetches = (uint16_t)fetches;
+        if (out) *out = Exit{cc, sx2 - tsr * tc_min};
         return h;
       }
       if (tsr * tc_min > sx2 || scale_max - scale == scale_max - 1) {
@@ -207,6 +215,7 @@ Hit cast_treelet(const uint32_t* nodes, uint64_t num_nodes, V3 o, V3 d, float ts
         h.t = p.tmin;
         h.loops = (uint16_t)loops;
         h.fetches = (uint16_t)fetches;
+        if (out) *out = Exit{cc, 0.0f};
         return h;
       }
       p.tmin = tc_max;
@@ -469,9 +478,9 @@ inline void pixel_ray(const FrameParams& fp, uint32_t x, uint32_t y, V3& o, V3& 
   o = V3{fp.cam[0], fp.cam[1], fp.cam[2]};
 }
 
-// float -> unsigned 8-bit normalised: round(clamp(c, 0, 1) * 255).
+// float -> unsigned 8-bit normalised: round(clamp(c, 0, 1) * 255), NaN -> 0.
 inline uint32_t to_unorm8(float c) {
-  c = c < 0.0f ? 0.0f : (c > 1.0f ? 1.0f : c);
+  c = c > 0.0f ? (c < 1.0f ? c : 1.0f) : 0.0f;
   return (uint32_t)(c * 255.0f + 0.5f);
 }
 inline uint32_t pack_rgba8(float r, float g, float b, float a) {
@@ -487,13 +496,138 @@ inline void unpack_rgba(uint32_t v, float out[4]) {
   out[0] = (float)((v >> 24) & 255u);
 }
 
+inline float dot3(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+inline V3 normalize3(V3 v) {
+  const float l = std::sqrt(dot3(v, v));
+  return V3{v.x / l, v.y / l, v.z / l};
+}
+
+// getNormal (opencl/treeletRenderer_rgba.cl:388-393).
+inline V3 get_normal(uint32_t packed) {
+  const float k = 0.003921569f;
+  float c[4];
+  unpack_rgba(packed, c);
+  return V3{(c[0] * k - 0.5f) * 2.0f, (c[1] * k - 0.5f) * 2.0f, (c[2] * k - 0.5f) * 2.0f};
+}
+
+// smoothstep(0, 1, x): t = clamp((x - 0) / (1 - 0), 0, 1), t * t * (3 - 2t).
+inline float smoothstep01(float x) {
+  const float t = x < 0.0f ? 0.0f : (x > 1.0f ? 1.0f : x);
+  return t * t * (3.0f - 2.0f * t);
+}
+
+// Adjust (opencl/treeletRenderer_rgba.cl:518-528): Gamma is the double
+// literal 0.80, so the power and the scaling by 255 run in double.
+inline float wl_adjust(float color, float factor) {
+  if (color == 0.0f) return 0.0f;
+  const int res = (int)std::round(255.0 * std::pow((double)(color * factor), 0.80));
+  return (float)std::min(255, std::max(0, res));
+}
+
+// DataPointToColor(value, 0, vmax) (opencl/treeletRenderer_rgba.cl:532-603).
+void wavelength_color(float value, float vmax, float rgb[3]) {
+  const float w = (value - 0.0f) / (vmax - 0.0f) * (780.0f - 380.0f) + 380.0f;
+  float r, g, b, f;
+  if (380.0f <= w && w <= 440.0f) {
+    r = -(w - 440.0f) / (440.0f - 380.0f);
+    g = 0.0f;
+    b = 1.0f;
+  } else if (440.0f < w && w <= 490.0f) {
+    r = 0.0f;
+    g = (w - 440.0f) / (490.0f - 440.0f);
+    b = 1.0f;
+  } else if (490.0f < w && w <= 510.0f) {
+    r = 0.0f;
+    g = 1.0f;
+    b = -(w - 510.0f) / (510.0f - 490.0f);
+  } else if (510.0f < w && w <= 580.0f) {
+    r = (w - 510.0f) / (580.0f - 510.0f);
+    g = 1.0f;
+    b = 0.0f;
+  } else if (580.0f < w && w <= 645.0f) {
+    r = 1.0f;
+    g = -(w - 645.0f) / (645.0f - 580.0f);
+    b = 0.0f;
+  } else if (645.0f < w && w <= 780.0f) {
+    r = 1.0f;
+    g = 0.0f;
+    b = 0.0f;
+  } else {
+    r = g = b = 0.0f;
+  }
+  if (380.0f <= w && w <= 420.0f)
+    f = 0.3f + 0.7f * (w - 380.0f) / (420.0f - 380.0f);
+  else if (420.0f < w && w <= 701.0f)
+    f = 1.0f;
+  else if (701.0f < w && w <= 780.0f)
+    f = 0.3f + 0.7f * (780.0f - w) / (780.0f - 701.0f);
+  else
+    f = 0.0f;
+  const float fac = 1.0f / 255.0f;
+  rgb[0] = wl_adjust(r, f) * fac;
+  rgb[1] = wl_adjust(g, f) * fac;
+  rgb[2] = wl_adjust(b, f) * fac;
+}
+
+// shade_phong (opencl/treeletRenderer_rgba.cl:451-504; its shadow ray is
+// compiled out, so shadow = 1 - 0).  d is the unclamped primary direction.
+void shade_phong(const Hit& h, const Exit& ex, V3 d, const uint32_t* attribs, uint64_t num_nodes,
+                 float rgba[4]) {
+  if (!h.hit) {
+    rgba[0] = 0.4f;
+    rgba[1] = 0.6f;
+    rgba[2] = 0.4f;
+    rgba[3] = 1.0f;
+    return;
+  }
+  if (h.node >= num_nodes) {  // outside the pool: the reference reads out of bounds
+    rgba[0] = rgba[1] = rgba[2] = 0.0f;
+    rgba[3] = 1.0f;
+    return;
+  }
+  const float k = 0.003921569f;
+  const V3 n = normalize3(get_normal(attribs[2 * (uint64_t)h.node]));
+  float c[4];
+  unpack_rgba(attribs[2 * (uint64_t)h.node + 1], c);
+  for (float& v : c) v = v * k;
+  const V3 l = normalize3(V3{-120.0f - ex.center.x, 0.0f - ex.center.y, 0.0f - ex.center.z});
+  const float ndl = cl_max(0.0f, dot3(n, l));
+  const V3 rf = normalize3(V3{((2.0f * n.x) * ndl) - l.x, ((2.0f * n.y) * ndl) - l.y,
+                              ((2.0f * n.z) * ndl) - l.z});
+  const float rdv = cl_max(0.0f, dot3(rf, V3{-d.x, -d.y, -d.z}));
+  const float spec = cl_max(0.0f, std::pow(rdv, 10.0f)) * (float)(ndl > 0.0f);
+  const float shadow = 1.0f - 0.0f;
+  for (int i = 0; i < 3; ++i)
+    rgba[i] = smoothstep01(c[i] * 0.5f + ((c[i] * ndl) * shadow + (spec * shadow) * 0.2f) * 0.5f);
+  rgba[3] = 1.0f;
+}
+
 // Fragment colour for view mode `mode` (renderToBuffer's switch,
-// opencl/treeletRenderer_rgba.cl:644-694): 0 colour, 1 normal, 3 octree depth,
-// 4 pixel depth, 5 iteration count.
+// opencl/treeletRenderer_rgba.cl:644-734): 0 colour, 1 normal, 2 iteration
+// count as a wavelength colour, 3 octree depth, 4 pixel depth, 5 iteration
+// count, 6 Phong, 7 LOD quality.  `ex` and `d` are used by modes 6 and 7.
 void shade(int mode, const Hit& h, const uint32_t* attribs, uint64_t num_nodes, int S,
-           float rgba[4]) {
+           float rgba[4], const Exit& ex = Exit{}, V3 d = V3{0.0f, 0.0f, 0.0f}) {
   const float k = 0.003921569f;
   switch (mode) {
+    case 2:
+      wavelength_color((float)h.loops, (float)(S * 30), rgba);
+      rgba[3] = 1.0f;
+      return;
+    case 6:
+      shade_phong(h, ex, d, attribs, num_nodes, rgba);
+      return;
+    case 7:
+      if (h.hit) {
+        const float q = std::sqrt(std::sqrt(ex.quality));
+        rgba[0] = rgba[1] = rgba[2] = q;
+      } else {
+        rgba[0] = 0.6f;
+        rgba[1] = 0.3f;
+        rgba[2] = 0.3f;
+      }
+      rgba[3] = 1.0f;
+      return;
     case 0:
     case 1:
       if (h.hit && h.node < num_nodes) {
@@ -542,8 +676,9 @@ void shade(int mode, const Hit& h, const uint32_t* attribs, uint64_t num_nodes, 
 }
 
 inline Hit cast_any(int flat, const uint32_t* nodes, uint64_t n, V3 o, V3 d, float tsr, int S,
-                    RayCount& rc) {
-  return flat ? cast_flat(nodes, n, o, d, tsr, S, rc) : cast_treelet(nodes, n, o, d, tsr, S, rc);
+                    RayCount& rc, Exit* ex = nullptr) {
+  return flat ? cast_flat(nodes, n, o, d, tsr, S, rc)
+              : cast_treelet(nodes, n, o, d, tsr, S, rc, ex);
 }
 
 template <class Fn>
@@ -587,16 +722,72 @@ uint64_t oracle_render(const uint32_t* nodes, const uint32_t* attribs, uint64_t 
     for (uint32_t x = 0; x < fp.width; ++x) {
       V3 o, d;
       pixel_ray(fp, x, y, o, d);
-      const Hit h = cast_any(flat, nodes, num_nodes, o, d, fp.t_scale_ratio, S, rc);
+      Exit ex;
+      const Hit h = cast_any(flat, nodes, num_nodes, o, d, fp.t_scale_ratio, S, rc, &ex);
       rc.fetches += h.fetches;
       const uint64_t pix = (uint64_t)y * fp.width + x;
       if (hrec) hrec[pix] = h;
       if (rgba8 || rgbaf) {
         float c[4];
-        shade(fp.mode, h, attribs, num_nodes, S, c);
+        shade(fp.mode, h, attribs, num_nodes, S, c, ex, d);
         if (rgba8) rgba8[pix] = pack_rgba8(c[0], c[1], c[2], c[3]);
         if (rgbaf) std::memcpy(rgbaf + 4 * pix, c, sizeof(c));
       }
+    }
+    total.fetch_add(rc.fetches, std::memory_order_relaxed);
+  });
+  return total.load();
+}
+
+// Primary ray plus one shadow ray per hit (treelet traversal), shaded as
+// shade_diffuse_color_shadow (opencl/fillFrameBuffer_rgba.cl:494-529) with the
+// live renderer's attribute index (= node index):
+//   n = getNormal, c = getColor, nDotL = max(0, dot(n, L)),
+//   shadow = sample(nodeCenter + n * offset, L, shadow_tsr) ? 1 : 0,
+//   colour = c * nDotL * (1 - shadow) + c * 0.2, alpha 1; misses and hits
+//   outside the pool (0.2, 0.3, 0.2).
+// light: the unit direction toward the light, used as given.  Outputs as in
+// oracle_render, plus shadow_hits (zeros where no shadow ray was cast).
+// Returns the node fetches of both ray kinds.
+uint64_t oracle_render_shadow(const uint32_t* nodes, const uint32_t* attribs, uint64_t num_nodes,
+                              const void* params, int S, const float* light, float shadow_tsr,
+                              float offset, uint32_t* rgba8, float* rgbaf,
+                              void* hits, void* shadow_hits, int threads) {
+  const FrameParams& fp = *(const FrameParams*)params;
+  std::atomic<uint64_t> total{0};
+  Hit* hrec = (Hit*)hits;
+  Hit* srec = (Hit*)shadow_hits;
+  const V3 l{light[0], light[1], light[2]};
+  parallel_lines(fp.height, 4, threads, [&](uint32_t y) {
+    RayCount rc;
+    for (uint32_t x = 0; x < fp.width; ++x) {
+      V3 o, d;
+      pixel_ray(fp, x, y, o, d);
+      Exit ex;
+      const Hit h = cast_treelet(nodes, num_nodes, o, d, fp.t_scale_ratio, S, rc, &ex);
+      rc.fetches += h.fetches;
+      Hit sh{};
+      float c[4] = {0.2f, 0.3f, 0.2f, 1.0f};
+      if (h.hit && h.node < num_nodes) {
+        const V3 n = get_normal(attribs[2 * (uint64_t)h.node]);
+        float col[4];
+        unpack_rgba(attribs[2 * (uint64_t)h.node + 1], col);
+        const float k = 0.003921569f;
+        for (float& v : col) v = v * k;
+        const float ndl = cl_max(0.0f, dot3(n, l));
+        const V3 so{ex.center.x + n.x * offset, ex.center.y + n.y * offset,
+                    ex.center.z + n.z * offset};
+        sh = cast_treelet(nodes, num_nodes, so, l, shadow_tsr, S, rc);
+        rc.fetches += sh.fetches;
+        const float shadow = sh.hit ? 1.0f : 0.0f;
+        for (int i = 0; i < 3; ++i) c[i] = col[i] * ndl * (1.0f - shadow) + col[i] * 0.2f;
+        c[3] = 1.0f;
+      }
+      const uint64_t pix = (uint64_t)y * fp.width + x;
+      if (hrec) hrec[pix] = h;
+      if (srec) srec[pix] = sh;
+      if (rgba8) rgba8[pix] = pack_rgba8(c[0], c[1], c[2], c[3]);
+      if (rgbaf) std::memcpy(rgbaf + 4 * pix, c, sizeof(c));
     }
     total.fetch_add(rc.fetches, std::memory_order_relaxed);
   });

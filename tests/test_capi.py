@@ -45,9 +45,25 @@ def test_null_arguments_are_status_codes():
     assert lib.svo_render(1, 1, 1, ctypes.byref(p), ctypes.byref(cfg), 1, None, None, None) == L.SVO_ERR_RANGE
     cfg = L.trace_cfg(traversal=7)
     assert lib.svo_render(1, 1, 1, ctypes.byref(p), ctypes.byref(cfg), 1, None, None, None) == L.SVO_ERR_NOTSUP
-    p.mode = 2
+    p.mode = 8
     cfg = L.trace_cfg()
     assert lib.svo_render(1, 1, 1, ctypes.byref(p), ctypes.byref(cfg), 1, None, None, None) == L.SVO_ERR_NOTSUP
+    p.mode = 6  # Phong and quality need the treelet traversal's node centre and quality
+    cfg = L.trace_cfg(traversal=L.TRAVERSAL_FLAT, stack_size=8)
+    assert lib.svo_render(1, 1, 1, ctypes.byref(p), ctypes.byref(cfg), 1, None, None, None) == L.SVO_ERR_NOTSUP
+    sc = L.shadow_cfg()
+    assert lib.svo_render_shadow(1, 1, 1, ctypes.byref(p), ctypes.byref(cfg), ctypes.byref(sc), 1, None, None, None,
+                                 None) == L.SVO_ERR_NOTSUP
+    cfg = L.trace_cfg()
+    assert lib.svo_render_shadow(1, None, 1, ctypes.byref(p), ctypes.byref(cfg), ctypes.byref(sc), 1, None, None,
+                                 None, None) == L.SVO_ERR_INVALID
+    assert lib.svo_render_shadow(1, 1, 1, ctypes.byref(p), ctypes.byref(cfg), None, 1, None, None, None,
+                                 None) == L.SVO_ERR_INVALID
+    sc.reserved = 1
+    assert lib.svo_render_shadow(1, 1, 1, ctypes.byref(p), ctypes.byref(cfg), ctypes.byref(sc), 1, None, None, None,
+                                 None) == L.SVO_ERR_INVALID
+    assert lib.svo_mm_render_shadow(None, ctypes.byref(p), ctypes.byref(cfg), ctypes.byref(sc), 1, None, None,
+                                    None) == L.SVO_ERR_INVALID
 
 
 def test_manager_without_device_buffer_rejects_renders(menger_scene):

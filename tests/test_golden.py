@@ -50,3 +50,14 @@ def test_oracle_reproduces_reference_outputs(path):
         assert np.array_equal(rec.view(np.uint8).reshape(-1), z[f"fb_rec_{k}"].reshape(-1)), f"feedback {k}"
         assert np.array_equal(img.view(np.uint32), z[f"fb_img_{k}"].view(np.uint32))
         k += 1
+    k = 0
+    while f"sh_params_{k}" in z:
+        _, _, shits, _, rgbaf = oracle.render_shadow(
+            nodes, attribs, z[f"sh_params_{k}"].tobytes(), z[f"sh_light_{k}"], float(z[f"sh_tsr_{k}"]),
+            float(z[f"sh_offset_{k}"]), want_rgbaf=True)
+        assert np.array_equal(rgbaf.view(np.uint32), z[f"sh_rgbaf_{k}"].view(np.uint32)), f"shadow frame {k}"
+        want = z[f"sh_hits_{k}"].view(oracle.HIT_DTYPE).reshape(shits.shape)
+        for f in ("node", "t", "depth", "hit", "loops"):
+            assert np.array_equal(shits[f].view(np.uint32) if f == "t" else shits[f],
+                                  want[f].view(np.uint32) if f == "t" else want[f]), f"shadow {f}"
+        k += 1

@@ -56,11 +56,68 @@ def test_menger_frames(menger_scene, seed):
 
 
 @ref_needed
-@pytest.mark.parametrize("mode", [0, 1, 3, 4, 5])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3, 4, 5, 6, 7])
 def test_view_modes(menger_scene, mode):
     mm = L.TreeletMemoryManagerCuda(menger_scene, menger_scene.info.treelet_bytes)
     nodes, attribs = mm.getIncoreBuffer()
     check_frame(nodes, attribs, L.orbit_camera(4, 160, 100).frame_params(mode=mode))
+    # LOD stops give quality 0 in mode 7, leaves a positive or negative one
+    check_frame(nodes, attribs, L.orbit_camera(5, 96, 64, radius=1.2).frame_params(mode=mode, t_scale_ratio=0.02))
+
+
+def small_icosphere_pool():
+    from libsvo_b200 import scenes
+
+    wl = scenes.icosphere(subdivisions=4, depth=9, treelet_levels=5, width=160, height=96)
+    info = wl.scene.info
+    mm = L.TreeletMemoryManagerCuda(wl.scene, info.treelet_bytes * info.num_treelets)
+    mm.insertAll()
+    nodes, attribs = mm.getIncoreBuffer()
+    return wl, nodes, attribs
+
+
+@ref_needed
+@pytest.mark.parametrize("mode", [2, 6, 7])
+def test_view_modes_icosphere(mode):
+    wl, nodes, attribs = small_icosphere_pool()
+    check_frame(nodes, attribs, wl.cameras[0].frame_params(mode=mode))
+
+
+def check_shadow_frame(nodes, attribs, params, light, tsr=0.001, offset=0.01):
+    """The oracle's shadow frame against the same shading over the
+    reference's own sample() (oracle/ref_harness.inc)."""
+    rgba, hits, shits, _, rgbaf = oracle.render_shadow(nodes, attribs, bytes(params), light, tsr, offset,
+                                                       want_rgbaf=True)
+    ref, ref_shits = oracle.reference_render_shadow(nodes, attribs, bytes(params), light, tsr, offset)
+    assert np.array_equal(rgbaf.view(np.uint32), ref.view(np.uint32)), "shadow fragment colours differ"
+    assert np.array_equal(rgba, oracle.to_rgba8(ref))
+    for k in ("node", "depth", "hit", "loops"):
+        assert np.array_equal(shits[k], ref_shits[k]), f"shadow {k}"
+    assert np.array_equal(shits["t"].view(np.uint32), ref_shits["t"].view(np.uint32))
+    return hits, shits
+
+
+@ref_needed
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_shadow_frames_icosphere(seed):
+    wl, nodes, attribs = small_icosphere_pool()
+    light = L.default_light() if seed == 0 else L.seeded_light(seed)
+    for tsr in (None, 0.0):
+        hits, shits = check_shadow_frame(nodes, attribs, wl.cameras[0].frame_params(t_scale_ratio=tsr), light)
+        assert hits["hit"].sum() > 500
+        assert 0 < shits["hit"].sum() < hits["hit"].sum()
+
+
+@ref_needed
+@pytest.mark.parametrize("seed", [1, 2])
+def test_shadow_frames_menger_and_random(menger_scene, seed):
+    mm = L.TreeletMemoryManagerCuda(menger_scene, menger_scene.info.treelet_bytes)
+    nodes, attribs = mm.getIncoreBuffer()
+    check_shadow_frame(nodes, attribs, L.orbit_camera(seed, 160, 120, radius=1.4).frame_params(),
+                       L.seeded_light(seed))
+    nodes, attribs = random_octree_pool(seed, depth=5)
+    check_shadow_frame(nodes, attribs, L.orbit_camera(seed, 96, 96, radius=(1.0, 2.0)).frame_params(t_scale_ratio=0.0),
+                       L.seeded_light(seed + 5), 0.0, 0.02)
 
 
 @ref_needed
