@@ -143,6 +143,38 @@ int svo_scene_build_mesh(const float* h_vertices, uint64_t num_vertices,
                          uint32_t treelet_levels, uint32_t treelet_bytes, int32_t threads,
                          svo_scene** out);
 
+/* ---- scenes built on the GPU ------------------------------------------- */
+
+/* svo_scene_build_mesh + svo_mm_create_from_scene + svo_mm_insert_all +
+ * svo_mm_init_device_buffer in one step on the GPU, for octrees too large to
+ * build on the host: the mesh is voxelised, the octree built and cut into
+ * treelets in device memory, and every treelet written to its slot of a
+ * fully resident incore pool (treelet gid g in slot g, sub-treelet roots
+ * patched into their parents' leaves), bit for bit the pool the host path
+ * produces.  Stands in for TreeletBuilderFromFaces / TreeletBuildManager
+ * (src/TreeletBuilderFromFaces.cpp:189-365, src/TreeletBuildManager.cpp:
+ * 150-258) and the insertion loop (src/TreeletMemoryManager.cpp:518-545).
+ * The slot size is always the automatic one (largest treelet + 8 nodes).
+ * Blocks until the pool is built; scratch memory is freed before returning. */
+typedef struct svo_device_scene svo_device_scene;
+int svo_device_scene_build_mesh(const float* h_vertices, uint64_t num_vertices,
+                                const uint32_t* h_triangles, uint64_t num_triangles,
+                                uint32_t depth, uint32_t treelet_levels, void* stream,
+                                svo_device_scene** out);
+/* As svo_scene_info_get of the equivalent host scene. */
+int svo_device_scene_info_get(const svo_device_scene* scene, svo_scene_info* out);
+/* The pool: num_nodes = num_treelets * nodes_per_treelet records each. */
+int svo_device_scene_buffers(const svo_device_scene* scene, const svo_node** d_nodes,
+                             const svo_attrib** d_attribs, uint64_t* num_nodes);
+/* Copies pool records [first, first + count) to host memory (either output
+ * may be NULL); blocking. */
+int svo_device_scene_copy(const svo_device_scene* scene, uint64_t first, uint64_t count,
+                          svo_node* h_nodes, svo_attrib* h_attribs);
+/* Octree nodes over all levels and voxel/triangle overlaps found. */
+int svo_device_scene_counts(const svo_device_scene* scene, uint64_t* octree_nodes,
+                            uint64_t* overlaps);
+void svo_device_scene_destroy(svo_device_scene* scene);
+
 /* Seeded synthetic meshes (inputs for svo_scene_build_mesh).  The reference
  * voxelises scanned PLY meshes that are not part of it; these stand in with
  * the triangle counts of the benchmark configurations.  Call *_size first.

@@ -183,6 +183,12 @@ _SIGS = {
     "svo_batcher_launch": ([_vp, _vp, _vp], ctypes.c_int),
     "svo_batcher_autotune": ([_vp, _u32, _vp, _P(svo_batch_cfg), _P(_f32)], ctypes.c_int),
     "svo_batcher_size": ([_vp, _P(_u64), _P(_u64)], ctypes.c_int),
+    "svo_device_scene_build_mesh": ([_vp, _u64, _vp, _u64, _u32, _u32, _vp, _P(_vp)], ctypes.c_int),
+    "svo_device_scene_info_get": ([_vp, _P(svo_scene_info)], ctypes.c_int),
+    "svo_device_scene_buffers": ([_vp, _P(_vp), _P(_vp), _P(_u64)], ctypes.c_int),
+    "svo_device_scene_copy": ([_vp, _u64, _u64, _vp, _vp], ctypes.c_int),
+    "svo_device_scene_counts": ([_vp, _P(_u64), _P(_u64)], ctypes.c_int),
+    "svo_device_scene_destroy": ([_vp], None),
     "svo_render_batch_static": ([_P(svo_octree_desc), _u32, _P(svo_view_desc), _u32, _u32, _u32, _vp, _vp],
                                 ctypes.c_int),
 }
@@ -387,6 +393,62 @@ class Scene:
 
 
 # ---- memory manager ----------------------------------------------------------
+class DeviceScene:
+    """A mesh voxelised, built, cut into treelets and made fully resident on
+    the GPU (svo_device_scene_build_mesh): the incore pool the host path
+    Scene.from_mesh + TreeletMemoryManagerCuda.insertAll + initDeviceBuffer
+    produces, without the host holding the octree."""
+
+    def __init__(self, vertices: np.ndarray, triangles: np.ndarray, depth: int, treelet_levels=0,
+                 stream=None):
+        v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
+        t = np.ascontiguousarray(triangles, dtype=np.uint32).reshape(-1, 3)
+        h = ctypes.c_void_p()
+        _check(_L.svo_device_scene_build_mesh(_np_ptr(v), v.shape[0], _np_ptr(t), t.shape[0], depth,
+                                              treelet_levels, _stream_ptr(stream), ctypes.byref(h)),
+               "svo_device_scene_build_mesh")
+        self._h = h
+
+    @property
+    def info(self) -> svo_scene_info:
+        i = svo_scene_info()
+        _check(_L.svo_device_scene_info_get(self._h, ctypes.byref(i)), "svo_device_scene_info_get")
+        return i
+
+    def buffers(self):
+        """(device node pointer, device attribute pointer, pool records)."""
+        n, a, c = ctypes.c_void_p(), ctypes.c_void_p(), _u64()
+        _check(_L.svo_device_scene_buffers(self._h, ctypes.byref(n), ctypes.byref(a), ctypes.byref(c)),
+               "svo_device_scene_buffers")
+        return n.value, a.value, c.value
+
+    def counts(self):
+        """(octree nodes over all levels, voxel/triangle overlaps)."""
+        o, p = _u64(), _u64()
+        _check(_L.svo_device_scene_counts(self._h, ctypes.byref(o), ctypes.byref(p)), "svo_device_scene_counts")
+        return o.value, p.value
+
+    def getIncoreBuffer(self, first: int = 0, count: int | None = None):
+        total = self.buffers()[2]
+        count = total - first if count is None else count
+        nodes = np.zeros((count, 2), dtype=np.uint32)
+        attribs = np.zeros((count, 2), dtype=np.uint32)
+        _check(_L.svo_device_scene_copy(self._h, first, count, _np_ptr(nodes), _np_ptr(attribs)),
+               "svo_device_scene_copy")
+        return nodes, attribs
+
+    def close(self):
+        if self._h and self._h.value:
+            _L.svo_device_scene_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class TreeletMemoryManagerCuda:
     """TreeletMemoryManager + TreeletMemoryManagerCl with the incore buffer in
     HBM.  Method names follow the reference; insert/remove/free return bool
@@ -896,7 +958,7 @@ def _close_all():
 
 _atexit.register(_close_all)
 
-for _cls in (Scene, TreeletMemoryManagerCuda, Batcher, Server):
+for _cls in (Scene, DeviceScene, TreeletMemoryManagerCuda, Batcher, Server):
     _orig_init = _cls.__init__
 
     def _init(self, *a, __orig=_orig_init, **k):

@@ -10,6 +10,7 @@
 #include "../../include/libsvo_b200.h"
 #include "errors.h"
 #include "feedback.h"
+#include "gpu_builder.h"
 #include "memory_manager.h"
 #include "render.h"
 #include "scene.h"
@@ -112,6 +113,75 @@ int svo_scene_build_mesh(const float* h_vertices, uint64_t num_vertices,
     return build_scene(depth, codes, attribs, treelet_levels, treelet_bytes, out);
   });
 }
+
+struct svo_device_scene {
+  svo::DeviceScene impl;
+};
+
+int svo_device_scene_build_mesh(const float* h_vertices, uint64_t num_vertices,
+                                const uint32_t* h_triangles, uint64_t num_triangles,
+                                uint32_t depth, uint32_t treelet_levels, void* stream,
+                                svo_device_scene** out) {
+  if (!out || !h_vertices || !h_triangles) return SVO_ERR_INVALID;
+  *out = nullptr;
+  return guarded([&] {
+    svo_device_scene* s = new svo_device_scene;
+    const int rc = s->impl.build_mesh(h_vertices, num_vertices, h_triangles, num_triangles, depth,
+                                      treelet_levels, (cudaStream_t)stream);
+    if (rc != SVO_OK) {
+      delete s;
+      return rc;
+    }
+    *out = s;
+    return SVO_OK;
+  });
+}
+
+int svo_device_scene_info_get(const svo_device_scene* scene, svo_scene_info* out) {
+  if (!scene || !out) return SVO_ERR_INVALID;
+  const svo::DeviceScene& d = scene->impl;
+  out->num_treelets = d.num_treelets;
+  out->treelet_bytes = (uint32_t)(d.nodes_per_slot * 8);
+  out->nodes_per_treelet = (uint32_t)d.nodes_per_slot;
+  out->max_depth = d.depth;
+  out->total_nodes = d.treelet_nodes;
+  out->leaf_voxels = d.leaf_voxels;
+  return SVO_OK;
+}
+
+int svo_device_scene_buffers(const svo_device_scene* scene, const svo_node** d_nodes,
+                             const svo_attrib** d_attribs, uint64_t* num_nodes) {
+  if (!scene) return SVO_ERR_INVALID;
+  if (d_nodes) *d_nodes = scene->impl.d_nodes;
+  if (d_attribs) *d_attribs = scene->impl.d_attribs;
+  if (num_nodes) *num_nodes = scene->impl.pool_nodes;
+  return SVO_OK;
+}
+
+int svo_device_scene_copy(const svo_device_scene* scene, uint64_t first, uint64_t count,
+                          svo_node* h_nodes, svo_attrib* h_attribs) {
+  if (!scene) return SVO_ERR_INVALID;
+  const svo::DeviceScene& d = scene->impl;
+  if (first > d.pool_nodes || count > d.pool_nodes - first) return SVO_ERR_RANGE;
+  if (count == 0) return SVO_OK;
+  if (h_nodes)
+    SVO_CUDA_TRY(cudaMemcpy(h_nodes, d.d_nodes + first, count * sizeof(svo_node),
+                            cudaMemcpyDeviceToHost));
+  if (h_attribs)
+    SVO_CUDA_TRY(cudaMemcpy(h_attribs, d.d_attribs + first, count * sizeof(svo_attrib),
+                            cudaMemcpyDeviceToHost));
+  return SVO_OK;
+}
+
+int svo_device_scene_counts(const svo_device_scene* scene, uint64_t* octree_nodes,
+                            uint64_t* overlaps) {
+  if (!scene) return SVO_ERR_INVALID;
+  if (octree_nodes) *octree_nodes = scene->impl.octree_nodes;
+  if (overlaps) *overlaps = scene->impl.pairs;
+  return SVO_OK;
+}
+
+void svo_device_scene_destroy(svo_device_scene* scene) { delete scene; }
 
 int svo_scene_write(const svo_scene* scene, const char* path_base) {
   if (!scene || !path_base) return SVO_ERR_INVALID;

@@ -409,6 +409,17 @@ bool tri_box_overlap(const float bc[3], float h, const float* a, const float* b,
   return n[0] * vmax[0] + n[1] * vmax[1] + n[2] * vmax[2] + d >= 0.0f;
 }
 
+// floor(x) as a lattice coordinate, clamped to [-2, R + 1] (NaN -> -2) so
+// that degenerate triangles cannot overflow the int conversion; every caller
+// clamps the result into [0, R - 1] afterwards, so the clamp changes nothing
+// for coordinates inside the cube.  The GPU builder uses the same rule.
+int cell_floor(float x, uint32_t R) {
+  const float hi = (float)R + 1.0f;
+  if (!(x >= -2.0f)) return -2;
+  if (x > hi) return (int)R + 1;
+  return (int)std::floor(x);
+}
+
 struct VoxelTri {
   uint64_t code;
   uint32_t tri;
@@ -450,8 +461,8 @@ int build_mesh_leaves(const float* V, uint64_t nv, const uint32_t* T, uint64_t n
       for (int k = 0; k < 3; ++k) {
         const float mn = std::min(a[k], std::min(b[k], c[k]));
         const float mx = std::max(a[k], std::max(b[k], c[k]));
-        lo[k] = std::max(0, (int)std::floor((mn + 0.5f) * (float)R));
-        hi[k] = std::min((int)R - 1, (int)std::floor((mx + 0.5f) * (float)R));
+        lo[k] = std::max(0, cell_floor((mn + 0.5f) * (float)R, R));
+        hi[k] = std::min((int)R - 1, cell_floor((mx + 0.5f) * (float)R, R));
         if (lo[k] > hi[k]) lo[k] = hi[k] + 1;
       }
       if (lo[0] > hi[0] || lo[1] > hi[1] || lo[2] > hi[2]) continue;
@@ -476,8 +487,8 @@ int build_mesh_leaves(const float* V, uint64_t nv, const uint32_t* T, uint64_t n
                 wmin = std::min(wmin, ww);
                 wmax = std::max(wmax, ww);
               }
-            wlo = std::max(wlo, (int)std::floor((wmin + 0.5f) * (float)R) - 1);
-            whi = std::min(whi, (int)std::floor((wmax + 0.5f) * (float)R) + 1);
+            wlo = std::max(wlo, cell_floor((wmin + 0.5f) * (float)R, R) - 1);
+            whi = std::min(whi, cell_floor((wmax + 0.5f) * (float)R, R) + 1);
           }
           for (int iw = wlo; iw <= whi; ++iw) {
             int ijk[3];
