@@ -324,6 +324,70 @@ def served_leg(dev, n=400, rates=(4000, 16000)):
             "paging_half_budget": paging}
 
 
+def large_shadow_leg(dev, reps=10, cap_gb=60.0):
+    """the depth-14 icosphere built on the GPU, one
+    3840x2160 frame of primary rays plus one shadow ray per hit.  The metric
+    counts both kinds of ray."""
+    import torch
+
+    import libsvo_b200 as L
+    from libsvo_b200 import scenes
+
+    t0 = time.perf_counter()
+    wl = scenes.large_shadowed()
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    info = wl.scene.info
+    d_nodes, d_attribs, n = wl.scene.buffers()
+    pool_gb = 16 * n / 1e9
+    octree_nodes, overlaps = wl.scene.counts()
+    p = wl.camera.frame_params()
+    cfg = L.trace_cfg(L.TRAVERSAL_TREELET, wl.stack_size)
+    sc = L.shadow_cfg(wl.light)
+    px = p.width * p.height
+    rgba = torch.empty((p.height, p.width), dtype=torch.int32, device=dev)
+    hb = torch.empty(px * 16, dtype=torch.uint8, device=dev)
+    sb = torch.empty(px * 16, dtype=torch.uint8, device=dev)
+    stats = torch.zeros(4, dtype=torch.int32, device=dev)
+    s = torch.cuda.current_stream()
+    L.render_shadow(d_nodes, d_attribs, n, p, rgba, sc, hb, sb, cfg=cfg, d_stats=stats, stream=s)
+    torch.cuda.synchronize()
+    h = hb.cpu().numpy().view(L.HIT_DTYPE)
+    sh = sb.cpu().numpy().view(L.HIT_DTYPE)
+    del hb, sb
+    primary_hits = int(h["hit"].astype(np.int64).sum())
+    shadow_rays = primary_hits  # one per hit (all hits lie in the pool)
+    shadowed = int(sh["hit"].astype(np.int64).sum())
+    fetches = int(h["fetches"].astype(np.int64).sum()) + int(sh["fetches"].astype(np.int64).sum())
+    algo_bytes = 8 * fetches + 8 * primary_hits + 4 * px
+    rays = px + shadow_rays
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(reps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(reps)]
+    for i in range(3):
+        L.render_shadow(d_nodes, d_attribs, n, p, rgba, sc, cfg=cfg, stream=s)
+    for i in range(reps):
+        flush.fill_(i)
+        starts[i].record(s)
+        L.render_shadow(d_nodes, d_attribs, n, p, rgba, sc, cfg=cfg, stream=s)
+        ends[i].record(s)
+    torch.cuda.synchronize()
+    ms = statistics.mean(a.elapsed_time(b) for a, b in zip(starts, ends))
+    peak, _ = load_peaks()
+    out = {"workload": wl.name, "description": wl.description, "scene_build_s": round(build_s, 2),
+           "treelets": int(info.num_treelets), "treelet_bytes": int(info.treelet_bytes),
+           "octree_nodes": int(octree_nodes), "leaf_voxels": int(info.leaf_voxels),
+           "voxel_triangle_overlaps": int(overlaps), "pool_gb": pool_gb, "residency_cap_gb": cap_gb,
+           "resident": "all treelets (the pool fits the cap)" if pool_gb <= cap_gb else "over the cap",
+           "primary_rays": px, "shadow_rays": shadow_rays, "shadowed_hits": shadowed,
+           "ms_per_frame": ms, "mrays_s": rays / ms / 1e3, "primary_mrays_s": px / ms / 1e3,
+           "capped_rays": int(stats[0].item()), "bounds_errors": int(stats[1].item()),
+           "roofline": {"algorithmic_bytes_per_frame": algo_bytes, "achieved_gbs": algo_bytes / ms / 1e6,
+                        "frac": algo_bytes / ms / 1e6 / peak, "node_reads_per_ray": fetches / rays}}
+    wl.scene.close()
+    return out
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -471,7 +535,8 @@ def main():
             line["cpu_baseline"] = cpu_reference_frames(wl, nodes, attribs)
         mm.close()
         if world == 1 and not args.no_extra:
-            for key, leg in (("batched", batched_leg), ("served", served_leg)):
+            for key, leg in (("batched", batched_leg), ("served", served_leg),
+                             ("large_shadowed", large_shadow_leg)):
                 try:
                     line[key] = leg(dev)
                 except Exception as e:  # a failing extra leg must not lose the primary line

@@ -20,6 +20,12 @@ configurations name:
                    with sides drawn log-uniformly from 256 to 2048 pixels,
                    eyes above the terrain looking at seeded points on it,
                    60 degree fov.
+* ``large_shadowed`` -- icosphere subdivided 9 times (5,242,880 triangles),
+                   4-octave noise, depth-14 octree (16384^3) cut into 8-level
+                   treelets, built on the GPU (DeviceScene, about 40 GB of
+                   pool); one 3840x2160 view from the icosphere orbit, primary
+                   rays plus one shadow ray per hit toward a seeded
+                   directional light, stack size 15 (depth 14 + 1).
 """
 from __future__ import annotations
 
@@ -28,7 +34,8 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from . import Camera, Scene, icosphere as icosphere_mesh, orbit_camera, terrain as terrain_mesh
+from . import (Camera, DeviceScene, Scene, icosphere as icosphere_mesh, orbit_camera, seeded_light,
+               terrain as terrain_mesh)
 
 
 @dataclass
@@ -87,6 +94,31 @@ def terrain(grid=1024, depth=12, treelet_levels=6, seed=1, views=64, min_side=25
                     description=f"terrain {grid}x{grid} grid ({t.shape[0]} triangles), 6-octave fBm, "
                                 f"depth {depth}, {treelet_levels}-level treelets, {views} views "
                                 f"{min_side}^2..{max_side}^2 log-uniform, fov {fov_deg}")
+
+
+@dataclass
+class LargeShadowedWorkload:
+    name: str
+    scene: DeviceScene
+    camera: Camera
+    light: np.ndarray
+    stack_size: int
+    description: str = ""
+
+
+def large_shadowed(subdivisions=9, depth=14, treelet_levels=8, seed=1, width=3840, height=2160,
+                   fov_deg=25.0, radius=2.5, stream=None) -> LargeShadowedWorkload:
+    v, t = icosphere_mesh(subdivisions, radius=0.4, octaves=4, amplitude=0.05, frequency=2.0, seed=seed)
+    scene = DeviceScene(v, t, depth, treelet_levels=treelet_levels, stream=stream)
+    rng = np.random.default_rng(seed)
+    cam = orbit_pose(radius, float(rng.uniform(0, 360)), float(rng.uniform(-30, 30)), width, height, fov_deg)
+    return LargeShadowedWorkload(
+        f"icosphere_s{subdivisions}_d{depth}_{width}x{height}_shadow", scene, cam, seeded_light(seed),
+        depth + 1,
+        description=f"icosphere {subdivisions}x subdivided ({t.shape[0]} triangles), 4-octave noise 0.05, "
+                    f"depth {depth}, {treelet_levels}-level treelets built on the GPU, {width}x{height} "
+                    f"primary rays + 1 shadow ray per hit toward a seeded directional light, "
+                    f"orbit radius {radius}, fov {fov_deg}")
 
 
 @dataclass
