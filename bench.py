@@ -324,6 +324,66 @@ def served_leg(dev, n=400, rates=(4000, 16000)):
             "paging_half_budget": paging}
 
 
+def incore_update_leg(dev, scene, incore_mb=256, frames=20, seed=5):
+    """The reference's incore update measurement (its thesis: 256 MB incore
+    buffer, dirty slots uploaded per frame with coalescing ratio 0.6, one copy
+    per slot, and ratio 0) on the icosphere scene: each frame evicts 12 MB
+    worth of childless resident treelets and inserts as many treelets whose
+    parent is resident, then times updateDeviceMemory until the copies
+    finish.  Every policy replays the same eviction/insertion sequence."""
+    import torch
+
+    import libsvo_b200 as L
+
+    nt = scene.info.num_treelets
+    tb = scene.info.treelet_bytes
+    parent = [scene.treelet(g)["parent_gid"] if g else -1 for g in range(nt)]
+    kids = {}
+    for g in range(1, nt):
+        kids.setdefault(parent[g], []).append(g)
+    policies = [("coalesced_0.6", L.UPLOAD_COALESCED, 0.6), ("one_copy_per_slot", L.UPLOAD_COALESCED, 1.0),
+                ("one_range_ratio_0", L.UPLOAD_COALESCED, 0.0), ("packed_scatter", L.UPLOAD_PACKED, 0.6),
+                ("pinned_mirror_gather", L.UPLOAD_PINNED, 0.6)]
+    out = {"scene": "icosphere_s6_d11 (6-level treelets)", "incore_mb": incore_mb, "treelet_bytes": tb,
+           "frames": frames}
+    for name, policy, ratio in policies:
+        mm = L.TreeletMemoryManagerCuda(scene, incore_mb << 20)
+        mm.setUploadPolicy(policy)
+        mm.setUploadRatio(ratio)
+        mm.initDeviceBuffer()
+        mm.insertAll()
+        k = max(1, (12 << 20) // tb)
+        resident = {g for g in range(nt) if mm.getSlotGid(g) >= 0}
+        mm.updateDeviceMemory()
+        torch.cuda.synchronize()
+        rng = np.random.default_rng(seed)
+        ms, calls, dirty, moved = [], [], [], []
+        for _ in range(frames):
+            leaves = sorted(g for g in resident if g and not any(c in resident for c in kids.get(g, ())))
+            for g in rng.permutation(leaves)[:k].tolist():
+                mm.removeTreeletFromIncoreBuffer(g)
+                resident.discard(g)
+            cands = sorted(g for g in range(1, nt) if g not in resident and parent[g] in resident)
+            for g in rng.permutation(cands)[:k].tolist():
+                if mm.insertTreeletIntoIncoreBuffer(g):
+                    resident.add(g)
+            ds = mm.getIncoreSlotsToUpload()
+            dirty.append(len(ds))
+            plan = mm.planUploads()
+            moved.append(2 * tb * (len(ds) if policy != L.UPLOAD_COALESCED else sum(c for _, c in plan)))
+            t0 = time.perf_counter()
+            calls.append(mm.updateDeviceMemory())
+            torch.cuda.synchronize()
+            ms.append((time.perf_counter() - t0) * 1e3)
+        mm.close()
+        out[name] = {"ms_mean": statistics.mean(ms), "ms_median": statistics.median(ms),
+                     "copy_calls_mean": statistics.mean(calls), "dirty_slots_mean": statistics.mean(dirty),
+                     "mb_over_pcie_mean": statistics.mean(moved) / 1e6}
+    out["reference_thesis_ms"] = {"coalesced_0.6": 2.48, "one_copy_per_slot": 4.23, "one_range_ratio_0": 52.51,
+                                  "hardware": "GTX 580, PCIe 2 (ergebnisse_diskussionen.tex:111)"}
+    return out
+
+
 def large_shadow_leg(dev, reps=10, cap_gb=60.0):
     """the depth-14 icosphere built on the GPU, one
     3840x2160 frame of primary rays plus one shadow ray per hit.  The metric
@@ -534,6 +594,11 @@ def main():
             nodes, attribs = mm.getIncoreBuffer()
             line["cpu_baseline"] = cpu_reference_frames(wl, nodes, attribs)
         mm.close()
+        if world == 1 and not args.no_extra and args.workload == "icosphere":
+            try:
+                line["incore_update"] = incore_update_leg(dev, wl.scene)
+            except Exception as e:  # a failing extra leg must not lose the primary line
+                line["incore_update"] = {"error": f"{type(e).__name__}: {e}"}
         if world == 1 and not args.no_extra:
             for key, leg in (("batched", batched_leg), ("served", served_leg),
                              ("large_shadowed", large_shadow_leg)):

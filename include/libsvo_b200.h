@@ -260,8 +260,28 @@ int svo_mm_update_client_side(svo_mm* mm, const int32_t* new_gids, const float* 
 /* updateDeviceMemory (src/TreeletMemoryManagerCl.cpp:155-251): uploads the
  * dirty slots, merging neighbours with the reference's 0.6 coalescing rule,
  * as async copies on the side stream; renders issued afterwards wait for
- * them.  *num_copy_calls (optional) receives the number of ranges. */
+ * them.  *num_copy_calls (optional) receives the number of ranges (packed
+ * policy: the number of packed copies). */
 int svo_mm_update_device_memory(svo_mm* mm, uint32_t* num_copy_calls);
+/* Upload policies.  COALESCED (default): the reference's slot ranges, each
+ * staged through a pinned ring.  PACKED: only dirty slots, packed back to
+ * back into the ring in 4 MB chunks (one copy per chunk), placed by a scatter
+ * kernel.  PINNED: the host mirror is page-locked and mapped
+ * (cudaHostRegister, so it costs its size in locked host memory) and one
+ * kernel reads the dirty slots from it over PCIe and writes them in place;
+ * host-side treelet changes then wait for a gather still reading the mirror.
+ * All leave the same device pool.  No reference
+ * counterpart: the reference hard-codes the coalesced form. */
+#define SVO_UPLOAD_COALESCED 0
+#define SVO_UPLOAD_PACKED 1
+#define SVO_UPLOAD_PINNED 2
+int svo_mm_set_upload_policy(svo_mm* mm, int32_t policy);
+/* The coalescing ratio of the COALESCED policy: a range grows over the next
+ * dirty slot while (treelets + 1) / (slot distance + 1) >= 2 * ratio.  The
+ * reference's value is 0.6 (TreeletMemoryManagerCl.cpp:188); 1 copies each
+ * slot alone, 0 copies one range from the first to the last dirty slot.
+ * SVO_ERR_RANGE outside [0, 1]. */
+int svo_mm_set_upload_ratio(svo_mm* mm, float ratio);
 /* The copy ranges the next svo_mm_update_device_memory will issue: slot
  * ranges (first slot, slot count) merged with the 0.6 rule of
  * TreeletMemoryManagerCl.cpp:177-211.  Pass NULL arrays to query the count. */

@@ -43,6 +43,9 @@ SVO_ERR_CUDA = -1000
 
 _ERR_NAMES = {v: k for k, v in dict(globals()).items() if k.startswith("SVO_ERR_")}
 
+UPLOAD_COALESCED = 0
+UPLOAD_PACKED = 1
+UPLOAD_PINNED = 2
 TRAVERSAL_TREELET = 0
 TRAVERSAL_FLAT = 1
 HITFLAG_CAPPED = 1
@@ -172,6 +175,8 @@ _SIGS = {
     "svo_mm_render": ([_vp, _P(svo_frame_params), _P(svo_trace_cfg), _vp, _vp, _vp], ctypes.c_int),
     "svo_mm_render_host": ([_vp, _P(svo_frame_params), _P(svo_trace_cfg), _vp, _vp], ctypes.c_int),
     "svo_mm_sync": ([_vp, _vp, _P(svo_stats)], ctypes.c_int),
+    "svo_mm_set_upload_policy": ([_vp, _i32], ctypes.c_int),
+    "svo_mm_set_upload_ratio": ([_vp, _f32], ctypes.c_int),
     "svo_render_shadow": ([_vp, _vp, _u64, _P(svo_frame_params), _P(svo_trace_cfg), _P(svo_shadow_cfg), _vp, _vp,
                            _vp, _vp, _vp], ctypes.c_int),
     "svo_mm_render_shadow": ([_vp, _P(svo_frame_params), _P(svo_trace_cfg), _P(svo_shadow_cfg), _vp, _vp, _vp,
@@ -513,6 +518,17 @@ class TreeletMemoryManagerCuda:
         _check(_L.svo_mm_plan_uploads(self._h, _np_ptr(f), _np_ptr(c), n.value, ctypes.byref(n)),
                "svo_mm_plan_uploads")
         return list(zip(f.tolist(), c.tolist()))
+
+    def setUploadPolicy(self, policy: int):
+        """UPLOAD_COALESCED (the reference's ranges, staged), UPLOAD_PACKED
+        (dirty slots packed, scatter kernel) or UPLOAD_PINNED (page-locked
+        mirror, ranges copied directly)."""
+        _check(_L.svo_mm_set_upload_policy(self._h, policy), "svo_mm_set_upload_policy")
+
+    def setUploadRatio(self, ratio: float):
+        """The coalescing ratio (the reference's 0.6; 1 = one copy per slot,
+        0 = one range over all dirty slots)."""
+        _check(_L.svo_mm_set_upload_ratio(self._h, ratio), "svo_mm_set_upload_ratio")
 
     def resetIncoreBuffer(self):
         _check(_L.svo_mm_reset(self._h), "svo_mm_reset")

@@ -333,6 +333,16 @@ int svo_mm_update_client_side(svo_mm* mm, const int32_t* new_gids, const float* 
   });
 }
 
+int svo_mm_set_upload_policy(svo_mm* mm, int32_t policy) {
+  if (!mm) return SVO_ERR_INVALID;
+  return mm->impl.set_upload_policy(policy);
+}
+
+int svo_mm_set_upload_ratio(svo_mm* mm, float ratio) {
+  if (!mm) return SVO_ERR_INVALID;
+  return mm->impl.set_upload_ratio(ratio);
+}
+
 int svo_mm_update_device_memory(svo_mm* mm, uint32_t* num_copy_calls) {
   if (!mm) return SVO_ERR_INVALID;
   return guarded([&] { return mm->impl.update_device_memory(num_copy_calls); });

@@ -7,6 +7,7 @@
 #include <deque>
 
 #include "errors.h"
+#include "upload.h"
 
 namespace svo {
 
@@ -200,9 +201,15 @@ int TreeletMemoryManager::insert_all(uint32_t* inserted) {
   return rc;
 }
 
+int TreeletMemoryManager::set_upload_ratio(float ratio) {
+  if (!(ratio >= 0.0f && ratio <= 1.0f)) return SVO_ERR_RANGE;
+  upload_ratio_ = ratio;
+  return SVO_OK;
+}
+
 std::vector<std::pair<uint32_t, uint32_t>> TreeletMemoryManager::upload_ranges() const {
   std::vector<std::pair<uint32_t, uint32_t>> out;
-  const float ratio_limit = 0.6f * 2.0f;
+  const float ratio_limit = upload_ratio_ * 2.0f;
   auto it = upload_.begin();
   while (it != upload_.end()) {
     const uint32_t start = *it;
@@ -227,6 +234,11 @@ std::vector<std::pair<uint32_t, uint32_t>> TreeletMemoryManager::upload_ranges()
 
 TreeletMemoryManagerCuda::~TreeletMemoryManagerCuda() {
   if (copy_stream_) cudaStreamSynchronize(copy_stream_);
+  if (mirror_pinned_) {
+    cudaHostUnregister(incore_);
+    cudaHostUnregister(incore_attr_);
+  }
+  if (h_slot_ids_) cudaFreeHost(h_slot_ids_);
   if (owns_device_) {
     cudaFree(d_nodes_);
     cudaFree(d_attribs_);
@@ -237,6 +249,9 @@ TreeletMemoryManagerCuda::~TreeletMemoryManagerCuda() {
   for (int i = 0; i < 2; ++i) {
     if (stage_evt_[i]) cudaEventDestroy(stage_evt_[i]);
     if (stage_[i]) cudaFreeHost(stage_[i]);
+    if (h_ids_[i]) cudaFreeHost(h_ids_[i]);
+    cudaFree(d_stage_[i]);
+    cudaFree(d_ids_[i]);
   }
   if (upload_done_) cudaEventDestroy(upload_done_);
   if (copy_stream_) cudaStreamDestroy(copy_stream_);
@@ -326,10 +341,116 @@ int TreeletMemoryManagerCuda::stage_copy(void* dst, const void* src, uint64_t by
   return SVO_OK;
 }
 
+int TreeletMemoryManagerCuda::set_upload_policy(int policy) {
+  if (policy != SVO_UPLOAD_COALESCED && policy != SVO_UPLOAD_PACKED && policy != SVO_UPLOAD_PINNED)
+    return SVO_ERR_NOTSUP;
+  if (policy == SVO_UPLOAD_PINNED && !mirror_pinned_) {
+    const uint64_t bytes = incore_nodes() * sizeof(svo_node);
+    cudaError_t e = cudaHostRegister(incore_, bytes, cudaHostRegisterMapped);
+    if (e == cudaSuccess) {
+      e = cudaHostRegister(incore_attr_, bytes, cudaHostRegisterMapped);
+      if (e != cudaSuccess) cudaHostUnregister(incore_);
+    }
+    void* dn = nullptr;
+    void* da = nullptr;
+    void* di = nullptr;
+    if (e == cudaSuccess && !h_slot_ids_)
+      e = cudaHostAlloc(&h_slot_ids_, (size_t)num_slots() * sizeof(uint32_t), cudaHostAllocMapped);
+    if (e == cudaSuccess) e = cudaHostGetDevicePointer(&dn, incore_, 0);
+    if (e == cudaSuccess) e = cudaHostGetDevicePointer(&da, incore_attr_, 0);
+    if (e == cudaSuccess) e = cudaHostGetDevicePointer(&di, h_slot_ids_, 0);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return cuda_status(e);
+    }
+    mapped_nodes_ = (const svo_node*)dn;
+    mapped_attribs_ = (const svo_attrib*)da;
+    mapped_slot_ids_ = (const uint32_t*)di;
+    mirror_pinned_ = true;
+  }
+  upload_policy_ = policy;
+  return SVO_OK;
+}
+
+// With the mirror page-locked, the gather kernel reads it directly: a
+// host-side change waits for the gather still in flight.
+void TreeletMemoryManagerCuda::before_host_write() {
+  if (upload_policy_ == SVO_UPLOAD_PINNED && upload_pending_ && copy_stream_)
+    cudaStreamSynchronize(copy_stream_);
+}
+
+// Dirty slots packed back to back into a ring half ({nodes, attributes} per
+// slot), one copy of the packed bytes and one of the slot ids, then the
+// scatter kernel, all on the copy stream; the next use of a half waits for
+// the event recorded after its scatter.
+int TreeletMemoryManagerCuda::upload_packed(uint32_t* copy_calls) {
+  const uint64_t slot_bytes = (uint64_t)N_ * (sizeof(svo_node) + sizeof(svo_attrib));
+  // chunks of about 4 MB, so that packing the next chunk overlaps the copy
+  // of the previous one
+  const uint64_t chunk = std::min<uint64_t>(kStageBytes, std::max<uint64_t>(slot_bytes, 4ull << 20));
+  const uint64_t per_half = chunk / slot_bytes;
+  for (int i = 0; i < 2; ++i) {
+    if (!d_stage_[i]) SVO_CUDA_TRY(cudaMalloc(&d_stage_[i], kStageBytes));
+    if (!h_ids_[i]) SVO_CUDA_TRY(cudaMallocHost(&h_ids_[i], per_half * sizeof(uint32_t)));
+    if (!d_ids_[i]) SVO_CUDA_TRY(cudaMalloc(&d_ids_[i], per_half * sizeof(uint32_t)));
+  }
+  uint32_t calls = 0;
+  auto it = upload_.begin();
+  while (it != upload_.end()) {
+    const int h = stage_next_;
+    stage_next_ ^= 1;
+    SVO_CUDA_TRY(cudaEventSynchronize(stage_evt_[h]));
+    char* dst = (char*)stage_[h];
+    uint32_t k = 0;
+    for (; it != upload_.end() && k < per_half; ++it, ++k) {
+      const uint64_t first = (uint64_t)*it * N_;
+      std::memcpy(dst, incore_ + first, (size_t)N_ * sizeof(svo_node));
+      std::memcpy(dst + (size_t)N_ * sizeof(svo_node), incore_attr_ + first,
+                  (size_t)N_ * sizeof(svo_attrib));
+      dst += slot_bytes;
+      h_ids_[h][k] = *it;
+    }
+    SVO_CUDA_TRY(cudaMemcpyAsync(d_stage_[h], stage_[h], k * slot_bytes, cudaMemcpyHostToDevice,
+                                 copy_stream_));
+    SVO_CUDA_TRY(cudaMemcpyAsync(d_ids_[h], h_ids_[h], k * sizeof(uint32_t),
+                                 cudaMemcpyHostToDevice, copy_stream_));
+    const int rc = launch_slot_scatter(d_stage_[h], d_ids_[h], k, N_, d_nodes_, d_attribs_,
+                                       copy_stream_);
+    if (rc != SVO_OK) return rc;
+    SVO_CUDA_TRY(cudaEventRecord(stage_evt_[h], copy_stream_));
+    ++calls;
+  }
+  if (copy_calls) *copy_calls = calls;
+  return SVO_OK;
+}
+
 int TreeletMemoryManagerCuda::update_device_memory(uint32_t* copy_calls) {
   if (copy_calls) *copy_calls = 0;
   if (upload_.empty()) return SVO_OK;
   if (!d_nodes_) return SVO_ERR_INVALID;  // init_device_buffer first
+  const uint64_t slot_bytes = (uint64_t)N_ * (sizeof(svo_node) + sizeof(svo_attrib));
+  if (upload_policy_ == SVO_UPLOAD_PACKED && slot_bytes <= kStageBytes) {
+    const int rc = upload_packed(copy_calls);
+    if (rc != SVO_OK) return rc;
+    SVO_CUDA_TRY(cudaEventRecord(upload_done_, copy_stream_));
+    upload_pending_ = true;
+    upload_.clear();
+    return SVO_OK;
+  }
+  if (upload_policy_ == SVO_UPLOAD_PINNED) {
+    // the slot-id list is read by the previous gather until it finishes
+    if (upload_pending_) SVO_CUDA_TRY(cudaStreamSynchronize(copy_stream_));
+    uint32_t k = 0;
+    for (uint32_t s : upload_) h_slot_ids_[k++] = s;
+    const int rc = launch_slot_gather(mapped_nodes_, mapped_attribs_, mapped_slot_ids_, k, N_,
+                                      d_nodes_, d_attribs_, copy_stream_);
+    if (rc != SVO_OK) return rc;
+    SVO_CUDA_TRY(cudaEventRecord(upload_done_, copy_stream_));
+    upload_pending_ = true;
+    if (copy_calls) *copy_calls = 1;
+    upload_.clear();
+    return SVO_OK;
+  }
   const auto ranges = upload_ranges();
   for (const auto& r : ranges) {
     const uint64_t first = (uint64_t)r.first * N_;

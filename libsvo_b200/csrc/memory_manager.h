@@ -71,8 +71,15 @@ class TreeletMemoryManager {
   uint32_t default_max_new_treelets() const;
 
   // Slot ranges the reference's updateDeviceMemory would copy
-  // (TreeletMemoryManagerCl.cpp:177-236), as (first slot, slot count).
+  // (TreeletMemoryManagerCl.cpp:177-236), as (first slot, slot count).  A
+  // range keeps growing over the next dirty slot while (treelets + 1) /
+  // (slot distance + 1) >= 2 * ratio; the reference hard-codes ratio 0.6,
+  // ratio 1 copies every slot alone, ratio 0 one range over all dirty slots.
   std::vector<std::pair<uint32_t, uint32_t>> upload_ranges() const;
+  // 0 <= ratio <= 1 (a larger ratio would stop the reference's loop from
+  // advancing).
+  int set_upload_ratio(float ratio);
+  float upload_ratio() const { return upload_ratio_; }
 
  protected:
   // Called before the host mirror changes, so uploads still reading it
@@ -90,6 +97,7 @@ class TreeletMemoryManager {
   std::vector<uint32_t> free_;  // top = back()
   std::set<uint32_t> upload_;
   uint32_t search_pos_ = 1;
+  float upload_ratio_ = 0.6f;
 };
 
 class TreeletMemoryManagerCuda : public TreeletMemoryManager {
@@ -104,6 +112,14 @@ class TreeletMemoryManagerCuda : public TreeletMemoryManager {
   // Forgets attached buffers (after waiting for uploads into them).
   int detach_device_buffers();
   int update_device_memory(uint32_t* copy_calls);   // updateDeviceMemory
+  // SVO_UPLOAD_COALESCED: the reference's slot ranges (upload_ranges), each
+  // staged through the pinned ring.  SVO_UPLOAD_PACKED: only the dirty slots,
+  // packed back to back into the pinned ring, one host-to-device copy per
+  // 4 MB chunk, and a scatter kernel that moves each slot to its place.
+  // SVO_UPLOAD_PINNED: the mirror itself is page-locked and mapped; one
+  // kernel reads the dirty slots from it over PCIe and writes them in place.
+  int set_upload_policy(int policy);
+  int upload_policy() const { return upload_policy_; }
   int reset_incore_buffer() override;
 
   const svo_node* device_nodes() const { return d_nodes_; }
@@ -122,6 +138,8 @@ class TreeletMemoryManagerCuda : public TreeletMemoryManager {
 
  private:
   int stage_copy(void* dst, const void* src, uint64_t bytes);
+  int upload_packed(uint32_t* copy_calls);
+  void before_host_write() override;
   int init_transfer();
   int upload_all();
 
@@ -137,6 +155,16 @@ class TreeletMemoryManagerCuda : public TreeletMemoryManager {
   static constexpr uint64_t kStageBytes = 32ull << 20;  // per half of the ring
   void* stage_[2] = {nullptr, nullptr};
   cudaEvent_t stage_evt_[2] = {nullptr, nullptr};
+  // packed uploads: device halves of the ring and the slot ids of each half
+  void* d_stage_[2] = {nullptr, nullptr};
+  uint32_t* h_ids_[2] = {nullptr, nullptr};
+  uint32_t* d_ids_[2] = {nullptr, nullptr};
+  int upload_policy_ = SVO_UPLOAD_COALESCED;
+  bool mirror_pinned_ = false;  // incore_ / incore_attr_ registered with CUDA
+  const svo_node* mapped_nodes_ = nullptr;     // their device-side addresses
+  const svo_attrib* mapped_attribs_ = nullptr;
+  uint32_t* h_slot_ids_ = nullptr;             // page-locked, mapped
+  const uint32_t* mapped_slot_ids_ = nullptr;
   int stage_next_ = 0;
   uint32_t* d_rgba_ = nullptr;
   uint64_t d_rgba_pixels_ = 0;

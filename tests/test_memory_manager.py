@@ -180,6 +180,36 @@ def test_upload_coalescing_rule(scene):
     assert restate([0, 1, 2]) == [(0, 3)]
 
 
+def test_upload_ratio_knob(scene):
+    """The coalescing ratio the reference hard-codes (0.6): ratio 1 copies
+    every dirty slot alone, ratio 0 one range from the first to the last dirty
+    slot; ratios outside [0, 1] are refused (the reference's loop would stop
+    advancing above 1)."""
+    top = children_of(scene, 0)
+    mm = L.TreeletMemoryManagerCuda(scene, scene.info.treelet_bytes * (len(top) + 1))
+    for g in top:
+        assert mm.insertTreeletIntoIncoreBuffer(g)
+    for g in top[1::3]:
+        mm.removeTreeletFromIncoreBuffer(g)
+    for g in top[1::3]:
+        mm.insertTreeletIntoIncoreBuffer(g)
+    dirty = mm.getIncoreSlotsToUpload().tolist()
+    mm.setUploadRatio(1.0)
+    assert mm.planUploads() == [(s, 1) for s in dirty]
+    mm.setUploadRatio(0.0)
+    assert mm.planUploads() == [(dirty[0], dirty[-1] - dirty[0] + 1)]
+    mm.setUploadRatio(0.6)
+    assert len(mm.planUploads()) < len(dirty)
+    for bad in (-0.1, 1.01, float("nan")):
+        with pytest.raises(L.SvoError) as e:
+            mm.setUploadRatio(bad)
+        assert e.value.code == L.SVO_ERR_RANGE
+    with pytest.raises(L.SvoError) as e:
+        mm.setUploadPolicy(7)
+    assert e.value.code == L.SVO_ERR_NOTSUP
+    mm.setUploadPolicy(L.UPLOAD_PACKED)
+
+
 def test_insert_all_and_reset(scene):
     n = scene.info.num_treelets
     mm = L.TreeletMemoryManagerCuda(scene, scene.info.treelet_bytes * n)
