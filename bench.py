@@ -47,7 +47,10 @@ def parse():
     ap.add_argument("--workload", default="icosphere")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
-                    help="skip the batched-views and served-requests measurements")
+                    help="skip the batched, served, large-shadowed and incore-update measurements")
+    ap.add_argument("--shadow", action="store_true",
+                    help="cast one shadow ray per hit as well (svo_mm_render_shadow, seeded light); "
+                         "the metric then counts primary and shadow rays")
     return ap.parse_args()
 
 
@@ -271,7 +274,7 @@ def batched_leg(dev, reps=10):
                           "top_nodes": best.top_nodes, "graph": True}}
 
 
-def served_leg(dev, n=400, rates=(4000, 16000)):
+def served_leg(dev, n=400, rates=(4000, 16000, 64000)):
     """8 octrees served to a Poisson stream of requests
     from 64x64 to 1920x1080: batched server vs the plain per-frame kernel in the
     same request loop, all octrees resident; then the batched server with a
@@ -313,7 +316,7 @@ def served_leg(dev, n=400, rates=(4000, 16000)):
     all_rates = list(rates) + [0]
     batched = run(L.SERVE_BATCHED, 2 * footprint, all_rates)
     plain = run(L.SERVE_PLAIN, 2 * footprint, all_rates)
-    paging = run(L.SERVE_BATCHED, footprint // 2, [rates[-1]])
+    paging = run(L.SERVE_BATCHED, footprint // 2, [16000])
     return {"workload": wl.name, "description": wl.description, "requests": n, "rays": rays,
             "scene_build_s": round(build_s, 2), "octree_footprint_gb": footprint / 1e9,
             "budget_note": "the stand-in octrees total far less than the configuration's 40 GB cap; "
@@ -489,20 +492,33 @@ def main():
 
     # algorithmic bytes of one step, from the kernel's own per-ray counters
     fetches = hits = 0
+    shadow = L.shadow_cfg(L.seeded_light(1)) if args.shadow else None
     with torch.cuda.stream(stream):
         for p, o in zip(params, outs):
             hb = torch.empty(p.width * p.height * 16, dtype=torch.uint8, device=dev)
-            mm.render(p, o, hb, cfg=cfg, stream=stream)
+            sb = torch.empty(p.width * p.height * 16, dtype=torch.uint8, device=dev) if shadow else None
+            if shadow:
+                mm.render_shadow(p, o, shadow, hb, sb, cfg=cfg, stream=stream)
+            else:
+                mm.render(p, o, hb, cfg=cfg, stream=stream)
             stream.synchronize()
             h = hb.cpu().numpy().view(L.HIT_DTYPE)
             fetches += int(h["fetches"].astype(np.int64).sum())
             hits += int(h["hit"].astype(np.int64).sum())
-            del hb
+            if shadow:
+                fetches += int(sb.cpu().numpy().view(L.HIT_DTYPE)["fetches"].astype(np.int64).sum())
+            del hb, sb
     algo_bytes = 8 * fetches + 8 * hits + 4 * rays
+    primary_rays = rays
+    if shadow:
+        rays += hits  # one shadow ray per primary hit
 
     def step():
         for p, o in zip(params, outs):
-            mm.render(p, o, None, cfg=cfg, stream=stream)
+            if shadow:
+                mm.render_shadow(p, o, shadow, cfg=cfg, stream=stream)
+            else:
+                mm.render(p, o, None, cfg=cfg, stream=stream)
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
@@ -537,17 +553,26 @@ def main():
 
     # end to end through the C ABI: host output buffers, image copied back each step
     host_out = [torch.empty((p.height, p.width), dtype=torch.int32).pin_memory() for p in params]
+
+    def e2e_step():
+        for p, o, ho in zip(params, outs, host_out):
+            if shadow:  # render, then the image to pinned host memory, waited for
+                mm.render_shadow(p, o, shadow, cfg=cfg, stream=stream)
+                with torch.cuda.stream(stream):
+                    ho.copy_(o, non_blocking=True)
+                stream.synchronize()
+            else:
+                mm.render_host(p, ho, cfg=cfg, stream=stream)
+
     for _ in range(max(1, args.warmup)):
-        for p, ho in zip(params, host_out):
-            mm.render_host(p, ho, cfg=cfg, stream=stream)
+        e2e_step()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(args.steps):
-        for p, ho in zip(params, host_out):
-            mm.render_host(p, ho, cfg=cfg, stream=stream)
+        e2e_step()
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / args.steps
@@ -564,21 +589,26 @@ def main():
         traffic = None
         tp = ROOT / "profiles" / "render_frame_kernel_dram_traffic.json"
         if tp.is_file():
-            traffic = json.loads(tp.read_text()).get(wl.name)
+            traffic = json.loads(tp.read_text()).get(wl.name + ("_shadow" if shadow else ""))
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded scene generators; see libsvo_b200/scenes.py)",
-            "config": {"workload": wl.name, "description": wl.description, "rays_per_step": rays,
+            "config": {"workload": wl.name + ("_shadow" if shadow else ""),
+                       "description": wl.description + (" + one shadow ray per hit (seeded light)"
+                                                        if shadow else ""),
+                       "rays_per_step": rays, "primary_rays_per_step": primary_rays,
                        "octree_nodes": int(info.total_nodes), "treelets": int(info.num_treelets),
                        "treelet_bytes": int(info.treelet_bytes), "stack_size": wl.stack_size,
                        "l2": "flushed between steps (256 MB write)",
                        "parallelism": f"replicas x{world}", "scene_build_s": round(build_s, 2)},
             "clocks": clk,
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 4 * rays,
-                    "note": "svo_mm_render_host: launch + RGBA8 image to pinned host memory; "
+                    "d2h_bytes_per_step": 4 * primary_rays,
+                    "note": ("svo_mm_render_shadow + RGBA8 image copy to pinned host memory, waited for"
+                             if shadow else "svo_mm_render_host: launch + RGBA8 image to pinned host memory")
+                            + "; "
                             "frame parameters travel as kernel arguments"},
             "gpu_launches": args.steps * len(params),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
