@@ -126,25 +126,35 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_reference_frames(wl, nodes, attribs, seconds=10.0, max_frames=200):
+def cpu_reference_frames(wl, nodes, attribs, seconds=10.0, max_frames=200, light=None):
     """Times the reference's renderToBuffer compiled for the host (or the
-    oracle port) over whole frames of the workload, all host threads."""
+    oracle port) over whole frames of the workload, all host threads.  With
+    `light`, the primary + shadow frame (the shadow shading over the
+    reference's own sample()); shadow rays count as rays."""
     import oracle
 
     threads = os.cpu_count() or 1
     ref = oracle.reference_lib() is not None
     params = [bytes(c.frame_params()) for c in wl.cameras]
+    # shadow rays per frame = primary hits (counted once, outside the timing)
+    shadow_rays = [int(oracle.render(nodes, attribs, p, stack_size=wl.stack_size, threads=threads)[1]["hit"].sum())
+                   if light is not None else 0 for p in params]
     rays = 0
     frames = 0
     t0 = time.perf_counter()
     while True:
-        for p in params:
-            if ref:
+        for p, ns in zip(params, shadow_rays):
+            w, h = np.frombuffer(p[:8], dtype=np.uint32)
+            rays += int(w) * int(h) + ns
+            if light is not None:
+                if ref:
+                    oracle.reference_render_shadow(nodes, attribs, p, light, threads=threads)
+                else:
+                    oracle.render_shadow(nodes, attribs, p, light, stack_size=wl.stack_size, threads=threads)
+            elif ref:
                 oracle.reference_render(nodes, attribs, p, threads=threads)
             else:
                 oracle.render(nodes, attribs, p, stack_size=wl.stack_size, threads=threads)
-            w, h = np.frombuffer(p[:8], dtype=np.uint32)
-            rays += int(w) * int(h)
         frames += 1
         el = time.perf_counter() - t0
         if el >= seconds or frames >= max_frames:
@@ -153,7 +163,8 @@ def cpu_reference_frames(wl, nodes, attribs, seconds=10.0, max_frames=200):
             "kind": "reference" if ref else "port",
             "sample": f"{frames} whole frame(s) of the workload ({rays} rays) in {el:.1f} s; "
                       + ("reference treeletRenderer_rgba.cl renderToBuffer compiled for the host"
-                         if ref else "oracle restatement of sample()")}
+                         if ref else "oracle restatement of sample()")
+                      + ("; primary + shadow rays" if light is not None else "")}
 
 
 def run_reference(args, wl):
@@ -622,7 +633,8 @@ def main():
         }
         if not args.no_cpu_baseline and world == 1:
             nodes, attribs = mm.getIncoreBuffer()
-            line["cpu_baseline"] = cpu_reference_frames(wl, nodes, attribs)
+            line["cpu_baseline"] = cpu_reference_frames(wl, nodes, attribs,
+                                                        light=L.seeded_light(1) if shadow else None)
         mm.close()
         if world == 1 and not args.no_extra and args.workload == "icosphere":
             try:
