@@ -240,8 +240,10 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
         tz1 = s;
       }
     }
-    const float tc_min = cl_max(tx0, cl_max(ty0, tz0));
-    const float tc_max = cl_min(tx1, cl_min(ty1, tz1));
+    // kSigned: no NaN and no -0 among the distances (see cast_ray), so the
+    // hardware min/max equal the reference's max/min bit for bit
+    const float tc_min = kSigned ? fmaxf(tx0, fmaxf(ty0, tz0)) : cl_max(tx0, cl_max(ty0, tz0));
+    const float tc_max = kSigned ? fminf(tx1, fminf(ty1, tz1)) : cl_min(tx1, cl_min(ty1, tz1));
 
     if (!in_pool) {
       h.flags = SVO_HITFLAG_BOUNDS;
@@ -253,10 +255,11 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
     const uint32_t bx = fbx != 0.0f, by = fby != 0.0f, bz = fbz != 0.0f;
     const uint32_t ci = (bx << 2) | (by << 1) | bz;
     const uint32_t masks = nd.y;
-    if ((masks >> (ci + 8u)) & 1u) {
-      const uint32_t below = __popc((masks >> 8) & ((1u << ci) - 1u));
+    const uint32_t sh = masks >> ci;  // bit 8: valid, bit 0: leaf
+    if (sh & 0x100u) {
+      const uint32_t below = __popc(masks & ((0x100u << ci) - 0x100u));
       const uint32_t child = (kFlat ? 0u : node) + nd.x + below;
-      const bool leaf = (masks >> ci) & 1u;
+      const bool leaf = sh & 1u;
       const bool lod = kFlat ? (__fmul_rn(tsr, tc_max) > sx2)
                              : (__fmul_rn(tsr, tc_min) > sx2 || scale == 1);
       if (leaf || lod) {
@@ -352,7 +355,14 @@ __device__ __forceinline__ RayHit cast_ray(const Fetch& fetch, uint64_t num_node
   const float rx = __frcp_rn(dx), px = __fmul_rn(-o[0], rx);
   const float ry = __frcp_rn(dy), py = __fmul_rn(-o[1], ry);
   const float rz = __frcp_rn(dz), pz = __fmul_rn(-o[2], rz);
-  if (isfinite(rx) && isfinite(ry) && isfinite(rz))
+  // kSigned needs finite reciprocals.  It also takes the hardware min/max:
+  // with finite r, a slab distance r * plane + p is -0 only for the plane at
+  // 0 when the origin coordinate is -0 and r < 0 (x + (-x) rounds to +0), so
+  // rays with a -0 origin coordinate keep the reference's compare/select.
+  const bool neg_zero = __float_as_uint(o[0]) == 0x80000000u ||
+                        __float_as_uint(o[1]) == 0x80000000u ||
+                        __float_as_uint(o[2]) == 0x80000000u;
+  if (isfinite(rx) && isfinite(ry) && isfinite(rz) && !neg_zero)
     descend<kFlat, true>(fetch, num_nodes, o, dx, dy, dz, rx, px, ry, py, rz, pz, t_min, t_max,
                          tsr, S, stack, stride, h);
   else

@@ -5,13 +5,14 @@ import libsvo_b200 as L
 
 
 def edge_rays(n_random=20000, seed=0):
-    """Axis-aligned, zero-component, grazing, inside-the-cube and random rays."""
+    """Axis-aligned, zero-component, grazing, inside-the-cube, -0.0-origin and
+    random rays."""
     rng = np.random.default_rng(seed)
     o, d = [], []
     for origin in ([0.1, 0.2, 3.0], [0.0, 0.0, 2.0], [0.0, 0.0, 0.0], [0.25, -0.25, 0.1],
-                   [0.5, 0.5, 2.0], [-0.5, 0.3, -3.0]):
+                   [0.5, 0.5, 2.0], [-0.5, 0.3, -3.0], [-0.0, 0.25, 2.0], [-0.0, -0.0, -2.5]):
         for dirv in ([0, 0, -1], [0, 0, 1], [1, 0, 0], [0, -1, 0], [0, 0.00005, -1], [1e-6, 0, -1],
-                     [-0.0, 0.0, -1.0], [0.3, 0.4, -0.866]):
+                     [-0.0, 0.0, -1.0], [0.3, 0.4, -0.866], [-0.3, -0.2, 0.9], [-0.01, 0.02, -1.0]):
             o.append(origin)
             v = np.asarray(dirv, dtype=np.float64)
             d.append(v / np.linalg.norm(v))
