@@ -356,7 +356,15 @@ int svo_mm_render_shadow(svo_mm* mm, const svo_frame_params* params, const svo_t
                          const svo_shadow_cfg* shadow, uint32_t* d_rgba, svo_hit* d_hits,
                          svo_hit* d_shadow_hits, void* stream);
 
-/* Waits for `stream` and returns the manager's accumulated counters
+/* Non-blocking svo_mm_render_host for frame loops: the frame is cast on
+ * `stream` into one of two device images and copied to h_rgba on a second
+ * stream, so the copy of one frame overlaps the cast of the next.  h_rgba
+ * (page-locked host memory, W*H RGBA8) holds the frame once svo_mm_sync
+ * returns; it must stay valid until then. */
+int svo_mm_render_host_async(svo_mm* mm, const svo_frame_params* params, const svo_trace_cfg* cfg,
+                             uint32_t* h_rgba, void* stream);
+/* Waits for `stream` and for every svo_mm_render_host_async copy, and
+ * returns the manager's accumulated counters
  * (capped rays = the watchdog status word), then clears them. */
 int svo_mm_sync(svo_mm* mm, void* stream, svo_stats* out);
 

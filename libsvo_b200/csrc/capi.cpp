@@ -511,11 +511,24 @@ int svo_mm_render_host(svo_mm* mm, const svo_frame_params* params, const svo_tra
   return SVO_OK;
 }
 
+int svo_mm_render_host_async(svo_mm* mm, const svo_frame_params* params, const svo_trace_cfg* cfg,
+                             uint32_t* h_rgba, void* stream) {
+  if (!mm || !params || !h_rgba || !mm->impl.device_ready()) return SVO_ERR_INVALID;
+  int rc = check_cfg(cfg);
+  if (rc != SVO_OK) return rc;
+  rc = check_frame_mode(params->mode, cfg->traversal);
+  if (rc != SVO_OK) return rc;
+  cudaStream_t s = stream ? (cudaStream_t)stream : mm->impl.render_stream();
+  return guarded([&] { return mm->impl.render_to_host_async(*params, *cfg, h_rgba, s); });
+}
+
 int svo_mm_sync(svo_mm* mm, void* stream, svo_stats* out) {
   if (!mm || !mm->impl.device_ready()) return SVO_ERR_INVALID;
   cudaStream_t s = stream ? (cudaStream_t)stream : mm->impl.render_stream();
   svo_stats st;
   SVO_CUDA_TRY(cudaStreamSynchronize(s));
+  const int rc = mm->impl.wait_host_frames();
+  if (rc != SVO_OK) return rc;
   SVO_CUDA_TRY(cudaMemcpy(&st, mm->impl.device_stats(), sizeof(st), cudaMemcpyDeviceToHost));
   SVO_CUDA_TRY(cudaMemset(mm->impl.device_stats(), 0, sizeof(svo_stats)));
   if (out) *out = st;

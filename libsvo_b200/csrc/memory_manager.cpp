@@ -7,6 +7,7 @@
 #include <deque>
 
 #include "errors.h"
+#include "render.h"
 #include "upload.h"
 
 namespace svo {
@@ -239,6 +240,13 @@ TreeletMemoryManagerCuda::~TreeletMemoryManagerCuda() {
     cudaHostUnregister(incore_attr_);
   }
   if (h_slot_ids_) cudaFreeHost(h_slot_ids_);
+  if (d2h_stream_) cudaStreamSynchronize(d2h_stream_);
+  for (int i = 0; i < 2; ++i) {
+    cudaFree(d_img_[i]);
+    if (cast_done_[i]) cudaEventDestroy(cast_done_[i]);
+    if (copy_done_[i]) cudaEventDestroy(copy_done_[i]);
+  }
+  if (d2h_stream_) cudaStreamDestroy(d2h_stream_);
   if (owns_device_) {
     cudaFree(d_nodes_);
     cudaFree(d_attribs_);
@@ -489,6 +497,49 @@ int TreeletMemoryManagerCuda::rgba_scratch(uint64_t pixels, uint32_t** out) {
     d_rgba_pixels_ = pixels;
   }
   *out = d_rgba_;
+  return SVO_OK;
+}
+
+int TreeletMemoryManagerCuda::render_to_host_async(const svo_frame_params& p,
+                                                   const svo_trace_cfg& cfg, uint32_t* h_rgba,
+                                                   cudaStream_t stream) {
+  const uint64_t pixels = (uint64_t)p.width * p.height;
+  if (pixels == 0) return SVO_OK;
+  if (!d2h_stream_) {
+    SVO_CUDA_TRY(cudaStreamCreateWithFlags(&d2h_stream_, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; ++i) {
+      SVO_CUDA_TRY(cudaEventCreateWithFlags(&cast_done_[i], cudaEventDisableTiming));
+      SVO_CUDA_TRY(cudaEventCreateWithFlags(&copy_done_[i], cudaEventDisableTiming));
+    }
+  }
+  const int k = img_next_;
+  img_next_ ^= 1;
+  if (pixels > d_img_pixels_[k]) {
+    SVO_CUDA_TRY(cudaStreamSynchronize(d2h_stream_));  // the image may still be copied out
+    SVO_CUDA_TRY(cudaStreamSynchronize(stream));
+    cudaFree(d_img_[k]);
+    d_img_[k] = nullptr;
+    d_img_pixels_[k] = 0;
+    SVO_CUDA_TRY(cudaMalloc(&d_img_[k], pixels * sizeof(uint32_t)));
+    d_img_pixels_[k] = pixels;
+  }
+  // the cast may overwrite image k once its previous copy has left
+  SVO_CUDA_TRY(cudaStreamWaitEvent(stream, copy_done_[k], 0));
+  int rc = wait_uploads(stream);
+  if (rc != SVO_OK) return rc;
+  rc = launch_render(d_nodes_, d_attribs_, incore_nodes(), p, cfg, d_img_[k], nullptr, d_stats_,
+                     stream);
+  if (rc != SVO_OK) return rc;
+  SVO_CUDA_TRY(cudaEventRecord(cast_done_[k], stream));
+  SVO_CUDA_TRY(cudaStreamWaitEvent(d2h_stream_, cast_done_[k], 0));
+  SVO_CUDA_TRY(cudaMemcpyAsync(h_rgba, d_img_[k], pixels * sizeof(uint32_t),
+                               cudaMemcpyDeviceToHost, d2h_stream_));
+  SVO_CUDA_TRY(cudaEventRecord(copy_done_[k], d2h_stream_));
+  return SVO_OK;
+}
+
+int TreeletMemoryManagerCuda::wait_host_frames() {
+  if (d2h_stream_) SVO_CUDA_TRY(cudaStreamSynchronize(d2h_stream_));
   return SVO_OK;
 }
 

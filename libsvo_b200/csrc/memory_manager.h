@@ -133,6 +133,13 @@ class TreeletMemoryManagerCuda : public TreeletMemoryManager {
   int wait_uploads(cudaStream_t stream);
   // Device RGBA scratch for host-output renders (grown on demand).
   int rgba_scratch(uint64_t pixels, uint32_t** out);
+  // Asynchronous host-output frames: cast on `stream` into one of two device
+  // images, copied to `h_rgba` on a second stream, so the copy of a frame
+  // overlaps the cast of the next.  wait_host_frames() blocks until every
+  // copy issued so far has landed.
+  int render_to_host_async(const svo_frame_params& p, const svo_trace_cfg& cfg, uint32_t* h_rgba,
+                           cudaStream_t stream);
+  int wait_host_frames();
   // Device feedback-record scratch for analysis passes (grown on demand).
   int feedback_scratch(uint64_t records, svo_feedback** out);
 
@@ -168,6 +175,13 @@ class TreeletMemoryManagerCuda : public TreeletMemoryManager {
   int stage_next_ = 0;
   uint32_t* d_rgba_ = nullptr;
   uint64_t d_rgba_pixels_ = 0;
+  // asynchronous host-output frames
+  uint32_t* d_img_[2] = {nullptr, nullptr};
+  uint64_t d_img_pixels_[2] = {0, 0};
+  cudaStream_t d2h_stream_ = nullptr;
+  cudaEvent_t cast_done_[2] = {nullptr, nullptr};
+  cudaEvent_t copy_done_[2] = {nullptr, nullptr};
+  int img_next_ = 0;
   svo_feedback* d_feedback_ = nullptr;
   uint64_t d_feedback_records_ = 0;
 };

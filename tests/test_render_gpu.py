@@ -203,3 +203,22 @@ def test_icosphere_frame_matches_oracle(cuda):
         assert_hits_equal(hits, o_hits, "icosphere")
         assert np.array_equal(rgba, o_rgba)
     mm.close()
+
+
+def test_async_host_frames_match_device(menger_mm):
+    """svo_mm_render_host_async: frames of different sizes in a row, each
+    copied back on the second stream; every host image equals the device
+    render, and the watchdog counters still add up."""
+    import torch
+
+    menger_mm.sync()
+    frames = [L.orbit_camera(s, w, h).frame_params() for s, (w, h) in
+              enumerate([(300, 200), (64, 48), (512, 512), (300, 200), (17, 13)])]
+    outs = [torch.empty((p.height, p.width), dtype=torch.int32).pin_memory() for p in frames]
+    for p, o in zip(frames, outs):
+        menger_mm.render_host_async(p, o)
+    st = menger_mm.sync()
+    for p, o in zip(frames, outs):
+        rgba, _ = gpu_frame(menger_mm, p)
+        assert np.array_equal(o.numpy().view(np.uint32), rgba)
+    assert st.bounds_errors == 0
