@@ -233,6 +233,24 @@ def run_reference(args, wl):
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(x: float, world: int, device) -> float:
+    """The slowest rank's value (every rank takes part; world 1: x itself)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_mrays_per_s(world: int, rays_per_rank: int, ms_per_step: float) -> float:
+    """Whole-job throughput: every rank casts its own replica of the step's
+    rays, and the step takes the slowest rank's time."""
+    return world * rays_per_rank / (ms_per_step * 1e-3) / 1e6
+
+
 def _event_ms(torch, fn, reps):
     fn()
     torch.cuda.synchronize()
@@ -555,12 +573,8 @@ def main():
         dist.barrier()
     clk = clocks.stop()
     kernel_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    ms = statistics.mean(kernel_ms)
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * rays / (ms * 1e-3) / 1e6
+    ms = max_over_ranks(statistics.mean(kernel_ms), world, dev)
+    value = job_mrays_per_s(world, rays, ms)
 
     # end to end through the C ABI: host output buffers, image copied back each step
     host_out = [torch.empty((p.height, p.width), dtype=torch.int32).pin_memory() for p in params]
@@ -591,12 +605,8 @@ def main():
     for i in range(args.steps):
         e2e_step(i)
     st = mm.sync(stream)  # every image is in host memory; counters of the e2e frames
-    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * rays / (e2e_ms * 1e-3) / 1e6
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps, world, dev)
+    e2e_value = job_mrays_per_s(world, rays, e2e_ms)
 
     if rank == 0:
         peak, peak_kind = load_peaks()
