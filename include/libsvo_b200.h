@@ -175,6 +175,32 @@ int svo_device_scene_counts(const svo_device_scene* scene, uint64_t* octree_node
                             uint64_t* overlaps);
 void svo_device_scene_destroy(svo_device_scene* scene);
 
+/* svo_scene_build_mesh / svo_device_scene_build_mesh with per-vertex normals
+ * and colours (num_vertices x 3 floats each, colours in [0, 1]; both or
+ * neither).  A leaf then gets the reference's attributes
+ * (src/attribute_generators/Ag_colorAndNormalsTriangles.cpp:110-155 with
+ * src/BuilderTriangleFace.cpp:211-329): for each overlapping triangle the
+ * barycentric (u, v) of the voxel centre along the triangle's mean vertex
+ * normal, clamped to [0, 1], the normalised interpolated vertex normal and the
+ * interpolated colour; their mean over the triangles, the normal normalised.
+ * Without them: normalised sum of the face normals, colour = normal*0.5+0.5. */
+int svo_scene_build_mesh_attributed(const float* h_vertices, const float* h_normals,
+                                    const float* h_colors, uint64_t num_vertices,
+                                    const uint32_t* h_triangles, uint64_t num_triangles,
+                                    uint32_t depth, uint32_t treelet_levels,
+                                    uint32_t treelet_bytes, int32_t threads, svo_scene** out);
+int svo_device_scene_build_mesh_attributed(const float* h_vertices, const float* h_normals,
+                                           const float* h_colors, uint64_t num_vertices,
+                                           const uint32_t* h_triangles, uint64_t num_triangles,
+                                           uint32_t depth, uint32_t treelet_levels, void* stream,
+                                           svo_device_scene** out);
+/* Per-vertex attributes for a mesh: normals = normalised sum of the adjacent
+ * (area-weighted) face normals; colours = a seeded smooth field of the
+ * position.  Writes num_vertices x 3 floats to each output. */
+int svo_mesh_vertex_attributes(const float* h_vertices, uint64_t num_vertices,
+                               const uint32_t* h_triangles, uint64_t num_triangles, uint64_t seed,
+                               float* h_normals, float* h_colors);
+
 /* Seeded synthetic meshes (inputs for svo_scene_build_mesh).  The reference
  * voxelises scanned PLY meshes that are not part of it; these stand in with
  * the triangle counts of the benchmark configurations.  Call *_size first.

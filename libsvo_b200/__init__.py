@@ -190,6 +190,11 @@ _SIGS = {
     "svo_batcher_autotune": ([_vp, _u32, _vp, _P(svo_batch_cfg), _P(_f32)], ctypes.c_int),
     "svo_batcher_size": ([_vp, _P(_u64), _P(_u64)], ctypes.c_int),
     "svo_device_scene_build_mesh": ([_vp, _u64, _vp, _u64, _u32, _u32, _vp, _P(_vp)], ctypes.c_int),
+    "svo_device_scene_build_mesh_attributed": ([_vp, _vp, _vp, _u64, _vp, _u64, _u32, _u32, _vp, _P(_vp)],
+                                               ctypes.c_int),
+    "svo_scene_build_mesh_attributed": ([_vp, _vp, _vp, _u64, _vp, _u64, _u32, _u32, _u32, _i32, _P(_vp)],
+                                        ctypes.c_int),
+    "svo_mesh_vertex_attributes": ([_vp, _u64, _vp, _u64, _u64, _vp, _vp], ctypes.c_int),
     "svo_device_scene_info_get": ([_vp, _P(svo_scene_info)], ctypes.c_int),
     "svo_device_scene_buffers": ([_vp, _P(_vp), _P(_vp), _P(_u64)], ctypes.c_int),
     "svo_device_scene_copy": ([_vp, _u64, _u64, _vp, _vp], ctypes.c_int),
@@ -328,6 +333,30 @@ def terrain(grid: int, octaves=6, base=-0.45, height=0.3, frequency=2.0, seed=1)
     return v, t
 
 
+def vertex_attributes(vertices: np.ndarray, triangles: np.ndarray, seed=1):
+    """(normals, colours), float32 (V, 3) each: area-weighted vertex normals
+    and a seeded smooth colour field (svo_mesh_vertex_attributes)."""
+    v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
+    t = np.ascontiguousarray(triangles, dtype=np.uint32).reshape(-1, 3)
+    n = np.zeros_like(v)
+    c = np.zeros_like(v)
+    _check(_L.svo_mesh_vertex_attributes(_np_ptr(v), v.shape[0], _np_ptr(t), t.shape[0], seed, _np_ptr(n),
+                                         _np_ptr(c)), "svo_mesh_vertex_attributes")
+    return n, c
+
+
+def _vertex_arrays(normals, colors, nv):
+    if (normals is None) != (colors is None):
+        raise ValueError("pass both per-vertex normals and colours, or neither")
+    if normals is None:
+        return None, None
+    n = np.ascontiguousarray(normals, dtype=np.float32).reshape(-1, 3)
+    c = np.ascontiguousarray(colors, dtype=np.float32).reshape(-1, 3)
+    if n.shape[0] != nv or c.shape[0] != nv:
+        raise ValueError("one normal and one colour per vertex")
+    return n, c
+
+
 # ---- scenes ----------------------------------------------------------------
 class Scene:
     """An octree cut into treelets (what TreeletBuildManager writes)."""
@@ -344,13 +373,18 @@ class Scene:
 
     @classmethod
     def from_mesh(cls, vertices: np.ndarray, triangles: np.ndarray, depth: int,
-                  treelet_levels=0, treelet_bytes=0, threads=0) -> "Scene":
+                  treelet_levels=0, treelet_bytes=0, threads=0, normals: np.ndarray | None = None,
+                  colors: np.ndarray | None = None) -> "Scene":
+        """Voxelises a mesh.  With per-vertex normals and colours the leaves
+        get the reference's interpolated attributes; without, face normals."""
         v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
         t = np.ascontiguousarray(triangles, dtype=np.uint32).reshape(-1, 3)
+        n, c = _vertex_arrays(normals, colors, v.shape[0])
         h = ctypes.c_void_p()
-        _check(_L.svo_scene_build_mesh(_np_ptr(v), v.shape[0], _np_ptr(t), t.shape[0], depth,
-                                       treelet_levels, treelet_bytes, threads, ctypes.byref(h)),
-               "svo_scene_build_mesh")
+        _check(_L.svo_scene_build_mesh_attributed(
+            _np_ptr(v), None if n is None else _np_ptr(n), None if c is None else _np_ptr(c), v.shape[0],
+            _np_ptr(t), t.shape[0], depth, treelet_levels, treelet_bytes, threads, ctypes.byref(h)),
+            "svo_scene_build_mesh")
         return cls(h.value)
 
     @classmethod
@@ -406,13 +440,15 @@ class DeviceScene:
     produces, without the host holding the octree."""
 
     def __init__(self, vertices: np.ndarray, triangles: np.ndarray, depth: int, treelet_levels=0,
-                 stream=None):
+                 stream=None, normals: np.ndarray | None = None, colors: np.ndarray | None = None):
         v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
         t = np.ascontiguousarray(triangles, dtype=np.uint32).reshape(-1, 3)
+        n, c = _vertex_arrays(normals, colors, v.shape[0])
         h = ctypes.c_void_p()
-        _check(_L.svo_device_scene_build_mesh(_np_ptr(v), v.shape[0], _np_ptr(t), t.shape[0], depth,
-                                              treelet_levels, _stream_ptr(stream), ctypes.byref(h)),
-               "svo_device_scene_build_mesh")
+        _check(_L.svo_device_scene_build_mesh_attributed(
+            _np_ptr(v), None if n is None else _np_ptr(n), None if c is None else _np_ptr(c), v.shape[0],
+            _np_ptr(t), t.shape[0], depth, treelet_levels, _stream_ptr(stream), ctypes.byref(h)),
+            "svo_device_scene_build_mesh")
         self._h = h
 
     @property

@@ -98,36 +98,48 @@ int svo_scene_build_menger(uint32_t level, uint32_t depth, uint64_t seed, uint32
   });
 }
 
-int svo_scene_build_mesh(const float* h_vertices, uint64_t num_vertices,
-                         const uint32_t* h_triangles, uint64_t num_triangles, uint32_t depth,
-                         uint32_t treelet_levels, uint32_t treelet_bytes, int32_t threads,
-                         svo_scene** out) {
+int svo_scene_build_mesh_attributed(const float* h_vertices, const float* h_normals,
+                                    const float* h_colors, uint64_t num_vertices,
+                                    const uint32_t* h_triangles, uint64_t num_triangles,
+                                    uint32_t depth, uint32_t treelet_levels,
+                                    uint32_t treelet_bytes, int32_t threads, svo_scene** out) {
   if (!out || !h_vertices || !h_triangles) return SVO_ERR_INVALID;
   *out = nullptr;
   return guarded([&] {
     std::vector<uint64_t> codes;
     std::vector<svo_attrib> attribs;
-    int rc = svo::build_mesh_leaves(h_vertices, num_vertices, h_triangles, num_triangles, depth,
-                                    threads, codes, attribs);
+    int rc = svo::build_mesh_leaves(h_vertices, h_normals, h_colors, num_vertices, h_triangles,
+                                    num_triangles, depth, threads, codes, attribs);
     if (rc != SVO_OK) return rc;
     return build_scene(depth, codes, attribs, treelet_levels, treelet_bytes, out);
   });
+}
+
+int svo_scene_build_mesh(const float* h_vertices, uint64_t num_vertices,
+                         const uint32_t* h_triangles, uint64_t num_triangles, uint32_t depth,
+                         uint32_t treelet_levels, uint32_t treelet_bytes, int32_t threads,
+                         svo_scene** out) {
+  return svo_scene_build_mesh_attributed(h_vertices, nullptr, nullptr, num_vertices, h_triangles,
+                                         num_triangles, depth, treelet_levels, treelet_bytes,
+                                         threads, out);
 }
 
 struct svo_device_scene {
   svo::DeviceScene impl;
 };
 
-int svo_device_scene_build_mesh(const float* h_vertices, uint64_t num_vertices,
-                                const uint32_t* h_triangles, uint64_t num_triangles,
-                                uint32_t depth, uint32_t treelet_levels, void* stream,
-                                svo_device_scene** out) {
+int svo_device_scene_build_mesh_attributed(const float* h_vertices, const float* h_normals,
+                                           const float* h_colors, uint64_t num_vertices,
+                                           const uint32_t* h_triangles, uint64_t num_triangles,
+                                           uint32_t depth, uint32_t treelet_levels, void* stream,
+                                           svo_device_scene** out) {
   if (!out || !h_vertices || !h_triangles) return SVO_ERR_INVALID;
+  if ((h_normals == nullptr) != (h_colors == nullptr)) return SVO_ERR_INVALID;
   *out = nullptr;
   return guarded([&] {
     svo_device_scene* s = new svo_device_scene;
-    const int rc = s->impl.build_mesh(h_vertices, num_vertices, h_triangles, num_triangles, depth,
-                                      treelet_levels, (cudaStream_t)stream);
+    const int rc = s->impl.build_mesh(h_vertices, h_normals, h_colors, num_vertices, h_triangles,
+                                      num_triangles, depth, treelet_levels, (cudaStream_t)stream);
     if (rc != SVO_OK) {
       delete s;
       return rc;
@@ -135,6 +147,15 @@ int svo_device_scene_build_mesh(const float* h_vertices, uint64_t num_vertices,
     *out = s;
     return SVO_OK;
   });
+}
+
+int svo_device_scene_build_mesh(const float* h_vertices, uint64_t num_vertices,
+                                const uint32_t* h_triangles, uint64_t num_triangles,
+                                uint32_t depth, uint32_t treelet_levels, void* stream,
+                                svo_device_scene** out) {
+  return svo_device_scene_build_mesh_attributed(h_vertices, nullptr, nullptr, num_vertices,
+                                                h_triangles, num_triangles, depth, treelet_levels,
+                                                stream, out);
 }
 
 int svo_device_scene_info_get(const svo_device_scene* scene, svo_scene_info* out) {

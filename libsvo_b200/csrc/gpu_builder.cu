@@ -331,6 +331,124 @@ __global__ void leaf_reduce_kernel(const uint64_t* __restrict__ keys, uint64_t n
   attribs[r] = svo_attrib{packed, packed};  // colour = normal * 0.5 + 0.5 = the packed normal
 }
 
+__device__ __forceinline__ uint32_t compact3(uint64_t x) {
+  x &= 0x1249249249249249ull;
+  x = (x ^ (x >> 2)) & 0x10c30c30c30c30c3ull;
+  x = (x ^ (x >> 4)) & 0x100f00f00f00f00full;
+  x = (x ^ (x >> 8)) & 0x1f0000ff0000ffull;
+  x = (x ^ (x >> 16)) & 0x1f00000000ffffull;
+  x = (x ^ (x >> 32)) & 0x1fffffull;
+  return (uint32_t)x;
+}
+
+// leaf_contribution of the host builder (csrc/scene.cpp), operation for
+// operation: the reference's interpolated vertex normal and colour of one
+// triangle at the voxel centre c.
+__device__ void leaf_contribution(const float* __restrict__ V, const float* __restrict__ N,
+                                  const float* __restrict__ C, const uint32_t* tri,
+                                  const float c[3], float n_out[3], float c_out[3]) {
+  const float* p0 = V + 3 * (uint64_t)tri[0];
+  const float* p1 = V + 3 * (uint64_t)tri[1];
+  const float* p2 = V + 3 * (uint64_t)tri[2];
+  const float* n0 = N + 3 * (uint64_t)tri[0];
+  const float* n1 = N + 3 * (uint64_t)tri[1];
+  const float* n2 = N + 3 * (uint64_t)tri[2];
+  const float* c0 = C + 3 * (uint64_t)tri[0];
+  const float* c1 = C + 3 * (uint64_t)tri[1];
+  const float* c2 = C + 3 * (uint64_t)tri[2];
+  float d[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) d[k] = __fdiv_rn(__fadd_rn(__fadd_rn(n0[k], n1[k]), n2[k]), 3.0f);
+  float len = len3(d[0], d[1], d[2]);
+  if (len > 0.0f) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) d[k] = __fdiv_rn(d[k], len);
+  }
+  const float e1[3] = {__fsub_rn(p1[0], p0[0]), __fsub_rn(p1[1], p0[1]), __fsub_rn(p1[2], p0[2])};
+  const float e2[3] = {__fsub_rn(p2[0], p0[0]), __fsub_rn(p2[1], p0[1]), __fsub_rn(p2[2], p0[2])};
+  const float pv[3] = {__fsub_rn(__fmul_rn(d[1], e2[2]), __fmul_rn(d[2], e2[1])),
+                       __fsub_rn(__fmul_rn(d[2], e2[0]), __fmul_rn(d[0], e2[2])),
+                       __fsub_rn(__fmul_rn(d[0], e2[1]), __fmul_rn(d[1], e2[0]))};
+  const float det = dot3(e1[0], e1[1], e1[2], pv);
+  float u = 0.0f, v = 0.0f;
+  if (!(det > -1e-8f && det < 1e-8f)) {
+    const float inv = __fdiv_rn(1.0f, det);
+    const float tv[3] = {__fsub_rn(c[0], p0[0]), __fsub_rn(c[1], p0[1]), __fsub_rn(c[2], p0[2])};
+    u = __fmul_rn(dot3(tv[0], tv[1], tv[2], pv), inv);
+    const float qv[3] = {__fsub_rn(__fmul_rn(tv[1], e1[2]), __fmul_rn(tv[2], e1[1])),
+                         __fsub_rn(__fmul_rn(tv[2], e1[0]), __fmul_rn(tv[0], e1[2])),
+                         __fsub_rn(__fmul_rn(tv[0], e1[1]), __fmul_rn(tv[1], e1[0]))};
+    v = __fmul_rn(dot3(d[0], d[1], d[2], qv), inv);
+  }
+  u = u < 0.0f ? 0.0f : (u > 1.0f ? 1.0f : u);
+  v = v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v);
+  const float w = __fsub_rn(__fsub_rn(1.0f, u), v);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    n_out[k] = __fadd_rn(__fadd_rn(__fmul_rn(n0[k], w), __fmul_rn(n1[k], u)), __fmul_rn(n2[k], v));
+    c_out[k] = __fadd_rn(__fadd_rn(__fmul_rn(c0[k], w), __fmul_rn(c1[k], u)), __fmul_rn(c2[k], v));
+  }
+  len = len3(n_out[0], n_out[1], n_out[2]);
+  if (len > 0.0f) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) n_out[k] = __fdiv_rn(n_out[k], len);
+  }
+}
+
+// One thread per run of equal codes, with per-vertex attributes: the mean of
+// the triangles' interpolated normals (normalised) and colours.
+__global__ void leaf_reduce_attr_kernel(const uint64_t* __restrict__ keys, uint64_t n,
+                                        uint32_t tri_bits, uint64_t chunk_base, uint32_t depth,
+                                        const uint32_t* __restrict__ heads,
+                                        const uint32_t* __restrict__ run_of,
+                                        const float* __restrict__ V, const float* __restrict__ N,
+                                        const float* __restrict__ C,
+                                        const uint32_t* __restrict__ T,
+                                        uint64_t* __restrict__ codes,
+                                        svo_attrib* __restrict__ attribs) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !heads[i]) return;
+  const uint64_t code = keys[i] >> tri_bits;
+  const uint64_t full = chunk_base | code;
+  const uint64_t tmask = (1ull << tri_bits) - 1ull;
+  const float inv_r = __fdiv_rn(1.0f, (float)(1u << depth));
+  const uint32_t x = compact3(full >> 2), y = compact3(full >> 1), z = compact3(full);
+  const float c[3] = {__fadd_rn(-0.5f, __fmul_rn(__fadd_rn((float)x, 0.5f), inv_r)),
+                      __fadd_rn(-0.5f, __fmul_rn(__fadd_rn((float)y, 0.5f), inv_r)),
+                      __fadd_rn(-0.5f, __fmul_rn(__fadd_rn((float)z, 0.5f), inv_r))};
+  float sn[3] = {0.0f, 0.0f, 0.0f}, sc[3] = {0.0f, 0.0f, 0.0f};
+  uint64_t j = i;
+  do {
+    const uint64_t t = keys[j] & tmask;
+    float nn[3], cc[3];
+    leaf_contribution(V, N, C, T + 3 * t, c, nn, cc);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      sn[k] = __fadd_rn(sn[k], nn[k]);
+      sc[k] = __fadd_rn(sc[k], cc[k]);
+    }
+    ++j;
+  } while (j < n && (keys[j] >> tri_bits) == code);
+  const float cnt = (float)(j - i);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    sn[k] = __fdiv_rn(sn[k], cnt);
+    sc[k] = __fdiv_rn(sc[k], cnt);
+  }
+  const float len = len3(sn[0], sn[1], sn[2]);
+  if (len > 0.0f) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) sn[k] = __fdiv_rn(sn[k], len);
+  } else {
+    sn[0] = 0.0f;
+    sn[1] = 0.0f;
+    sn[2] = 1.0f;
+  }
+  const uint32_t r = run_of[i];
+  codes[r] = full;
+  attribs[r] = svo_attrib{pack_normal(sn[0], sn[1], sn[2]), pack_color(sc[0], sc[1], sc[2])};
+}
+
 // ---- 4. levels -------------------------------------------------------------------
 
 __global__ void parent_heads_kernel(const uint64_t* __restrict__ codes, uint64_t n,
@@ -594,11 +712,13 @@ int scan_flags(const uint32_t* flags, uint32_t* pos, uint64_t n, uint64_t* total
 
 }  // namespace
 
-int DeviceScene::build_mesh(const float* h_vertices, uint64_t nv, const uint32_t* h_triangles,
+int DeviceScene::build_mesh(const float* h_vertices, const float* h_normals,
+                            const float* h_colors, uint64_t nv, const uint32_t* h_triangles,
                             uint64_t nt, uint32_t depth_, uint32_t treelet_levels,
                             cudaStream_t st) {
   if (depth_ < 1 || depth_ > 21) return SVO_ERR_RANGE;
   if (nt == 0 || nv == 0) return SVO_ERR_INVALID;
+  if ((h_normals == nullptr) != (h_colors == nullptr)) return SVO_ERR_INVALID;
   for (uint64_t i = 0; i < 3 * nt; ++i)
     if (h_triangles[i] >= nv) return SVO_ERR_INVALID;
   depth = depth_;
@@ -609,12 +729,19 @@ int DeviceScene::build_mesh(const float* h_vertices, uint64_t nv, const uint32_t
   if (chunk_levels > 3 || 3 * (depth - chunk_levels) + tri_bits > 64) return SVO_ERR_RANGE;
   chunk_levels = std::min(chunk_levels, depth);
 
-  DevBuf<float> dV, dFn;
+  DevBuf<float> dV, dFn, dN, dC;
   DevBuf<uint32_t> dT;
   GB_TRY(dV.alloc(3 * nv));
   GB_TRY(dT.alloc(3 * nt));
   GB_TRY(dFn.alloc(3 * nt));
   GB_TRY(cudaMemcpyAsync(dV.p, h_vertices, 3 * nv * sizeof(float), cudaMemcpyHostToDevice, st));
+  const bool attributed = h_normals != nullptr;
+  if (attributed) {
+    GB_TRY(dN.alloc(3 * nv));
+    GB_TRY(dC.alloc(3 * nv));
+    GB_TRY(cudaMemcpyAsync(dN.p, h_normals, 3 * nv * sizeof(float), cudaMemcpyHostToDevice, st));
+    GB_TRY(cudaMemcpyAsync(dC.p, h_colors, 3 * nv * sizeof(float), cudaMemcpyHostToDevice, st));
+  }
   GB_TRY(cudaMemcpyAsync(dT.p, h_triangles, 3 * nt * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
   face_normals_kernel<<<grid_of(nt, 256), 256, 0, st>>>(dV.p, dT.p, nt, dFn.p);
   GB_TRY(cudaGetLastError());
@@ -689,9 +816,14 @@ int DeviceScene::build_mesh(const float* h_vertices, uint64_t nv, const uint32_t
     if (rc != SVO_OK) return rc;
     GB_TRY(chunk_codes.back().alloc(M));
     GB_TRY(chunk_attr.back().alloc(M));
-    leaf_reduce_kernel<<<grid_of(P, 256), 256, 0, st>>>(
-        sorted.p, P, tri_bits, (uint64_t)ci << ch.shift, heads.p, run_of.p, dFn.p,
-        chunk_codes.back().p, chunk_attr.back().p);
+    if (attributed)
+      leaf_reduce_attr_kernel<<<grid_of(P, 256), 256, 0, st>>>(
+          sorted.p, P, tri_bits, (uint64_t)ci << ch.shift, depth, heads.p, run_of.p, dV.p, dN.p,
+          dC.p, dT.p, chunk_codes.back().p, chunk_attr.back().p);
+    else
+      leaf_reduce_kernel<<<grid_of(P, 256), 256, 0, st>>>(
+          sorted.p, P, tri_bits, (uint64_t)ci << ch.shift, heads.p, run_of.p, dFn.p,
+          chunk_codes.back().p, chunk_attr.back().p);
     GB_TRY(cudaGetLastError());
     chunk_leaves.back() = M;
   }
@@ -700,6 +832,8 @@ int DeviceScene::build_mesh(const float* h_vertices, uint64_t nv, const uint32_t
   dV.reset();
   dT.reset();
   dFn.reset();
+  dN.reset();
+  dC.reset();
 
   // -- concatenate the chunks' leaves
   leaf_voxels = 0;

@@ -28,9 +28,11 @@ struct DeviceScene {
   DeviceScene& operator=(const DeviceScene&) = delete;
   ~DeviceScene();
 
-  int build_mesh(const float* h_vertices, uint64_t num_vertices, const uint32_t* h_triangles,
-                 uint64_t num_triangles, uint32_t depth, uint32_t treelet_levels,
-                 cudaStream_t stream);
+  // h_normals / h_colors: per-vertex attributes (both or neither), as the
+  // host builder's build_mesh_leaves takes them.
+  int build_mesh(const float* h_vertices, const float* h_normals, const float* h_colors,
+                 uint64_t num_vertices, const uint32_t* h_triangles, uint64_t num_triangles,
+                 uint32_t depth, uint32_t treelet_levels, cudaStream_t stream);
 };
 
 }  // namespace svo

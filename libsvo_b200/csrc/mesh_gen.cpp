@@ -159,4 +159,43 @@ int svo_mesh_terrain(uint32_t grid, uint32_t octaves, float base, float height, 
   return SVO_OK;
 }
 
+// Vertex normals: the normalised sum of the adjacent faces' cross products
+// (area weighted), in double.  Vertex colours: three seeded value-noise
+// fields of the position (frequency 3), mapped from [-1, 1] to [0.15, 0.95].
+int svo_mesh_vertex_attributes(const float* h_vertices, uint64_t num_vertices,
+                               const uint32_t* h_triangles, uint64_t num_triangles, uint64_t seed,
+                               float* h_normals, float* h_colors) {
+  if (!h_vertices || !h_triangles || !h_normals || !h_colors) return SVO_ERR_INVALID;
+  for (uint64_t i = 0; i < 3 * num_triangles; ++i)
+    if (h_triangles[i] >= num_vertices) return SVO_ERR_INVALID;
+  try {
+    std::vector<double> acc(3 * num_vertices, 0.0);
+    for (uint64_t t = 0; t < num_triangles; ++t) {
+      const uint32_t* f = h_triangles + 3 * t;
+      const float* a = h_vertices + 3 * (uint64_t)f[0];
+      const float* b = h_vertices + 3 * (uint64_t)f[1];
+      const float* c = h_vertices + 3 * (uint64_t)f[2];
+      const double e1[3] = {(double)b[0] - a[0], (double)b[1] - a[1], (double)b[2] - a[2]};
+      const double e2[3] = {(double)c[0] - a[0], (double)c[1] - a[1], (double)c[2] - a[2]};
+      const double n[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                           e1[0] * e2[1] - e1[1] * e2[0]};
+      for (int q = 0; q < 3; ++q)
+        for (int k = 0; k < 3; ++k) acc[3 * (uint64_t)f[q] + k] += n[k];
+    }
+    for (uint64_t i = 0; i < num_vertices; ++i) {
+      const double* n = &acc[3 * i];
+      const double l = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+      for (int k = 0; k < 3; ++k) h_normals[3 * i + k] = l > 0.0 ? (float)(n[k] / l) : (k == 2 ? 1.0f : 0.0f);
+      const float* p = h_vertices + 3 * i;
+      for (int k = 0; k < 3; ++k) {
+        const double f = value_noise3(3.0 * p[0], 3.0 * p[1], 3.0 * p[2], seed + 0x51ED27ull * (k + 1));
+        h_colors[3 * i + k] = (float)(0.55 + 0.4 * f);
+      }
+    }
+  } catch (...) {
+    return SVO_ERR_NOMEM;
+  }
+  return SVO_OK;
+}
+
 }  // extern "C"

@@ -84,6 +84,24 @@ void parallel_for(uint64_t n, int threads, Fn&& fn) {
 
 }  // namespace
 
+namespace {
+uint32_t compact3(uint64_t x) {
+  x &= 0x1249249249249249ull;
+  x = (x ^ (x >> 2)) & 0x10c30c30c30c30c3ull;
+  x = (x ^ (x >> 4)) & 0x100f00f00f00f00full;
+  x = (x ^ (x >> 8)) & 0x1f0000ff0000ffull;
+  x = (x ^ (x >> 16)) & 0x1f00000000ffffull;
+  x = (x ^ (x >> 32)) & 0x1fffffull;
+  return (uint32_t)x;
+}
+}  // namespace
+
+void morton3_decode(uint64_t code, uint32_t& x, uint32_t& y, uint32_t& z) {
+  x = compact3(code >> 2);
+  y = compact3(code >> 1);
+  z = compact3(code);
+}
+
 uint64_t morton3(uint32_t x, uint32_t y, uint32_t z, uint32_t depth) {
   (void)depth;
   return (split3(x) << 2) | (split3(y) << 1) | split3(z);
@@ -420,6 +438,56 @@ int cell_floor(float x, uint32_t R) {
   return (int)std::floor(x);
 }
 
+// One triangle's contribution to a leaf (src/attribute_generators/
+// Ag_colorAndNormalsTriangles.cpp:110-135 with BuilderTriangleFace.cpp:211-329):
+// the barycentric (u, v) where the ray from the voxel centre along the
+// triangle's mean vertex normal meets the triangle's plane (Moeller-Trumbore,
+// det within +-1e-8 = parallel: the reference leaves u, v unset there, this
+// takes u = v = 0), clamped to [0, 1]; the normalised interpolated vertex
+// normal and the interpolated vertex colour, w = (1 - u) - v.  FP32, in this
+// order; the GPU builder repeats it operation for operation.
+void leaf_contribution(const float* V, const float* N, const float* C, const uint32_t* tri,
+                       const float c[3], float n_out[3], float c_out[3]) {
+  const float* p0 = V + 3 * (uint64_t)tri[0];
+  const float* p1 = V + 3 * (uint64_t)tri[1];
+  const float* p2 = V + 3 * (uint64_t)tri[2];
+  const float* n0 = N + 3 * (uint64_t)tri[0];
+  const float* n1 = N + 3 * (uint64_t)tri[1];
+  const float* n2 = N + 3 * (uint64_t)tri[2];
+  const float* c0 = C + 3 * (uint64_t)tri[0];
+  const float* c1 = C + 3 * (uint64_t)tri[1];
+  const float* c2 = C + 3 * (uint64_t)tri[2];
+  float d[3];
+  for (int k = 0; k < 3; ++k) d[k] = ((n0[k] + n1[k]) + n2[k]) / 3.0f;
+  float len = std::sqrt((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]);
+  if (len > 0.0f)
+    for (int k = 0; k < 3; ++k) d[k] = d[k] / len;
+  const float e1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+  const float e2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
+  const float pv[3] = {d[1] * e2[2] - d[2] * e2[1], d[2] * e2[0] - d[0] * e2[2],
+                       d[0] * e2[1] - d[1] * e2[0]};
+  const float det = (e1[0] * pv[0] + e1[1] * pv[1]) + e1[2] * pv[2];
+  float u = 0.0f, v = 0.0f;
+  if (!(det > -1e-8f && det < 1e-8f)) {
+    const float inv = 1.0f / det;
+    const float tv[3] = {c[0] - p0[0], c[1] - p0[1], c[2] - p0[2]};
+    u = ((tv[0] * pv[0] + tv[1] * pv[1]) + tv[2] * pv[2]) * inv;
+    const float qv[3] = {tv[1] * e1[2] - tv[2] * e1[1], tv[2] * e1[0] - tv[0] * e1[2],
+                         tv[0] * e1[1] - tv[1] * e1[0]};
+    v = ((d[0] * qv[0] + d[1] * qv[1]) + d[2] * qv[2]) * inv;
+  }
+  u = u < 0.0f ? 0.0f : (u > 1.0f ? 1.0f : u);
+  v = v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v);
+  const float w = (1.0f - u) - v;
+  for (int k = 0; k < 3; ++k) {
+    n_out[k] = (n0[k] * w + n1[k] * u) + n2[k] * v;
+    c_out[k] = (c0[k] * w + c1[k] * u) + c2[k] * v;
+  }
+  len = std::sqrt((n_out[0] * n_out[0] + n_out[1] * n_out[1]) + n_out[2] * n_out[2]);
+  if (len > 0.0f)
+    for (int k = 0; k < 3; ++k) n_out[k] = n_out[k] / len;
+}
+
 struct VoxelTri {
   uint64_t code;
   uint32_t tri;
@@ -428,10 +496,12 @@ struct VoxelTri {
 
 }  // namespace
 
-int build_mesh_leaves(const float* V, uint64_t nv, const uint32_t* T, uint64_t nt, uint32_t depth,
-                      int threads, std::vector<uint64_t>& codes, std::vector<svo_attrib>& attribs) {
+int build_mesh_leaves(const float* V, const float* NV, const float* CV, uint64_t nv,
+                      const uint32_t* T, uint64_t nt, uint32_t depth, int threads,
+                      std::vector<uint64_t>& codes, std::vector<svo_attrib>& attribs) {
   if (depth < 1 || depth > 21) return SVO_ERR_RANGE;
   if (nt == 0 || nv == 0) return SVO_ERR_INVALID;
+  if ((NV == nullptr) != (CV == nullptr)) return SVO_ERR_INVALID;
   for (uint64_t i = 0; i < 3 * nt; ++i)
     if (T[i] >= nv) return SVO_ERR_INVALID;
   threads = resolve_threads(threads);
@@ -530,6 +600,40 @@ int build_mesh_leaves(const float* V, uint64_t nv, const uint32_t* T, uint64_t n
   codes.clear();
   attribs.clear();
   uint64_t i = 0;
+  if (NV) {  // the reference's interpolated attributes, averaged over the triangles
+    const float inv_r = 1.0f / (float)R;
+    while (i < all.size()) {
+      uint64_t j = i;
+      uint32_t x, y, z;
+      morton3_decode(all[i].code, x, y, z);
+      const float c[3] = {-0.5f + ((float)x + 0.5f) * inv_r, -0.5f + ((float)y + 0.5f) * inv_r,
+                          -0.5f + ((float)z + 0.5f) * inv_r};
+      float sn[3] = {0.0f, 0.0f, 0.0f}, sc[3] = {0.0f, 0.0f, 0.0f};
+      while (j < all.size() && all[j].code == all[i].code) {
+        float n[3], col[3];
+        leaf_contribution(V, NV, CV, T + 3 * (uint64_t)all[j].tri, c, n, col);
+        for (int k = 0; k < 3; ++k) {
+          sn[k] += n[k];
+          sc[k] += col[k];
+        }
+        ++j;
+      }
+      const float cnt = (float)(j - i);
+      for (int k = 0; k < 3; ++k) {
+        sn[k] = sn[k] / cnt;
+        sc[k] = sc[k] / cnt;
+      }
+      const float len = std::sqrt((sn[0] * sn[0] + sn[1] * sn[1]) + sn[2] * sn[2]);
+      if (len > 0.0f)
+        for (int k = 0; k < 3; ++k) sn[k] = sn[k] / len;
+      else
+        sn[0] = 0.0f, sn[1] = 0.0f, sn[2] = 1.0f;
+      codes.push_back(all[i].code);
+      attribs.push_back(svo_attrib{pack_normal(sn[0], sn[1], sn[2]), pack_color(sc[0], sc[1], sc[2])});
+      i = j;
+    }
+    return codes.empty() ? SVO_ERR_INVALID : SVO_OK;
+  }
   while (i < all.size()) {
     uint64_t j = i;
     float s[3] = {0.0f, 0.0f, 0.0f};

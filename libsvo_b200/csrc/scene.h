@@ -65,9 +65,17 @@ int cut_treelets(const Octree& tree, uint32_t treelet_levels, uint32_t treelet_b
 int build_menger(uint32_t level, uint32_t depth, uint64_t seed, std::vector<uint64_t>& codes,
                  std::vector<svo_attrib>& attribs);
 
-int build_mesh_leaves(const float* vertices, uint64_t num_vertices, const uint32_t* triangles,
-                      uint64_t num_triangles, uint32_t depth, int threads,
-                      std::vector<uint64_t>& codes, std::vector<svo_attrib>& attribs);
+// Leaves of a triangle mesh.  With per-vertex normals and colours (both
+// non-NULL, num_vertices x 3 floats each) a leaf gets the reference's rule
+// (interpolated_leaf_attribute); without them, the normalised sum of the
+// overlapping face normals and colour = normal * 0.5 + 0.5.
+int build_mesh_leaves(const float* vertices, const float* normals, const float* colors,
+                      uint64_t num_vertices, const uint32_t* triangles, uint64_t num_triangles,
+                      uint32_t depth, int threads, std::vector<uint64_t>& codes,
+                      std::vector<svo_attrib>& attribs);
+
+// Morton code -> lattice coordinates (inverse of morton3).
+void morton3_decode(uint64_t code, uint32_t& x, uint32_t& y, uint32_t& z);
 
 int write_scene(const svo_scene& s, const std::string& base);
 int read_scene(const std::string& base, svo_scene& s);

@@ -9,8 +9,10 @@ configurations name:
                    from a seeded camera outside the cube, 60 degree fov.
 * ``icosphere`` -- icosphere subdivided 6 times (81,920 triangles), radius
                    0.4 displaced radially by 3-octave value noise of amplitude
-                   0.05, depth-11 octree cut into 6-level treelets, colour from
-                   the face normal; one 1920x1080 view from an orbit of radius
+                   0.05, depth-11 octree cut into 6-level treelets, leaf normal
+                   and colour interpolated from seeded per-vertex attributes as
+                   the reference's attribute generator does; one 1920x1080 view
+                   from an orbit of radius
                    2.5.  The configuration names no field of view; 25 degrees
                    (vertical) makes the sphere fill the frame height, so most
                    rays enter the octree.
@@ -35,7 +37,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import (Camera, DeviceScene, Scene, icosphere as icosphere_mesh, orbit_camera, seeded_light,
-               terrain as terrain_mesh)
+               terrain as terrain_mesh, vertex_attributes)
 
 
 @dataclass
@@ -68,7 +70,8 @@ def orbit_pose(radius: float, angle_deg: float, elevation_deg: float, width: int
 def icosphere(subdivisions=6, depth=11, treelet_levels=6, seed=1, width=1920, height=1080,
               fov_deg=25.0, radius=2.5) -> Workload:
     v, t = icosphere_mesh(subdivisions, radius=0.4, octaves=3, amplitude=0.05, frequency=2.0, seed=seed)
-    scene = Scene.from_mesh(v, t, depth, treelet_levels=treelet_levels)
+    n, c = vertex_attributes(v, t, seed)
+    scene = Scene.from_mesh(v, t, depth, treelet_levels=treelet_levels, normals=n, colors=c)
     rng = np.random.default_rng(seed)
     cam = orbit_pose(radius, float(rng.uniform(0, 360)), float(rng.uniform(-30, 30)), width, height,
                      fov_deg)
@@ -81,7 +84,8 @@ def icosphere(subdivisions=6, depth=11, treelet_levels=6, seed=1, width=1920, he
 def terrain(grid=1024, depth=12, treelet_levels=6, seed=1, views=64, min_side=256, max_side=2048,
             fov_deg=60.0) -> Workload:
     v, t = terrain_mesh(grid, octaves=6, base=-0.45, height=0.3, frequency=2.0, seed=seed)
-    scene = Scene.from_mesh(v, t, depth, treelet_levels=treelet_levels)
+    n, c = vertex_attributes(v, t, seed)
+    scene = Scene.from_mesh(v, t, depth, treelet_levels=treelet_levels, normals=n, colors=c)
     rng = np.random.default_rng(seed + 1000)
     cams = []
     for _ in range(views):
@@ -109,7 +113,8 @@ class LargeShadowedWorkload:
 def large_shadowed(subdivisions=9, depth=14, treelet_levels=8, seed=1, width=3840, height=2160,
                    fov_deg=25.0, radius=2.5, stream=None) -> LargeShadowedWorkload:
     v, t = icosphere_mesh(subdivisions, radius=0.4, octaves=4, amplitude=0.05, frequency=2.0, seed=seed)
-    scene = DeviceScene(v, t, depth, treelet_levels=treelet_levels, stream=stream)
+    n, c = vertex_attributes(v, t, seed)
+    scene = DeviceScene(v, t, depth, treelet_levels=treelet_levels, stream=stream, normals=n, colors=c)
     rng = np.random.default_rng(seed)
     cam = orbit_pose(radius, float(rng.uniform(0, 360)), float(rng.uniform(-30, 30)), width, height, fov_deg)
     return LargeShadowedWorkload(
@@ -148,7 +153,8 @@ def serving(octrees=SERVING_OCTREES) -> ServingWorkload:
                                   frequency=2.0, seed=seed)
         else:
             v, t = terrain_mesh(size, octaves=6, base=-0.45, height=0.3, frequency=2.0, seed=seed)
-        scenes.append(Scene.from_mesh(v, t, depth, treelet_levels=levels))
+        n, c = vertex_attributes(v, t, seed)
+        scenes.append(Scene.from_mesh(v, t, depth, treelet_levels=levels, normals=n, colors=c))
     depths = [o[2] for o in octrees]
     return ServingWorkload("serving_8_octrees", scenes, [13] * len(scenes),
                            description=f"{len(scenes)} octrees (icospheres and terrains, depths "

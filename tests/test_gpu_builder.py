@@ -9,8 +9,8 @@ import libsvo_b200 as L
 pytestmark = pytest.mark.gpu
 
 
-def host_pool(v, t, depth, treelet_levels):
-    scene = L.Scene.from_mesh(v, t, depth, treelet_levels=treelet_levels)
+def host_pool(v, t, depth, treelet_levels, attrs=(None, None)):
+    scene = L.Scene.from_mesh(v, t, depth, treelet_levels=treelet_levels, normals=attrs[0], colors=attrs[1])
     info = scene.info
     mm = L.TreeletMemoryManagerCuda(scene, info.treelet_bytes * info.num_treelets)
     mm.insertAll()
@@ -19,9 +19,9 @@ def host_pool(v, t, depth, treelet_levels):
     return info, nodes, attribs
 
 
-def assert_same(v, t, depth, treelet_levels):
-    info, nodes, attribs = host_pool(v, t, depth, treelet_levels)
-    ds = L.DeviceScene(v, t, depth, treelet_levels=treelet_levels)
+def assert_same(v, t, depth, treelet_levels, attrs=(None, None)):
+    info, nodes, attribs = host_pool(v, t, depth, treelet_levels, attrs)
+    ds = L.DeviceScene(v, t, depth, treelet_levels=treelet_levels, normals=attrs[0], colors=attrs[1])
     di = ds.info
     for k in ("num_treelets", "treelet_bytes", "nodes_per_treelet", "max_depth", "total_nodes", "leaf_voxels"):
         assert getattr(di, k) == getattr(info, k), k
@@ -45,6 +45,17 @@ def test_icosphere_pool_matches_host(cuda, depth, levels):
 def test_terrain_pool_matches_host(cuda):
     v, t = L.terrain(64)
     assert_same(v, t, 9, 4)
+
+
+@pytest.mark.parametrize("depth,levels", [(7, 3), (10, 5)])
+def test_interpolated_vertex_attributes_match_host(cuda, depth, levels):
+    """The reference's interpolated leaf attributes (per-vertex normals and
+    colours) come out of both builders bit for bit."""
+    v, t = L.icosphere(4)
+    info = assert_same(v, t, depth, levels, L.vertex_attributes(v, t, 7))
+    assert info.leaf_voxels > 1000
+    v, t = L.terrain(48)
+    assert_same(v, t, depth, levels, L.vertex_attributes(v, t, 8))
 
 
 def test_rendering_the_device_pool(cuda):

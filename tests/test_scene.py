@@ -206,3 +206,59 @@ def test_meshes():
     assert v[:, 1].min() >= -0.45 - 1e-6 and v[:, 1].max() <= -0.15 + 1e-6
     v2, _ = L.terrain(33, octaves=6)
     assert np.array_equal(v, v2)  # seeded, deterministic
+
+
+def _leaf_attribs(scene):
+    mm = L.TreeletMemoryManagerCuda(scene, scene.info.treelet_bytes * scene.info.num_treelets)
+    mm.insertAll()
+    nodes, attribs = mm.getIncoreBuffer()
+    leaf = np.zeros(nodes.shape[0], dtype=bool)
+    # children flagged as leaves in their parent's masks
+    for i in np.nonzero(nodes[:, 1] & 0xFF)[0]:
+        m = int(nodes[i, 1])
+        first = (int(i) + int(nodes[i, 0])) & 0xFFFFFFFF
+        rank = 0
+        for c in range(8):
+            if (m >> (8 + c)) & 1:
+                if (m >> c) & 1:
+                    leaf[first + rank] = True
+                rank += 1
+    return attribs[leaf]
+
+
+def test_interpolated_attributes_of_a_flat_triangle():
+    """One triangle with equal vertex normals and colours: every leaf carries
+    exactly that normal and colour (the interpolation of equal values, whatever
+    u and v are); with different vertex colours, every leaf colour lies within
+    the vertex colours' range."""
+    v = np.array([[-0.4, -0.1, -0.3], [0.4, 0.05, -0.2], [0.0, 0.02, 0.4]], dtype=np.float32)
+    t = np.array([[0, 1, 2]], dtype=np.uint32)
+    n = np.tile(np.array([0.0, 1.0, 0.0], dtype=np.float32), (3, 1))
+    c = np.tile(np.array([0.8, 0.4, 0.2], dtype=np.float32), (3, 1))
+    scene = L.Scene.from_mesh(v, t, 6, normals=n, colors=c)
+    a = _leaf_attribs(scene)
+    assert a.shape[0] > 100
+    col = a[:, 1]
+    assert ((col >> 24) == 204).all() and (((col >> 16) & 255) == 102).all() and (((col >> 8) & 255) == 51).all()
+    nrm = a[:, 0]
+    assert (((nrm >> 16) & 255) == 255).all()  # y = 1 -> 1 * 0.5 + 0.5 -> 255
+    c2 = np.array([[1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 1.0]], dtype=np.float32)
+    a2 = _leaf_attribs(L.Scene.from_mesh(v, t, 6, normals=n, colors=c2))
+    rgb = np.stack([(a2[:, 1] >> 24) & 255, (a2[:, 1] >> 16) & 255, (a2[:, 1] >> 8) & 255], axis=1)
+    # the weights (1 - u - v, u, v) sum to 1; u and v are clamped separately,
+    # so 1 - u - v may go negative and its channel clamps to 0 (sum above 255)
+    assert (rgb.sum(axis=1) >= 253).all()
+    assert rgb.max(axis=0).min() > 128  # every vertex colour dominates somewhere
+
+
+def test_vertex_attribute_arguments():
+    v, t = L.icosphere(1)
+    n, c = L.vertex_attributes(v, t, 1)
+    assert np.allclose(np.linalg.norm(n, axis=1), 1.0, atol=1e-6)
+    assert (c >= 0.15).all() and (c <= 0.95).all()
+    with pytest.raises(ValueError):
+        L.Scene.from_mesh(v, t, 5, normals=n)
+    with pytest.raises(L.SvoError) as e:
+        L.lib.svo_scene_build_mesh_attributed(v.ctypes.data, n.ctypes.data, None, v.shape[0], t.ctypes.data,
+                                             t.shape[0], 5, 0, 0, 0, None) and L._check(-22, "x")
+    assert e.value.code == L.SVO_ERR_INVALID
