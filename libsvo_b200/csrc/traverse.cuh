@@ -122,13 +122,13 @@ struct StagedFetch {
 // kSigned: the reference orders each child's slab distances with a compare
 // and swap (tx0 > tx1).  When the reciprocal r is finite, rounding is
 // monotone, so the swap happens exactly when r < 0 (equal values swap to
-// themselves): the near face is lo when r > 0 and hi when r < 0.  With
-// m = bit + neg - 1 for the near face and bit - neg for the far face
-// (neg = 1 when r < 0), the faces are c + m * sx2 with m in {-1, 0, 1}, which
-// is exact, so the distances are the reference's bits computed on the FMA
-// pipe instead of the compare/select pipe.  Rays with an infinite or NaN
-// reciprocal (a direction component of exactly zero) take kSigned = false,
-// the literal compare and swap.
+// themselves): the near face is lo when r > 0 and hi when r < 0.  A child's
+// two faces along an axis are the parent's mid plane c and its outer face
+// c +- sx2 (exact dyadic numbers, the values the reference's childCenter +-
+// childSizeHalf produce), so each axis costs the distance to the mid plane,
+// the distance to the outer face and two selects that put the near one
+// first.  Rays with an infinite or NaN reciprocal (a direction component of
+// exactly zero) take kSigned = false, the literal compare and swap.
 template <bool kFlat, bool kSigned, class Fetch>
 __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
                                         const float o[3], float dx, float dy, float dz, float rx,
@@ -136,10 +136,8 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
                                         float t_min, float t_max, float tsr, int S, uint2* stack,
                                         int stride, RayHit& h) {
   const float eps = 0.00001f;
-  // per-axis near/far offsets (kSigned): near m = bit + kn, far m = bit + kf
-  const float knx = rx < 0.0f ? 0.0f : -1.0f, kfx = rx < 0.0f ? -1.0f : 0.0f;
-  const float kny = ry < 0.0f ? 0.0f : -1.0f, kfy = ry < 0.0f ? -1.0f : 0.0f;
-  const float knz = rz < 0.0f ? 0.0f : -1.0f, kfz = rz < 0.0f ? -1.0f : 0.0f;
+  // kSigned: the axis runs downwards (r < 0)
+  const bool negx = rx < 0.0f, negy = ry < 0.0f, negz = rz < 0.0f;
   const uint32_t max_loops = (uint32_t)((S + 1) * (S + 1) * 5);
   int scale = S - 1;
   uint32_t node = 0u;
@@ -202,22 +200,30 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
     const float ex = __fsub_rn(__fadd_rn(o[0], __fmul_rn(te, dx)), cx);
     const float ey = __fsub_rn(__fadd_rn(o[1], __fmul_rn(te, dy)), cy);
     const float ez = __fsub_rn(__fadd_rn(o[2], __fmul_rn(te, dz)), cz);
-    const float fbx = ex > 0.0f ? 1.0f : 0.0f;
-    const float fby = ey > 0.0f ? 1.0f : 0.0f;
-    const float fbz = ez > 0.0f ? 1.0f : 0.0f;
+    const bool bxp = ex > 0.0f, byp = ey > 0.0f, bzp = ez > 0.0f;
     float tx0, tx1, ty0, ty1, tz0, tz1;
     if (kSigned) {
-      tx0 = __fadd_rn(__fmul_rn(rx, __fadd_rn(cx, __fmul_rn(__fadd_rn(fbx, knx), sx2))), px);
-      tx1 = __fadd_rn(__fmul_rn(rx, __fadd_rn(cx, __fmul_rn(__fadd_rn(fbx, kfx), sx2))), px);
-      ty0 = __fadd_rn(__fmul_rn(ry, __fadd_rn(cy, __fmul_rn(__fadd_rn(fby, kny), sx2))), py);
-      ty1 = __fadd_rn(__fmul_rn(ry, __fadd_rn(cy, __fmul_rn(__fadd_rn(fby, kfy), sx2))), py);
-      tz0 = __fadd_rn(__fmul_rn(rz, __fadd_rn(cz, __fmul_rn(__fadd_rn(fbz, knz), sx2))), pz);
-      tz1 = __fadd_rn(__fmul_rn(rz, __fadd_rn(cz, __fmul_rn(__fadd_rn(fbz, kfz), sx2))), pz);
+      // The child's faces are the mid plane c and its outer face c +- sx2;
+      // the near one comes first (the mid plane when the child is the far
+      // half along the ray).
+      const float mx = __fadd_rn(__fmul_rn(rx, cx), px);
+      const float my = __fadd_rn(__fmul_rn(ry, cy), py);
+      const float mz = __fadd_rn(__fmul_rn(rz, cz), pz);
+      const float ox = __fadd_rn(__fmul_rn(rx, __fadd_rn(cx, bxp ? sx2 : -sx2)), px);
+      const float oy = __fadd_rn(__fmul_rn(ry, __fadd_rn(cy, byp ? sx2 : -sx2)), py);
+      const float oz = __fadd_rn(__fmul_rn(rz, __fadd_rn(cz, bzp ? sx2 : -sx2)), pz);
+      const bool fx = bxp != negx, fy = byp != negy, fz = bzp != negz;
+      tx0 = fx ? mx : ox;
+      tx1 = fx ? ox : mx;
+      ty0 = fy ? my : oy;
+      ty1 = fy ? oy : my;
+      tz0 = fz ? mz : oz;
+      tz1 = fz ? oz : mz;
     } else {
       // child centre (-0.5 + b) * sx2 + c = c +- half; faces ccx -+ half
-      const float ccx = __fadd_rn(fbx != 0.0f ? half : -half, cx);
-      const float ccy = __fadd_rn(fby != 0.0f ? half : -half, cy);
-      const float ccz = __fadd_rn(fbz != 0.0f ? half : -half, cz);
+      const float ccx = __fadd_rn(bxp ? half : -half, cx);
+      const float ccy = __fadd_rn(byp ? half : -half, cy);
+      const float ccz = __fadd_rn(bzp ? half : -half, cz);
       tx0 = __fadd_rn(__fmul_rn(rx, __fsub_rn(ccx, half)), px);
       tx1 = __fadd_rn(__fmul_rn(rx, __fadd_rn(ccx, half)), px);
       if (tx0 > tx1) {
@@ -252,7 +258,7 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
       return;
     }
     ++fetches;
-    const uint32_t bx = fbx != 0.0f, by = fby != 0.0f, bz = fbz != 0.0f;
+    const uint32_t bx = bxp, by = byp, bz = bzp;
     const uint32_t ci = (bx << 2) | (by << 1) | bz;
     const uint32_t masks = nd.y;
     const uint32_t sh = masks >> ci;  // bit 8: valid, bit 0: leaf
@@ -272,9 +278,9 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
         h.tc_min = tc_min;
         h.sx2 = sx2;
         h.leaf = leaf ? 1u : 0u;
-        h.cx = __fadd_rn(fbx != 0.0f ? half : -half, cx);
-        h.cy = __fadd_rn(fby != 0.0f ? half : -half, cy);
-        h.cz = __fadd_rn(fbz != 0.0f ? half : -half, cz);
+        h.cx = __fadd_rn(bxp ? half : -half, cx);
+        h.cy = __fadd_rn(byp ? half : -half, cy);
+        h.cz = __fadd_rn(bzp ? half : -half, cz);
         return;
       }
       if (kFlat && scale == 0) {  // non-leaf below the octree's depth: corrupt pool
