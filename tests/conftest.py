@@ -12,9 +12,9 @@ if str(ROOT) not in sys.path:
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
     # build the native library and the oracle once per session (no GPU needed)
-    from libsvo_b200 import _build
+    import __graft_entry__
 
-    _build.build()
+    __graft_entry__._load_build_module().build()
     import oracle
 
     oracle.build()
