@@ -416,6 +416,56 @@ def incore_update_leg(dev, scene, incore_mb=256, frames=20, seed=5):
     return out
 
 
+def streaming_leg(dev, scene, **kw):
+    """streaming_run with the reference's upload policy and with the
+    page-locked mirror and gather kernel."""
+    import libsvo_b200 as L
+
+    return {"coalesced_0.6": streaming_run(dev, scene, L.UPLOAD_COALESCED, **kw),
+            "pinned_mirror_gather": streaming_run(dev, scene, L.UPLOAD_PINNED, **kw),
+            "reference_thesis": "mostly above 50 Hz, GTX 580 (ergebnisse_diskussionen.tex:158)"}
+
+
+def streaming_run(dev, scene, policy, frames=150, incore_mb=256, size=1024):
+    """The loop the reference measured itself (its thesis: "out-of-core cycle
+    + ray cast run sequentially, 1024x1024", mostly above 50 Hz on a GTX 580):
+    per frame the analysis pass at 1/8 resolution (feedback kernel, records to
+    the host, analysis, insertion with eviction, upload of the new treelets),
+    then the 1024x1024 frame.  The incore buffer holds 256 MB (the thesis'
+    size; 87 % of the icosphere's treelets), only the root treelet is
+    resident at the start, and the camera orbits 3 degrees per frame while
+    moving in from radius 2.5 to 1.2, so treelets keep paging in and out."""
+    import torch
+
+    import libsvo_b200 as L
+    from libsvo_b200 import scenes as S
+
+    mm = L.TreeletMemoryManagerCuda(scene, incore_mb << 20)
+    mm.setUploadPolicy(policy)
+    mm.initDeviceBuffer()
+    out = torch.empty((size, size), dtype=torch.int32, device=dev)
+    s = torch.cuda.current_stream()
+    ms, new_total = [], 0
+    for f in range(frames):
+        r = 2.5 - 1.3 * f / max(1, frames - 1)
+        p = S.orbit_pose(r, 3.0 * f, 20.0, size, size, 25.0).frame_params()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        new, _ = mm.performAnalysePass(p, divisor=8, stream=s)
+        mm.render(p, out, stream=s)
+        s.synchronize()
+        ms.append((time.perf_counter() - t0) * 1e3)
+        new_total += new
+    info = mm.info
+    mm.close()
+    steady = ms[10:]
+    return {"scene": "icosphere_s6_d11 (3175 treelets of 98,848 B)", "incore_mb": incore_mb,
+            "frame": f"{size}x{size}", "frames": frames, "analysis_divisor": 8,
+            "hz_mean": 1e3 / statistics.mean(steady), "ms_p50": statistics.median(steady),
+            "ms_p99": float(np.percentile(steady, 99)), "ms_first_frame": ms[0],
+            "treelets_inserted": new_total, "resident_slots_at_end": info.num_slots - info.free_slots}
+
+
 def large_shadow_leg(dev, reps=10, cap_gb=60.0):
     """the depth-14 icosphere built on the GPU, one
     3840x2160 frame of primary rays plus one shadow ray per hit.  The metric
@@ -653,10 +703,11 @@ def main():
                                                         light=L.seeded_light(1) if shadow else None)
         mm.close()
         if world == 1 and not args.no_extra and args.workload == "icosphere":
-            try:
-                line["incore_update"] = incore_update_leg(dev, wl.scene)
-            except Exception as e:  # a failing extra leg must not lose the primary line
-                line["incore_update"] = {"error": f"{type(e).__name__}: {e}"}
+            for key, leg in (("incore_update", incore_update_leg), ("streaming", streaming_leg)):
+                try:
+                    line[key] = leg(dev, wl.scene)
+                except Exception as e:  # a failing extra leg must not lose the primary line
+                    line[key] = {"error": f"{type(e).__name__}: {e}"}
         if world == 1 and not args.no_extra:
             for key, leg in (("batched", batched_leg), ("served", served_leg),
                              ("large_shadowed", large_shadow_leg)):

@@ -428,7 +428,10 @@ int svo_mm_analyse_feedback(svo_mm* mm, const svo_feedback* h_feedback, uint64_t
  * origin offset by (jitter_x, jitter_y) * divisor / 2 frame pixels (the
  * reference's "rumble", RenderPassAnalyse.cpp:176-184; jitter in [-1, 1]),
  * records read back, analysed, treelets inserted (evicting by visibility)
- * and uploaded.  Blocks until the records are on the host. */
+ * and uploaded.  Blocks until the records are on the host.  *num_new: the
+ * treelets placed; like the reference's updateClientSideIncoreBuffer, the
+ * step skips new treelets that find no slot under memory pressure (the next
+ * step asks for them again).  *num_old: visible resident treelets. */
 int svo_mm_analysis_step(svo_mm* mm, const svo_frame_params* frame, uint32_t divisor,
                          float jitter_x, float jitter_y, int32_t stack_size, void* stream,
                          uint32_t* num_new, uint32_t* num_old);

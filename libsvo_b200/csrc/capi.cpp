@@ -635,8 +635,10 @@ int svo_mm_analysis_step(svo_mm* mm, const svo_frame_params* frame, uint32_t div
     std::vector<float> ne(nw.size());
     for (size_t i = 0; i < nw.size(); ++i) ng[i] = nw[i].first, ne[i] = nw[i].second;
     for (size_t i = 0; i < old.size(); ++i) og[i] = old[i].first;
+    uint32_t placed = 0;
     rc = mm->impl.update_client_side(ng.data(), ne.data(), (uint32_t)ng.size(), og.data(),
-                                     (uint32_t)og.size());
+                                     (uint32_t)og.size(), true, &placed);
+    if (num_new) *num_new = placed;
     const int up = mm->impl.update_device_memory(nullptr);
     return rc != SVO_OK ? rc : up;
   });

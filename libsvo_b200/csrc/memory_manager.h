@@ -41,8 +41,12 @@ class TreeletMemoryManager {
   int insert_treelet(const SlotInfo& tve);           // .cpp:456-548
   int remove_treelet(int32_t gid);                   // .cpp:666-700
   int free_incore_position();                        // .cpp:561-653
+  // updateClientSideIncoreBuffer.  skip_unplaceable: treelets that find no
+  // slot, or whose parent is not resident, are skipped instead of reported
+  // (as the reference does); *inserted counts the treelets placed.
   int update_client_side(const int32_t* new_gids, const float* new_errors, uint32_t num_new,
-                         const int32_t* old_gids, uint32_t num_old);  // .cpp:393-443
+                         const int32_t* old_gids, uint32_t num_old, bool skip_unplaceable = false,
+                         uint32_t* inserted = nullptr);  // .cpp:393-443
   virtual int reset_incore_buffer();                 // .cpp:304-380
   int insert_all(uint32_t* inserted);
 

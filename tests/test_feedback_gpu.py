@@ -82,3 +82,29 @@ def test_paging_by_analysis_converges_to_full_residency(cuda, scene_kind):
         total += new
     assert total > 0
     mm.close()
+
+
+def test_analysis_steps_under_memory_pressure(cuda):
+    """A pool far smaller than the visible treelets: every step evicts to make
+    room, some treelets find no slot or lose their parent to an eviction of
+    the same step and are skipped (the reference ignores those insertion
+    failures too), and every frame still matches the oracle on the manager's
+    host mirror."""
+    scene = L.Scene.menger(level=4, depth=7, seed=5, treelet_levels=2)
+    info = scene.info
+    mm = L.TreeletMemoryManagerCuda(scene, info.treelet_bytes * 40)
+    mm.initDeviceBuffer()
+    total = 0
+    for f in range(20):
+        p = L.orbit_camera(100 + f, 96, 80, radius=(1.1, 1.8)).frame_params(t_scale_ratio=0.0)
+        new, _ = mm.performAnalysePass(p, divisor=2)
+        total += new
+        rgba, hits = render(mm, p, cuda)
+        nodes, attribs = mm.getIncoreBuffer()
+        o_rgba, o_hits, _, _ = oracle.render(nodes, attribs, bytes(p))
+        assert np.array_equal(rgba.view(np.uint32), o_rgba), f"frame {f}"
+        assert np.array_equal(hits["node"], o_hits.reshape(-1)["node"])
+        assert mm.info.free_slots <= 40
+    # the pool ran full: the later steps placed treelets only by eviction
+    assert mm.info.free_slots == 0 and total >= 39
+    mm.close()
