@@ -48,6 +48,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the batched, served, large-shadowed and incore-update measurements")
+    ap.add_argument("--large-only", action="store_true",
+                    help="run only the large shadowed measurement (icosphere built on the GPU, 3840x2160 "
+                         "primary + shadow frame) and print its result")
+    ap.add_argument("--large-subdivisions", type=int, default=9)
+    ap.add_argument("--large-depth", type=int, default=14)
     ap.add_argument("--shadow", action="store_true",
                     help="cast one shadow ray per hit as well (svo_mm_render_shadow, seeded light); "
                          "the metric then counts primary and shadow rays")
@@ -251,6 +256,13 @@ def job_mrays_per_s(world: int, rays_per_rank: int, ms_per_step: float) -> float
     return world * rays_per_rank / (ms_per_step * 1e-3) / 1e6
 
 
+def _profiled_traffic(workload: str):
+    """DRAM bytes per launch of the workload's frame kernel from the
+    committed ncu summaries (profiles/), or None."""
+    tp = ROOT / "profiles" / "render_frame_kernel_dram_traffic.json"
+    return json.loads(tp.read_text()).get(workload) if tp.is_file() else None
+
+
 def _event_ms(torch, fn, reps):
     fn()
     torch.cuda.synchronize()
@@ -264,7 +276,7 @@ def _event_ms(torch, fn, reps):
 
 
 def batched_leg(dev, reps=10):
-    """64 terrain views of uneven size: the same views as
+    """64 terrain views of uneven size (depth-12 terrain, 256^2..2048^2): the same views as
     64 per-frame launches on one stream, and as one autotuned, graph-replayed
     persistent launch."""
     import torch
@@ -304,7 +316,7 @@ def batched_leg(dev, reps=10):
 
 
 def served_leg(dev, n=400, rates=(4000, 16000, 64000)):
-    """8 octrees served to a Poisson stream of requests
+    """8 octrees of depths 9..13 served to a Poisson stream of requests
     from 64x64 to 1920x1080: batched server vs the plain per-frame kernel in the
     same request loop, all octrees resident; then the batched server with a
     budget of half the octrees' footprint, so octrees page in and out."""
@@ -466,8 +478,8 @@ def streaming_run(dev, scene, policy, frames=150, incore_mb=256, size=1024):
             "treelets_inserted": new_total, "resident_slots_at_end": info.num_slots - info.free_slots}
 
 
-def large_shadow_leg(dev, reps=10, cap_gb=60.0):
-    """the depth-14 icosphere built on the GPU, one
+def large_shadow_leg(dev, reps=10, cap_gb=60.0, subdivisions=9, depth=14):
+    """The large shadowed workload: the depth-14 icosphere built on the GPU, one
     3840x2160 frame of primary rays plus one shadow ray per hit.  The metric
     counts both kinds of ray."""
     import torch
@@ -476,7 +488,7 @@ def large_shadow_leg(dev, reps=10, cap_gb=60.0):
     from libsvo_b200 import scenes
 
     t0 = time.perf_counter()
-    wl = scenes.large_shadowed()
+    wl = scenes.large_shadowed(subdivisions=subdivisions, depth=depth)
     torch.cuda.synchronize()
     build_s = time.perf_counter() - t0
     info = wl.scene.info
@@ -525,7 +537,8 @@ def large_shadow_leg(dev, reps=10, cap_gb=60.0):
            "ms_per_frame": ms, "mrays_s": rays / ms / 1e3, "primary_mrays_s": px / ms / 1e3,
            "capped_rays": int(stats[0].item()), "bounds_errors": int(stats[1].item()),
            "roofline": {"algorithmic_bytes_per_frame": algo_bytes, "achieved_gbs": algo_bytes / ms / 1e6,
-                        "frac": algo_bytes / ms / 1e6 / peak, "node_reads_per_ray": fetches / rays}}
+                        "frac": algo_bytes / ms / 1e6 / peak, "node_reads_per_ray": fetches / rays,
+                        "traffic": _profiled_traffic(wl.name)}}
     wl.scene.close()
     return out
 
@@ -549,6 +562,10 @@ def main():
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
+    if args.large_only:
+        print(json.dumps(large_shadow_leg(dev, reps=args.steps, subdivisions=args.large_subdivisions,
+                                          depth=args.large_depth)), flush=True)
+        return
     if world > 1:
         from datetime import timedelta
 
@@ -661,10 +678,7 @@ def main():
     if rank == 0:
         peak, peak_kind = load_peaks()
         achieved = algo_bytes / (ms * 1e-3) / 1e9
-        traffic = None
-        tp = ROOT / "profiles" / "render_frame_kernel_dram_traffic.json"
-        if tp.is_file():
-            traffic = json.loads(tp.read_text()).get(wl.name + ("_shadow" if shadow else ""))
+        traffic = _profiled_traffic(wl.name + ("_shadow" if shadow else ""))
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
