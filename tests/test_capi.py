@@ -64,6 +64,22 @@ def test_null_arguments_are_status_codes():
                                  None) == L.SVO_ERR_INVALID
     assert lib.svo_mm_render_shadow(None, ctypes.byref(p), ctypes.byref(cfg), ctypes.byref(sc), 1, None, None,
                                     None) == L.SVO_ERR_INVALID
+    assert lib.svo_mm_render_host_async(None, ctypes.byref(p), ctypes.byref(cfg), 1, None) == L.SVO_ERR_INVALID
+    out = ctypes.c_void_p()
+    assert lib.svo_device_scene_build_mesh(None, 3, None, 1, 5, 0, None, ctypes.byref(out)) == L.SVO_ERR_INVALID
+    v = (ctypes.c_float * 9)()
+    t = (ctypes.c_uint32 * 3)(0, 1, 2)
+    assert lib.svo_device_scene_build_mesh_attributed(v, v, None, 3, t, 1, 5, 0, None,
+                                                      ctypes.byref(out)) == L.SVO_ERR_INVALID
+    assert lib.svo_device_scene_info_get(None, None) == L.SVO_ERR_INVALID
+    assert lib.svo_device_scene_buffers(None, None, None, None) == L.SVO_ERR_INVALID
+    assert lib.svo_device_scene_copy(None, 0, 0, None, None) == L.SVO_ERR_INVALID
+    assert lib.svo_mm_set_upload_policy(None, 0) == L.SVO_ERR_INVALID
+    assert lib.svo_mm_set_upload_ratio(None, 0.6) == L.SVO_ERR_INVALID
+    assert lib.svo_mesh_vertex_attributes(v, 3, t, 1, 1, None, None) == L.SVO_ERR_INVALID
+    t_bad = (ctypes.c_uint32 * 3)(0, 1, 3)
+    nrm, col = (ctypes.c_float * 9)(), (ctypes.c_float * 9)()
+    assert lib.svo_mesh_vertex_attributes(v, 3, t_bad, 1, 1, nrm, col) == L.SVO_ERR_INVALID
 
 
 def test_manager_without_device_buffer_rejects_renders(menger_scene):
