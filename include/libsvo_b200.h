@@ -201,6 +201,31 @@ int svo_mesh_vertex_attributes(const float* h_vertices, uint64_t num_vertices,
                                const uint32_t* h_triangles, uint64_t num_triangles, uint64_t seed,
                                float* h_normals, float* h_colors);
 
+/* PLY meshes, the input of the reference's octree builder
+ * (projects/octree_builder/src/octree_builder.cpp:85-157: "*.ply files with
+ * per vertex color and normals").  ascii and binary_little_endian; vertex
+ * x, y, z and, when present, nx, ny, nz and red, green, blue (integer
+ * colours / 255); faces as vertex index lists, polygons split into fans.
+ * SVO_ERR_NOTSUP for big-endian files. */
+#define SVO_MESH_HAS_NORMALS 1u
+#define SVO_MESH_HAS_COLORS 2u
+typedef struct svo_mesh svo_mesh;
+int svo_mesh_load_ply(const char* path, svo_mesh** out);
+int svo_mesh_info(const svo_mesh* mesh, uint64_t* num_vertices, uint64_t* num_triangles,
+                  uint32_t* flags);
+/* Copies num_vertices x 3 floats (positions, normals, colours) and
+ * num_triangles x 3 indices; any output may be NULL, a missing attribute
+ * requested is SVO_ERR_INVALID. */
+int svo_mesh_copy(const svo_mesh* mesh, float* h_vertices, float* h_normals, float* h_colors,
+                  uint32_t* h_triangles);
+void svo_mesh_destroy(svo_mesh* mesh);
+/* The octree builder's placement (octree_builder.cpp:130-157): rotation by
+ * rotate_x_deg about x, the bounding box centred at the origin and its
+ * largest side scaled to 1, normals (optional) rotated and normalised; in
+ * place. */
+int svo_mesh_fit_unit_cube(float* h_vertices, float* h_normals, uint64_t num_vertices,
+                           float rotate_x_deg);
+
 /* Seeded synthetic meshes (inputs for svo_scene_build_mesh).  The reference
  * voxelises scanned PLY meshes that are not part of it; these stand in with
  * the triangle counts of the benchmark configurations.  Call *_size first.

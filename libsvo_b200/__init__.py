@@ -195,6 +195,11 @@ _SIGS = {
     "svo_scene_build_mesh_attributed": ([_vp, _vp, _vp, _u64, _vp, _u64, _u32, _u32, _u32, _i32, _P(_vp)],
                                         ctypes.c_int),
     "svo_mesh_vertex_attributes": ([_vp, _u64, _vp, _u64, _u64, _vp, _vp], ctypes.c_int),
+    "svo_mesh_load_ply": ([ctypes.c_char_p, _P(_vp)], ctypes.c_int),
+    "svo_mesh_info": ([_vp, _P(_u64), _P(_u64), _P(_u32)], ctypes.c_int),
+    "svo_mesh_copy": ([_vp, _vp, _vp, _vp, _vp], ctypes.c_int),
+    "svo_mesh_destroy": ([_vp], None),
+    "svo_mesh_fit_unit_cube": ([_vp, _vp, _u64, _f32], ctypes.c_int),
     "svo_device_scene_info_get": ([_vp, _P(svo_scene_info)], ctypes.c_int),
     "svo_device_scene_buffers": ([_vp, _P(_vp), _P(_vp), _P(_u64)], ctypes.c_int),
     "svo_device_scene_copy": ([_vp, _u64, _u64, _vp, _vp], ctypes.c_int),
@@ -343,6 +348,35 @@ def vertex_attributes(vertices: np.ndarray, triangles: np.ndarray, seed=1):
     _check(_L.svo_mesh_vertex_attributes(_np_ptr(v), v.shape[0], _np_ptr(t), t.shape[0], seed, _np_ptr(n),
                                          _np_ptr(c)), "svo_mesh_vertex_attributes")
     return n, c
+
+
+def read_ply(path) -> dict:
+    """A PLY mesh (the reference octree builder's input): {"vertices",
+    "triangles", "normals" or None, "colors" or None}, float32 / uint32."""
+    h = ctypes.c_void_p()
+    _check(_L.svo_mesh_load_ply(str(path).encode(), ctypes.byref(h)), "svo_mesh_load_ply")
+    try:
+        nv, nt, fl = _u64(), _u64(), _u32()
+        _check(_L.svo_mesh_info(h, ctypes.byref(nv), ctypes.byref(nt), ctypes.byref(fl)), "svo_mesh_info")
+        v = np.zeros((nv.value, 3), dtype=np.float32)
+        t = np.zeros((nt.value, 3), dtype=np.uint32)
+        n = np.zeros_like(v) if fl.value & 1 else None
+        c = np.zeros_like(v) if fl.value & 2 else None
+        _check(_L.svo_mesh_copy(h, _np_ptr(v), None if n is None else _np_ptr(n), None if c is None else _np_ptr(c),
+                                _np_ptr(t)), "svo_mesh_copy")
+    finally:
+        _L.svo_mesh_destroy(h)
+    return {"vertices": v, "triangles": t, "normals": n, "colors": c}
+
+
+def fit_unit_cube(vertices: np.ndarray, normals: np.ndarray | None = None, rotate_x_deg=0.0):
+    """The reference octree builder's placement, in place on float32 copies:
+    returns (vertices, normals)."""
+    v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3).copy()
+    n = None if normals is None else np.ascontiguousarray(normals, dtype=np.float32).reshape(-1, 3).copy()
+    _check(_L.svo_mesh_fit_unit_cube(_np_ptr(v), None if n is None else _np_ptr(n), v.shape[0], rotate_x_deg),
+           "svo_mesh_fit_unit_cube")
+    return v, n
 
 
 def _vertex_arrays(normals, colors, nv):
