@@ -126,7 +126,7 @@ struct StagedFetch {
 // two faces along an axis are the parent's mid plane c and its outer face
 // c +- sx2 (exact dyadic numbers, the values the reference's childCenter +-
 // childSizeHalf produce), so each axis costs the distance to the mid plane,
-// the distance to the outer face and two selects that put the near one
+// the distance to the outer face and a min and a max that put the near one
 // first.  Rays with an infinite or NaN reciprocal (a direction component of
 // exactly zero) take kSigned = false, the literal compare and swap.
 template <bool kFlat, bool kSigned, class Fetch>
@@ -136,8 +136,6 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
                                         float t_min, float t_max, float tsr, int S, uint2* stack,
                                         int stride, RayHit& h) {
   const float eps = 0.00001f;
-  // kSigned: the axis runs downwards (r < 0)
-  const bool negx = rx < 0.0f, negy = ry < 0.0f, negz = rz < 0.0f;
   const uint32_t max_loops = (uint32_t)((S + 1) * (S + 1) * 5);
   int scale = S - 1;
   uint32_t node = 0u;
@@ -196,11 +194,13 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
       }
       continue;
     }
+    // childEntryPoint = (o + (tMin + eps) d) - centre and its sign test: in
+    // IEEE arithmetic with subnormals, a - b > 0 exactly when a > b (a - b
+    // rounds to 0 only when a == b), so the subtraction is left out
     const float te = __fadd_rn(tmin, eps);
-    const float ex = __fsub_rn(__fadd_rn(o[0], __fmul_rn(te, dx)), cx);
-    const float ey = __fsub_rn(__fadd_rn(o[1], __fmul_rn(te, dy)), cy);
-    const float ez = __fsub_rn(__fadd_rn(o[2], __fmul_rn(te, dz)), cz);
-    const bool bxp = ex > 0.0f, byp = ey > 0.0f, bzp = ez > 0.0f;
+    const bool bxp = __fadd_rn(o[0], __fmul_rn(te, dx)) > cx;
+    const bool byp = __fadd_rn(o[1], __fmul_rn(te, dy)) > cy;
+    const bool bzp = __fadd_rn(o[2], __fmul_rn(te, dz)) > cz;
     float tx0, tx1, ty0, ty1, tz0, tz1;
     if (kSigned) {
       // The child's faces are the mid plane c and its outer face c +- sx2;
@@ -212,13 +212,14 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
       const float ox = __fadd_rn(__fmul_rn(rx, __fadd_rn(cx, bxp ? sx2 : -sx2)), px);
       const float oy = __fadd_rn(__fmul_rn(ry, __fadd_rn(cy, byp ? sx2 : -sx2)), py);
       const float oz = __fadd_rn(__fmul_rn(rz, __fadd_rn(cz, bzp ? sx2 : -sx2)), pz);
-      const bool fx = bxp != negx, fy = byp != negy, fz = bzp != negz;
-      tx0 = fx ? mx : ox;
-      tx1 = fx ? ox : mx;
-      ty0 = fy ? my : oy;
-      ty1 = fy ? oy : my;
-      tz0 = fz ? mz : oz;
-      tz1 = fz ? oz : mz;
+      // the near face is the nearer one: no NaN and no -0 here, so the
+      // hardware min/max give the reference's order bit for bit
+      tx0 = fminf(mx, ox);
+      tx1 = fmaxf(mx, ox);
+      ty0 = fminf(my, oy);
+      ty1 = fmaxf(my, oy);
+      tz0 = fminf(mz, oz);
+      tz1 = fmaxf(mz, oz);
     } else {
       // child centre (-0.5 + b) * sx2 + c = c +- half; faces ccx -+ half
       const float ccx = __fadd_rn(bxp ? half : -half, cx);
