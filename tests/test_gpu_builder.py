@@ -97,9 +97,8 @@ def test_bad_inputs_are_status_codes(cuda):
 
 def test_benchmark_icosphere_pool_matches_host(cuda):
     """The 1080p benchmark's octree (81,920 triangles, depth 11, 6-level
-    treelets, seeded vertex attributes): 3,175 treelets, record for record."""
-    from libsvo_b200 import scenes  # noqa: F401  (the same generator parameters)
-
+    treelets, seeded vertex attributes; the parameters of
+    libsvo_b200.scenes.icosphere): 3,175 treelets, record for record."""
     v, t = L.icosphere(6, radius=0.4, octaves=3, amplitude=0.05, frequency=2.0, seed=1)
     info = assert_same(v, t, 11, 6, L.vertex_attributes(v, t, 1))
     assert info.num_treelets > 3000
