@@ -68,8 +68,8 @@ typedef struct svo_frame_params {
   int32_t mode;             /* otherParams.x: 0 colour, 1 normal,
                                2 loops as wavelength colour, 3 octree
                                depth, 4 pixel depth, 5 loops, 6 Phong,
-                               7 LOD quality (2, 6, 7: svo_render and
-                               svo_mm_render only; 6, 7: treelet only)   */
+                               7 LOD quality (6, 7: treelet traversal
+                               only)                                     */
   float pixel_far_h[4];     /* pixelFarVectorH                           */
   float pixel_far_v[4];     /* pixelFarVectorV                           */
   float far_lower_left[4];  /* far_lower_left                            */

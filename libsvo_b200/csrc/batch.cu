@@ -29,7 +29,7 @@ namespace {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
-template <int TW>
+template <bool kExt>
 __device__ __forceinline__ void trace_tile_pixel(const BatchView& v, const BatchOctree& oct,
                                                  uint32_t x, uint32_t y, const uint2* top,
                                                  uint32_t top_count, uint2* stack, int stride,
@@ -47,12 +47,18 @@ __device__ __forceinline__ void trace_tile_pixel(const BatchView& v, const Batch
     h = cast_ray<false>(GlobalFetch{oct.nodes}, oct.num_nodes, o, dx, dy, dz,
                         v.params.t_scale_ratio, oct.stack_size, stack, stride);
   const uint64_t pix = (uint64_t)y * v.params.width + x;
-  v.rgba[pix] = shade(v.params.mode, h, oct.attribs, oct.num_nodes, oct.stack_size);
+  const int m = v.params.mode;
+  v.rgba[pix] = (kExt && (m == 2 || m == 6 || m == 7))
+                    ? shade_ext(m, h, oct.attribs, oct.num_nodes, oct.stack_size,
+                                v.params.t_scale_ratio, dx, dy, dz)
+                    : shade(m, h, oct.attribs, oct.num_nodes, oct.stack_size);
   if (v.hits != nullptr) store_hit(v.hits, pix, h);
   count_stats(stats, h);
 }
 
-template <int TW, int TH>
+// kExt: some view uses view mode 2, 6 or 7 (shade_ext); batches without
+// them run the instantiation that carries no extra exit state.
+template <int TW, int TH, bool kExt>
 __global__ void batch_kernel(const BatchView* __restrict__ views, uint32_t num_views,
                              const BatchOctree* __restrict__ octrees, uint64_t total_tiles,
                              unsigned long long* __restrict__ counter, svo_stats* stats, int max_s,
@@ -90,7 +96,7 @@ __global__ void batch_kernel(const BatchView* __restrict__ views, uint32_t num_v
     const uint32_t x = tx * TW + lane % TW, y = ty * TH + lane / TW;
     if (x < v.params.width && y < v.params.height) {
       const BatchOctree& oct = octrees[v.octree];
-      trace_tile_pixel<TW>(v, oct, x, y, top, v.octree == 0 ? top_count : 0u, stack, stride, stats);
+      trace_tile_pixel<kExt>(v, oct, x, y, top, v.octree == 0 ? top_count : 0u, stack, stride, stats);
     }
     __syncwarp();
   }
@@ -99,24 +105,37 @@ __global__ void batch_kernel(const BatchView* __restrict__ views, uint32_t num_v
 typedef void (*BatchKernelFn)(const BatchView*, uint32_t, const BatchOctree*, uint64_t,
                               unsigned long long*, svo_stats*, int, uint32_t);
 
-BatchKernelFn kernel_for(uint32_t tw, uint32_t th) {
-  if (tw == 8 && th == 4) return batch_kernel<8, 4>;
-  if (tw == 16 && th == 2) return batch_kernel<16, 2>;
-  if (tw == 4 && th == 8) return batch_kernel<4, 8>;
-  if (tw == 32 && th == 1) return batch_kernel<32, 1>;
+template <bool kExt>
+BatchKernelFn kernel_for_t(uint32_t tw, uint32_t th) {
+  if (tw == 8 && th == 4) return batch_kernel<8, 4, kExt>;
+  if (tw == 16 && th == 2) return batch_kernel<16, 2, kExt>;
+  if (tw == 4 && th == 8) return batch_kernel<4, 8, kExt>;
+  if (tw == 32 && th == 1) return batch_kernel<32, 1, kExt>;
   return nullptr;
+}
+
+BatchKernelFn kernel_for(uint32_t tw, uint32_t th, bool ext) {
+  return ext ? kernel_for_t<true>(tw, th) : kernel_for_t<false>(tw, th);
 }
 
 }  // namespace
 
-bool batch_tile_supported(uint32_t tw, uint32_t th) { return kernel_for(tw, th) != nullptr; }
+bool batch_tile_supported(uint32_t tw, uint32_t th) { return kernel_for(tw, th, false) != nullptr; }
+
+bool batch_needs_ext(const BatchView* views, uint32_t num_views) {
+  for (uint32_t i = 0; i < num_views; ++i) {
+    const int32_t m = views[i].params.mode;
+    if (m == 2 || m == 6 || m == 7) return true;
+  }
+  return false;
+}
 
 size_t batch_smem_bytes(int max_s, uint32_t threads, uint32_t top_nodes) {
   return ((size_t)max_s * threads + top_nodes) * sizeof(uint2);
 }
 
 int launch_batch(const BatchLaunch& L, cudaStream_t stream) {
-  BatchKernelFn fn = kernel_for(L.tile_w, L.tile_h);
+  BatchKernelFn fn = kernel_for(L.tile_w, L.tile_h, L.ext);
   if (!fn) return SVO_ERR_NOTSUP;
   const size_t smem = batch_smem_bytes(L.max_s, L.threads, L.top_nodes);
   if (smem > 48u * 1024u) {
@@ -128,8 +147,8 @@ int launch_batch(const BatchLaunch& L, cudaStream_t stream) {
 }
 
 int batch_grid(uint32_t tile_w, uint32_t tile_h, int max_s, uint32_t threads, uint32_t top_nodes,
-               uint32_t blocks_per_sm, uint32_t* blocks) {
-  BatchKernelFn fn = kernel_for(tile_w, tile_h);
+               uint32_t blocks_per_sm, uint32_t* blocks, bool ext) {
+  BatchKernelFn fn = kernel_for(tile_w, tile_h, ext);
   if (!fn) return SVO_ERR_NOTSUP;
   const size_t smem = batch_smem_bytes(max_s, threads, top_nodes);
   if (smem > 48u * 1024u) {

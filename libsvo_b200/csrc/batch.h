@@ -41,20 +41,28 @@ struct BatchLaunch {
   uint32_t top_nodes = 0;
   uint32_t tile_w = 8, tile_h = 4;
   uint32_t threads = 256, blocks = 0;
+  bool ext = false;  // some view uses view mode 2, 6 or 7
 };
 
 bool batch_tile_supported(uint32_t tile_w, uint32_t tile_h);
 size_t batch_smem_bytes(int max_s, uint32_t threads, uint32_t top_nodes);
 // Persistent grid size: blocks_per_sm (0 = as many as fit) times the SM count.
 int batch_grid(uint32_t tile_w, uint32_t tile_h, int max_s, uint32_t threads, uint32_t top_nodes,
-               uint32_t blocks_per_sm, uint32_t* blocks);
+               uint32_t blocks_per_sm, uint32_t* blocks, bool ext = false);
+// Whether a view of the table uses view mode 2, 6 or 7.
+bool batch_needs_ext(const BatchView* views, uint32_t num_views);
 // Launches the kernel; the caller has zeroed *counter on the same stream.
 int launch_batch(const BatchLaunch& launch, cudaStream_t stream);
 
 // Fills `out` (num_views entries) from the caller's view descriptors for
 // tiles of tile_w x tile_h pixels; returns the total tile count, or 0 if a
-// descriptor is invalid.
+// descriptor is invalid (view modes 0-7 are valid; whether the octree suits
+// the mode is check_batch_modes's).
 uint64_t layout_views(const svo_view_desc* views, uint32_t num_views, uint32_t num_octrees,
                       uint32_t tile_w, uint32_t tile_h, BatchView* out);
+// Per view: attributes present for modes 0, 1 and 6, the treelet traversal
+// for modes 6 and 7 (their node centre and quality).
+int check_batch_modes(const svo_view_desc* views, uint32_t num_views,
+                      const svo_octree_desc* octrees);
 
 }  // namespace svo

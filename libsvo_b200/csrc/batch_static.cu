@@ -89,10 +89,8 @@ extern "C" int svo_render_batch_static(const svo_octree_desc* octrees, uint32_t 
                                   o.traversal, o.stack_size};
     max_s = std::max(max_s, (int)o.stack_size);
   }
-  for (uint32_t i = 0; i < num_views; ++i) {
-    const int32_t m = views[i].params.mode;
-    if ((m == 0 || m == 1) && !octrees[views[i].octree].d_attribs) return SVO_ERR_INVALID;
-  }
+  const int mrc = check_batch_modes(views, num_views, octrees);
+  if (mrc != SVO_OK) return mrc;
   unsigned char* scratch = nullptr;
   int rc = scratch_address(&scratch);
   if (rc != SVO_OK) return rc;
@@ -115,7 +113,8 @@ extern "C" int svo_render_batch_static(const svo_octree_desc* octrees, uint32_t 
   L.tile_w = tile_w;
   L.tile_h = tile_h;
   L.threads = 256;
-  rc = batch_grid(tile_w, tile_h, max_s, L.threads, 0, 0, &L.blocks);
+  L.ext = batch_needs_ext(host_views, num_views);
+  rc = batch_grid(tile_w, tile_h, max_s, L.threads, 0, 0, &L.blocks, L.ext);
   if (rc != SVO_OK) return rc;
   return launch_batch(L, s);
 }

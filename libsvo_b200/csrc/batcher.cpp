@@ -18,7 +18,7 @@ uint64_t layout_views(const svo_view_desc* views, uint32_t num_views, uint32_t n
     const int32_t m = v.params.mode;
     if (v.octree >= num_octrees || !v.d_rgba || v.params.width == 0 || v.params.height == 0)
       return 0;
-    if (!(m == 0 || m == 1 || m == 3 || m == 4 || m == 5)) return 0;
+    if (m < 0 || m > 7) return 0;
     BatchView& b = out[i];
     b.params = v.params;
     b.octree = v.octree;
@@ -30,6 +30,17 @@ uint64_t layout_views(const svo_view_desc* views, uint32_t num_views, uint32_t n
     tiles += (uint64_t)b.tiles_x * ty;
   }
   return tiles;
+}
+
+int check_batch_modes(const svo_view_desc* views, uint32_t num_views,
+                      const svo_octree_desc* octrees) {
+  for (uint32_t i = 0; i < num_views; ++i) {
+    const int32_t m = views[i].params.mode;
+    const svo_octree_desc& o = octrees[views[i].octree];
+    if ((m == 0 || m == 1 || m == 6) && !o.d_attribs) return SVO_ERR_INVALID;
+    if ((m == 6 || m == 7) && o.traversal != SVO_TRAVERSAL_TREELET) return SVO_ERR_NOTSUP;
+  }
+  return SVO_OK;
 }
 
 }  // namespace svo
@@ -94,10 +105,8 @@ int apply(svo_batcher* b, const svo_batch_cfg& c, cudaStream_t stream) {
                                        o.traversal, o.stack_size};
     max_s = std::max(max_s, (int)o.stack_size);
   }
-  for (uint32_t i = 0; i < nv; ++i) {
-    const int32_t m = b->views[i].params.mode;
-    if ((m == 0 || m == 1) && !b->octrees[b->views[i].octree].d_attribs) return SVO_ERR_INVALID;
-  }
+  int mrc = svo::check_batch_modes(b->views.data(), nv, b->octrees.data());
+  if (mrc != SVO_OK) return mrc;
   SVO_CUDA_TRY(cudaMemcpyAsync(b->d_views, b->h_views, nv * sizeof(svo::BatchView),
                                cudaMemcpyHostToDevice, stream));
   SVO_CUDA_TRY(cudaMemcpyAsync(b->d_octrees, b->h_octrees, no * sizeof(svo::BatchOctree),
@@ -113,8 +122,9 @@ int apply(svo_batcher* b, const svo_batch_cfg& c, cudaStream_t stream) {
   L.tile_w = c.tile_w;
   L.tile_h = c.tile_h;
   L.threads = c.block_threads;
+  L.ext = svo::batch_needs_ext(b->h_views, nv);
   rc = svo::batch_grid(c.tile_w, c.tile_h, max_s, c.block_threads, c.top_nodes, c.blocks_per_sm,
-                       &L.blocks);
+                       &L.blocks, L.ext);
   if (rc != SVO_OK) return rc;
   b->launch = L;
   b->cfg = c;

@@ -507,7 +507,7 @@ int svo_server_submit(svo_server* s, const svo_request* req, uint64_t* ticket) {
   const double submitted = s ? s->now() : 0.0;  // before waiting for the lock
   if (!s || !req || !ticket || !req->d_rgba) return SVO_ERR_INVALID;
   const int32_t m = req->params.mode;
-  if (!(m == 0 || m == 1 || m == 3 || m == 4 || m == 5)) return SVO_ERR_NOTSUP;
+  if (m < 0 || m > 7) return SVO_ERR_NOTSUP;
   if (req->params.width == 0 || req->params.height == 0) return SVO_ERR_INVALID;
   {
     std::lock_guard<std::mutex> lk(s->mu);

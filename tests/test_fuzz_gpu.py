@@ -61,7 +61,8 @@ def test_random_frames(cuda, seed):
 
 def test_random_views_in_one_batch(cuda):
     """All random views of the frames above, over their own octrees, as one
-    batched launch (modes 0, 1, 3, 4, 5: the batch kernel's)."""
+    batched launch, all view modes mixed; then the same table without the
+    modes that need the extended instantiation."""
     import torch
 
     descs, views, checks, keep = [], [], [], []
@@ -69,7 +70,6 @@ def test_random_views_in_one_batch(cuda):
         rng = np.random.default_rng(seed)
         nodes, attribs = random_octree_pool(seed, depth=3 + seed % 5, fill=float(rng.uniform(0.2, 0.7)))
         p = random_view(rng, seed)
-        p.mode = int([0, 1, 3, 4, 5][seed % 5])
         dn = torch.from_numpy(nodes.view(np.int32)).to(cuda)
         da = torch.from_numpy(attribs.view(np.int32)).to(cuda)
         rgba = torch.empty((p.height, p.width), dtype=torch.int32, device=cuda)
@@ -80,6 +80,15 @@ def test_random_views_in_one_batch(cuda):
         keep += [dn, da]
     b = L.Batcher(max_views=64, max_octrees=64)
     b.set(descs, views, L.batch_cfg(tile_w=8, tile_h=4))
+    b.launch()
+    torch.cuda.synchronize()
+    for nodes, attribs, p, rgba, hits in checks:
+        check_frame(rgba.cpu().numpy().view(np.uint32), _hits_np(hits), nodes, attribs, p)
+    assert any(c[2].mode in (2, 6, 7) for c in checks)
+    for v, c in zip(views, checks):  # modes 0-5 only: the plain instantiation
+        if c[2].mode in (2, 6, 7):
+            v.params.mode = c[2].mode = 0
+    b.set(descs, views, L.batch_cfg(tile_w=16, tile_h=2))
     b.launch()
     torch.cuda.synchronize()
     for nodes, attribs, p, rgba, hits in checks:
