@@ -3,6 +3,7 @@
 // Every entry point validates its arguments, turns C++ exceptions (allocation
 // failures) into status codes, and never terminates the process.
 #include <cstring>
+#include <memory>
 #include <new>
 #include <string>
 #include <vector>
@@ -66,13 +67,10 @@ int build_scene(uint32_t depth, std::vector<uint64_t>& codes, std::vector<svo_at
   svo::Octree tree;
   int rc = svo::octree_from_leaves(depth, std::move(codes), std::move(attribs), tree);
   if (rc != SVO_OK) return rc;
-  svo_scene* s = new svo_scene;
+  std::unique_ptr<svo_scene> s(new svo_scene);
   rc = svo::cut_treelets(tree, treelet_levels, treelet_bytes, *s);
-  if (rc != SVO_OK) {
-    delete s;
-    return rc;
-  }
-  *out = s;
+  if (rc != SVO_OK) return rc;
+  *out = s.release();
   return SVO_OK;
 }
 
@@ -137,14 +135,11 @@ int svo_device_scene_build_mesh_attributed(const float* h_vertices, const float*
   if ((h_normals == nullptr) != (h_colors == nullptr)) return SVO_ERR_INVALID;
   *out = nullptr;
   return guarded([&] {
-    svo_device_scene* s = new svo_device_scene;
+    std::unique_ptr<svo_device_scene> s(new svo_device_scene);
     const int rc = s->impl.build_mesh(h_vertices, h_normals, h_colors, num_vertices, h_triangles,
                                       num_triangles, depth, treelet_levels, (cudaStream_t)stream);
-    if (rc != SVO_OK) {
-      delete s;
-      return rc;
-    }
-    *out = s;
+    if (rc != SVO_OK) return rc;
+    *out = s.release();
     return SVO_OK;
   });
 }
@@ -213,13 +208,10 @@ int svo_scene_read(const char* path_base, svo_scene** out) {
   if (!out || !path_base) return SVO_ERR_INVALID;
   *out = nullptr;
   return guarded([&] {
-    svo_scene* s = new svo_scene;
+    std::unique_ptr<svo_scene> s(new svo_scene);
     const int rc = svo::read_scene(path_base, *s);
-    if (rc != SVO_OK) {
-      delete s;
-      return rc;
-    }
-    *out = s;
+    if (rc != SVO_OK) return rc;
+    *out = s.release();
     return SVO_OK;
   });
 }
@@ -280,13 +272,10 @@ int svo_mm_create_from_scene(const svo_scene* scene, uint64_t incore_bytes, void
   *out = nullptr;
   return guarded([&] {
     svo_scene copy = *scene;
-    svo_mm* mm = new svo_mm((cudaStream_t)stream);
+    std::unique_ptr<svo_mm> mm(new svo_mm((cudaStream_t)stream));
     const int rc = mm->impl.init(std::move(copy), incore_bytes);
-    if (rc != SVO_OK) {
-      delete mm;
-      return rc;
-    }
-    *out = mm;
+    if (rc != SVO_OK) return rc;
+    *out = mm.release();
     return SVO_OK;
   });
 }
@@ -298,13 +287,10 @@ int svo_mm_create(const char* svo_path_base, uint64_t incore_bytes, void* stream
     svo_scene s;
     int rc = svo::read_scene(svo_path_base, s);
     if (rc != SVO_OK) return rc;
-    svo_mm* mm = new svo_mm((cudaStream_t)stream);
+    std::unique_ptr<svo_mm> mm(new svo_mm((cudaStream_t)stream));
     rc = mm->impl.init(std::move(s), incore_bytes);
-    if (rc != SVO_OK) {
-      delete mm;
-      return rc;
-    }
-    *out = mm;
+    if (rc != SVO_OK) return rc;
+    *out = mm.release();
     return SVO_OK;
   });
 }

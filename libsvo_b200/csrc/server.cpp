@@ -399,23 +399,8 @@ void dispatch_loop(svo_server* s) {
   }
 }
 
-}  // namespace
-
-extern "C" {
-
-int svo_server_create(const svo_server_cfg* cfg, svo_server** out) {
-  if (!cfg || !out) return SVO_ERR_INVALID;
-  *out = nullptr;
-  if (cfg->streams == 0 || cfg->streams > 16 || cfg->max_batch_views == 0 ||
-      cfg->max_batch_views > 4096 || cfg->max_inflight_rays == 0)
-    return SVO_ERR_RANGE;
-  if (cfg->mode != SVO_SERVE_BATCHED && cfg->mode != SVO_SERVE_PLAIN) return SVO_ERR_NOTSUP;
-  auto* s = new (std::nothrow) svo_server;
-  if (!s) return SVO_ERR_NOMEM;
-  s->cfg = *cfg;
-  if (s->cfg.tile_w == 0) s->cfg.tile_w = 8, s->cfg.tile_h = 4;
-  if (s->cfg.block_threads == 0) s->cfg.block_threads = 256;
-  s->t0 = Clock::now();
+// The pool, the slots' streams and batchers, and the dispatcher thread.
+int start_server(svo_server* s, const svo_server_cfg* cfg) {
   int rc = s->pool.init(cfg->hbm_budget_bytes);
   // Plain mode queues one per-frame kernel per request back to back on a
   // single stream (its slots share that stream); batched mode gives every
@@ -433,11 +418,40 @@ int svo_server_create(const svo_server_cfg* cfg, svo_server** out) {
     if (rc == SVO_OK && cfg->mode == SVO_SERVE_BATCHED)
       rc = svo_batcher_create(cfg->max_batch_views, 64, &sl.batcher);
   }
+  if (rc != SVO_OK) return rc;
+  s->dispatcher = std::thread(dispatch_loop, s);
+  return SVO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int svo_server_create(const svo_server_cfg* cfg, svo_server** out) {
+  if (!cfg || !out) return SVO_ERR_INVALID;
+  *out = nullptr;
+  if (cfg->streams == 0 || cfg->streams > 16 || cfg->max_batch_views == 0 ||
+      cfg->max_batch_views > 4096 || cfg->max_inflight_rays == 0)
+    return SVO_ERR_RANGE;
+  if (cfg->mode != SVO_SERVE_BATCHED && cfg->mode != SVO_SERVE_PLAIN) return SVO_ERR_NOTSUP;
+  auto* s = new (std::nothrow) svo_server;
+  if (!s) return SVO_ERR_NOMEM;
+  s->cfg = *cfg;
+  if (s->cfg.tile_w == 0) s->cfg.tile_w = 8, s->cfg.tile_h = 4;
+  if (s->cfg.block_threads == 0) s->cfg.block_threads = 256;
+  s->t0 = Clock::now();
+  int rc = SVO_OK;
+  try {
+    rc = start_server(s, cfg);
+  } catch (const std::bad_alloc&) {
+    rc = SVO_ERR_NOMEM;
+  } catch (...) {  // std::thread could not start
+    rc = SVO_ERR_INVALID;
+  }
   if (rc != SVO_OK) {
     svo_server_destroy(s);
     return rc;
   }
-  s->dispatcher = std::thread(dispatch_loop, s);
   *out = s;
   return SVO_OK;
 }
