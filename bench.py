@@ -48,9 +48,13 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the batched, served, large-shadowed and incore-update measurements")
+    ap.add_argument("--leg", choices=["batched", "served", "large_shadowed"],
+                    help="run only this measurement on one GPU and print its result: the 64 terrain "
+                         "views as one batched launch, the request server, or the large shadowed "
+                         "frame (--steps sets the timed repetitions of batched and large_shadowed)")
     ap.add_argument("--large-only", action="store_true",
                     help="run only the large shadowed measurement (icosphere built on the GPU, 3840x2160 "
-                         "primary + shadow frame) and print its result")
+                         "primary + shadow frame) and print its result; the same as --leg large_shadowed")
     ap.add_argument("--large-subdivisions", type=int, default=9)
     ap.add_argument("--large-depth", type=int, default=14)
     ap.add_argument("--shadow", action="store_true",
@@ -563,8 +567,14 @@ def main():
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     if args.large_only:
-        print(json.dumps(large_shadow_leg(dev, reps=args.steps, subdivisions=args.large_subdivisions,
-                                          depth=args.large_depth)), flush=True)
+        args.leg = "large_shadowed"
+    if args.leg:
+        legs = {"batched": lambda: batched_leg(dev, reps=args.steps),
+                "served": lambda: served_leg(dev),
+                "large_shadowed": lambda: large_shadow_leg(dev, reps=args.steps,
+                                                           subdivisions=args.large_subdivisions,
+                                                           depth=args.large_depth)}
+        print(json.dumps({"leg": args.leg, **legs[args.leg]()}), flush=True)
         return
     if world > 1:
         from datetime import timedelta

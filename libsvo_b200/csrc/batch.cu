@@ -29,7 +29,7 @@ namespace {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
-template <bool kExt>
+template <bool kExt, bool kTreelet>
 __device__ __forceinline__ void trace_tile_pixel(const BatchView& v, const BatchOctree& oct,
                                                  uint32_t x, uint32_t y, const uint2* top,
                                                  uint32_t top_count, uint2* stack, int stride,
@@ -37,7 +37,10 @@ __device__ __forceinline__ void trace_tile_pixel(const BatchView& v, const Batch
   float o[3], dx, dy, dz;
   pixel_ray(v.params, x, y, o, dx, dy, dz);
   RayHit h;
-  if (oct.traversal == SVO_TRAVERSAL_FLAT)
+  if (kTreelet)
+    h = cast_ray<false>(GlobalFetch{oct.nodes}, oct.num_nodes, o, dx, dy, dz,
+                        v.params.t_scale_ratio, oct.stack_size, stack, stride);
+  else if (oct.traversal == SVO_TRAVERSAL_FLAT)
     h = cast_ray<true>(GlobalFetch{oct.nodes}, oct.num_nodes, o, dx, dy, dz,
                        v.params.t_scale_ratio, oct.stack_size, stack, stride);
   else if (top_count)
@@ -58,7 +61,10 @@ __device__ __forceinline__ void trace_tile_pixel(const BatchView& v, const Batch
 
 // kExt: some view uses view mode 2, 6 or 7 (shade_ext); batches without
 // them run the instantiation that carries no extra exit state.
-template <int TW, int TH, bool kExt>
+// kTreelet: every octree takes the treelet traversal and no records are
+// staged, so only that traversal is compiled in (the register count and the
+// loop are then the per-frame kernel's).
+template <int TW, int TH, bool kExt, bool kTreelet>
 __global__ void batch_kernel(const BatchView* __restrict__ views, uint32_t num_views,
                              const BatchOctree* __restrict__ octrees, uint64_t total_tiles,
                              unsigned long long* __restrict__ counter, svo_stats* stats, int max_s,
@@ -69,7 +75,7 @@ __global__ void batch_kernel(const BatchView* __restrict__ views, uint32_t num_v
   const int stride = blockDim.x;
   uint2* top = smem + (size_t)max_s * blockDim.x;
   uint32_t top_count = 0;
-  if (top_nodes) {
+  if (!kTreelet && top_nodes) {
     const BatchOctree o0 = octrees[0];
     top_count = (uint32_t)min((uint64_t)top_nodes, o0.num_nodes);
     for (uint32_t i = threadIdx.x; i < top_count; i += blockDim.x) top[i] = __ldg(o0.nodes + i);
@@ -96,7 +102,7 @@ __global__ void batch_kernel(const BatchView* __restrict__ views, uint32_t num_v
     const uint32_t x = tx * TW + lane % TW, y = ty * TH + lane / TW;
     if (x < v.params.width && y < v.params.height) {
       const BatchOctree& oct = octrees[v.octree];
-      trace_tile_pixel<kExt>(v, oct, x, y, top, v.octree == 0 ? top_count : 0u, stack, stride, stats);
+      trace_tile_pixel<kExt, kTreelet>(v, oct, x, y, top, v.octree == 0 ? top_count : 0u, stack, stride, stats);
     }
     __syncwarp();
   }
@@ -105,22 +111,32 @@ __global__ void batch_kernel(const BatchView* __restrict__ views, uint32_t num_v
 typedef void (*BatchKernelFn)(const BatchView*, uint32_t, const BatchOctree*, uint64_t,
                               unsigned long long*, svo_stats*, int, uint32_t);
 
-template <bool kExt>
+template <bool kExt, bool kTreelet>
 BatchKernelFn kernel_for_t(uint32_t tw, uint32_t th) {
-  if (tw == 8 && th == 4) return batch_kernel<8, 4, kExt>;
-  if (tw == 16 && th == 2) return batch_kernel<16, 2, kExt>;
-  if (tw == 4 && th == 8) return batch_kernel<4, 8, kExt>;
-  if (tw == 32 && th == 1) return batch_kernel<32, 1, kExt>;
+  if (tw == 8 && th == 4) return batch_kernel<8, 4, kExt, kTreelet>;
+  if (tw == 16 && th == 2) return batch_kernel<16, 2, kExt, kTreelet>;
+  if (tw == 4 && th == 8) return batch_kernel<4, 8, kExt, kTreelet>;
+  if (tw == 32 && th == 1) return batch_kernel<32, 1, kExt, kTreelet>;
   return nullptr;
 }
 
-BatchKernelFn kernel_for(uint32_t tw, uint32_t th, bool ext) {
-  return ext ? kernel_for_t<true>(tw, th) : kernel_for_t<false>(tw, th);
+BatchKernelFn kernel_for(uint32_t tw, uint32_t th, bool ext, bool treelet_only) {
+  if (treelet_only) return ext ? kernel_for_t<true, true>(tw, th) : kernel_for_t<false, true>(tw, th);
+  return ext ? kernel_for_t<true, false>(tw, th) : kernel_for_t<false, false>(tw, th);
 }
 
 }  // namespace
 
-bool batch_tile_supported(uint32_t tw, uint32_t th) { return kernel_for(tw, th, false) != nullptr; }
+bool batch_tile_supported(uint32_t tw, uint32_t th) {
+  return kernel_for(tw, th, false, false) != nullptr;
+}
+
+bool batch_treelet_only(const BatchOctree* octrees, uint32_t num_octrees, uint32_t top_nodes) {
+  if (top_nodes) return false;
+  for (uint32_t i = 0; i < num_octrees; ++i)
+    if (octrees[i].traversal != SVO_TRAVERSAL_TREELET) return false;
+  return true;
+}
 
 bool batch_needs_ext(const BatchView* views, uint32_t num_views) {
   for (uint32_t i = 0; i < num_views; ++i) {
@@ -135,7 +151,7 @@ size_t batch_smem_bytes(int max_s, uint32_t threads, uint32_t top_nodes) {
 }
 
 int launch_batch(const BatchLaunch& L, cudaStream_t stream) {
-  BatchKernelFn fn = kernel_for(L.tile_w, L.tile_h, L.ext);
+  BatchKernelFn fn = kernel_for(L.tile_w, L.tile_h, L.ext, L.treelet_only);
   if (!fn) return SVO_ERR_NOTSUP;
   const size_t smem = batch_smem_bytes(L.max_s, L.threads, L.top_nodes);
   if (smem > 48u * 1024u) {
@@ -147,8 +163,8 @@ int launch_batch(const BatchLaunch& L, cudaStream_t stream) {
 }
 
 int batch_grid(uint32_t tile_w, uint32_t tile_h, int max_s, uint32_t threads, uint32_t top_nodes,
-               uint32_t blocks_per_sm, uint32_t* blocks, bool ext) {
-  BatchKernelFn fn = kernel_for(tile_w, tile_h, ext);
+               uint32_t blocks_per_sm, uint32_t* blocks, bool ext, bool treelet_only) {
+  BatchKernelFn fn = kernel_for(tile_w, tile_h, ext, treelet_only);
   if (!fn) return SVO_ERR_NOTSUP;
   const size_t smem = batch_smem_bytes(max_s, threads, top_nodes);
   if (smem > 48u * 1024u) {

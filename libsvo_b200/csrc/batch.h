@@ -41,16 +41,21 @@ struct BatchLaunch {
   uint32_t top_nodes = 0;
   uint32_t tile_w = 8, tile_h = 4;
   uint32_t threads = 256, blocks = 0;
-  bool ext = false;  // some view uses view mode 2, 6 or 7
+  bool ext = false;           // some view uses view mode 2, 6 or 7
+  bool treelet_only = false;  // treelet traversal everywhere, nothing staged
 };
 
 bool batch_tile_supported(uint32_t tile_w, uint32_t tile_h);
 size_t batch_smem_bytes(int max_s, uint32_t threads, uint32_t top_nodes);
 // Persistent grid size: blocks_per_sm (0 = as many as fit) times the SM count.
 int batch_grid(uint32_t tile_w, uint32_t tile_h, int max_s, uint32_t threads, uint32_t top_nodes,
-               uint32_t blocks_per_sm, uint32_t* blocks, bool ext = false);
+               uint32_t blocks_per_sm, uint32_t* blocks, bool ext = false,
+               bool treelet_only = false);
 // Whether a view of the table uses view mode 2, 6 or 7.
 bool batch_needs_ext(const BatchView* views, uint32_t num_views);
+// Whether every octree takes the treelet traversal and no records are staged
+// (the launch then runs the instantiation without the other traversals).
+bool batch_treelet_only(const BatchOctree* octrees, uint32_t num_octrees, uint32_t top_nodes);
 // Launches the kernel; the caller has zeroed *counter on the same stream.
 int launch_batch(const BatchLaunch& launch, cudaStream_t stream);
 

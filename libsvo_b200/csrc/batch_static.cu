@@ -114,7 +114,8 @@ extern "C" int svo_render_batch_static(const svo_octree_desc* octrees, uint32_t 
   L.tile_h = tile_h;
   L.threads = 256;
   L.ext = batch_needs_ext(host_views, num_views);
-  rc = batch_grid(tile_w, tile_h, max_s, L.threads, 0, 0, &L.blocks, L.ext);
+  L.treelet_only = batch_treelet_only(host_octrees, num_octrees, 0);
+  rc = batch_grid(tile_w, tile_h, max_s, L.threads, 0, 0, &L.blocks, L.ext, L.treelet_only);
   if (rc != SVO_OK) return rc;
   return launch_batch(L, s);
 }

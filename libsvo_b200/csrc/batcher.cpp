@@ -123,8 +123,9 @@ int apply(svo_batcher* b, const svo_batch_cfg& c, cudaStream_t stream) {
   L.tile_h = c.tile_h;
   L.threads = c.block_threads;
   L.ext = svo::batch_needs_ext(b->h_views, nv);
+  L.treelet_only = svo::batch_treelet_only(b->h_octrees, no, c.top_nodes);
   rc = svo::batch_grid(c.tile_w, c.tile_h, max_s, c.block_threads, c.top_nodes, c.blocks_per_sm,
-                       &L.blocks, L.ext);
+                       &L.blocks, L.ext, L.treelet_only);
   if (rc != SVO_OK) return rc;
   b->launch = L;
   b->cfg = c;
