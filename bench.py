@@ -48,10 +48,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the batched, served, large-shadowed and incore-update measurements")
-    ap.add_argument("--leg", choices=["batched", "served", "large_shadowed"],
+    ap.add_argument("--leg", choices=["batched", "served", "large_shadowed", "incore_update", "streaming"],
                     help="run only this measurement on one GPU and print its result: the 64 terrain "
-                         "views as one batched launch, the request server, or the large shadowed "
-                         "frame (--steps sets the timed repetitions of batched and large_shadowed)")
+                         "views as one batched launch, the request server, the large shadowed "
+                         "frame, the incore-update policies or the streaming loop on the icosphere "
+                         "scene (--steps sets the timed repetitions of batched and large_shadowed)")
     ap.add_argument("--large-only", action="store_true",
                     help="run only the large shadowed measurement (icosphere built on the GPU, 3840x2160 "
                          "primary + shadow frame) and print its result; the same as --leg large_shadowed")
@@ -573,7 +574,9 @@ def main():
                 "served": lambda: served_leg(dev),
                 "large_shadowed": lambda: large_shadow_leg(dev, reps=args.steps,
                                                            subdivisions=args.large_subdivisions,
-                                                           depth=args.large_depth)}
+                                                           depth=args.large_depth),
+                "incore_update": lambda: incore_update_leg(dev, make_workload("icosphere").scene),
+                "streaming": lambda: streaming_leg(dev, make_workload("icosphere").scene)}
         print(json.dumps({"leg": args.leg, **legs[args.leg]()}), flush=True)
         return
     if world > 1:

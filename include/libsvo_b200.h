@@ -447,16 +447,28 @@ int svo_mm_analyse_feedback(svo_mm* mm, const svo_feedback* h_feedback, uint64_t
                             int32_t* new_gids, float* new_errors, uint32_t new_capacity,
                             uint32_t* num_new, int32_t* old_gids, float* old_errors,
                             uint32_t old_capacity, uint32_t* num_old);
+/* The same processing over records in device memory (d_feedback, as
+ * svo_feedback_render writes them): the records are folded on the GPU into
+ * per-treelet largest errors and only those come back (4 bytes per treelet
+ * per list instead of 16 bytes per record); lists and statuses as
+ * svo_mm_analyse_feedback on the same records.  Blocks until the lists are
+ * on the host.  Needs svo_mm_init_device_buffer. */
+int svo_mm_analyse_feedback_device(svo_mm* mm, const svo_feedback* d_feedback, uint64_t n,
+                                   uint32_t max_new, void* stream, int32_t* new_gids,
+                                   float* new_errors, uint32_t new_capacity, uint32_t* num_new,
+                                   int32_t* old_gids, float* old_errors, uint32_t old_capacity,
+                                   uint32_t* num_old);
 /* One dynamic-loading step of the reference's frame loop
  * (raycast_serialized_opencl.cpp:684-716): the analysis pass over the
  * frame's view at (width/divisor, height/divisor) with the far plane's
  * origin offset by (jitter_x, jitter_y) * divisor / 2 frame pixels (the
  * reference's "rumble", RenderPassAnalyse.cpp:176-184; jitter in [-1, 1]),
- * records read back, analysed, treelets inserted (evicting by visibility)
- * and uploaded.  Blocks until the records are on the host.  *num_new: the
- * treelets placed; like the reference's updateClientSideIncoreBuffer, the
- * step skips new treelets that find no slot under memory pressure (the next
- * step asks for them again).  *num_old: visible resident treelets. */
+ * records analysed on the GPU (svo_mm_analyse_feedback_device), treelets
+ * inserted (evicting by visibility) and uploaded.  Blocks until the analysis
+ * lists are on the host.  *num_new: the treelets placed; like the
+ * reference's updateClientSideIncoreBuffer, the step skips new treelets that
+ * find no slot under memory pressure (the next step asks for them again).
+ * *num_old: visible resident treelets. */
 int svo_mm_analysis_step(svo_mm* mm, const svo_frame_params* frame, uint32_t divisor,
                          float jitter_x, float jitter_y, int32_t stack_size, void* stream,
                          uint32_t* num_new, uint32_t* num_old);

@@ -982,6 +982,8 @@ for _name, (_args, _res) in {
     "svo_feedback_render": ([_vp, _u64, _P(svo_frame_params), _i32, _vp, _vp, _vp], ctypes.c_int),
     "svo_mm_analyse_feedback": ([_vp, _vp, _u64, _u32, _vp, _vp, _u32, _P(_u32), _vp, _vp, _u32, _P(_u32)],
                                 ctypes.c_int),
+    "svo_mm_analyse_feedback_device": ([_vp, _vp, _u64, _u32, _vp, _vp, _vp, _u32, _P(_u32), _vp, _vp, _u32,
+                                        _P(_u32)], ctypes.c_int),
     "svo_mm_analysis_step": ([_vp, _P(svo_frame_params), _u32, _f32, _f32, _i32, _vp, _P(_u32), _P(_u32)],
                              ctypes.c_int),
 }.items():
@@ -1013,6 +1015,21 @@ def _analyse_feedback(self, records: np.ndarray, max_new: int = 0):
     return list(zip(ng.tolist(), ne.tolist())), list(zip(og.tolist(), oe.tolist()))
 
 
+def _analyse_feedback_device(self, d_records, n: int, max_new: int = 0, stream=None):
+    """The same processing over n records in device memory, folded on the GPU:
+    ([(gid, error)] new, [(gid, error)] old)."""
+    cap = self.info.num_treelets + 1  # neither list can be longer
+    nn, no = _u32(), _u32()
+    ng = np.zeros(cap, np.int32); ne = np.zeros(cap, np.float32)
+    og = np.zeros(cap, np.int32); oe = np.zeros(cap, np.float32)
+    _check(_L.svo_mm_analyse_feedback_device(self._h, _dptr(d_records), n, max_new, _stream_ptr(stream),
+                                             _np_ptr(ng), _np_ptr(ne), cap, ctypes.byref(nn), _np_ptr(og),
+                                             _np_ptr(oe), cap, ctypes.byref(no)),
+           "svo_mm_analyse_feedback_device")
+    k, m = nn.value, no.value
+    return list(zip(ng[:k].tolist(), ne[:k].tolist())), list(zip(og[:m].tolist(), oe[:m].tolist()))
+
+
 def _perform_analyse_pass(self, frame: svo_frame_params, divisor=8, jitter=(0.0, 0.0), stack_size=13,
                           stream=None):
     """One dynamic-loading step (analysis pass, insert, upload): (new, old) counts."""
@@ -1024,6 +1041,7 @@ def _perform_analyse_pass(self, frame: svo_frame_params, divisor=8, jitter=(0.0,
 
 
 TreeletMemoryManagerCuda.analyseFeedback = _analyse_feedback
+TreeletMemoryManagerCuda.analyseFeedbackDevice = _analyse_feedback_device
 TreeletMemoryManagerCuda.performAnalysePass = _perform_analyse_pass
 
 

@@ -74,6 +74,27 @@ int build_scene(uint32_t depth, std::vector<uint64_t>& codes, std::vector<svo_at
   return SVO_OK;
 }
 
+// Copies analysis lists to caller arrays (svo_mm_analyse_feedback*).
+int export_lists(int rc, const std::vector<std::pair<int32_t, float>>& nw,
+                 const std::vector<std::pair<int32_t, float>>& old, int32_t* new_gids,
+                 float* new_errors, uint32_t new_capacity, uint32_t* num_new, int32_t* old_gids,
+                 float* old_errors, uint32_t old_capacity, uint32_t* num_old) {
+  if (num_new) *num_new = (uint32_t)nw.size();
+  if (num_old) *num_old = (uint32_t)old.size();
+  if (rc != SVO_OK) return rc;
+  if ((new_gids || new_errors) && nw.size() > new_capacity) return SVO_ERR_RANGE;
+  if ((old_gids || old_errors) && old.size() > old_capacity) return SVO_ERR_RANGE;
+  for (size_t i = 0; i < nw.size(); ++i) {
+    if (new_gids) new_gids[i] = nw[i].first;
+    if (new_errors) new_errors[i] = nw[i].second;
+  }
+  for (size_t i = 0; i < old.size(); ++i) {
+    if (old_gids) old_gids[i] = old[i].first;
+    if (old_errors) old_errors[i] = old[i].second;
+  }
+  return SVO_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -563,20 +584,24 @@ int svo_mm_analyse_feedback(svo_mm* mm, const svo_feedback* h_feedback, uint64_t
     std::vector<std::pair<int32_t, float>> nw, old;
     const uint32_t cap = max_new ? max_new : mm->impl.default_max_new_treelets();
     const int rc = mm->impl.analyse_feedback(h_feedback, n, cap, nw, old);
-    if (num_new) *num_new = (uint32_t)nw.size();
-    if (num_old) *num_old = (uint32_t)old.size();
-    if (rc != SVO_OK) return rc;
-    if ((new_gids || new_errors) && nw.size() > new_capacity) return SVO_ERR_RANGE;
-    if ((old_gids || old_errors) && old.size() > old_capacity) return SVO_ERR_RANGE;
-    for (size_t i = 0; i < nw.size(); ++i) {
-      if (new_gids) new_gids[i] = nw[i].first;
-      if (new_errors) new_errors[i] = nw[i].second;
-    }
-    for (size_t i = 0; i < old.size(); ++i) {
-      if (old_gids) old_gids[i] = old[i].first;
-      if (old_errors) old_errors[i] = old[i].second;
-    }
-    return SVO_OK;
+    return export_lists(rc, nw, old, new_gids, new_errors, new_capacity, num_new, old_gids,
+                        old_errors, old_capacity, num_old);
+  });
+}
+
+int svo_mm_analyse_feedback_device(svo_mm* mm, const svo_feedback* d_feedback, uint64_t n,
+                                   uint32_t max_new, void* stream, int32_t* new_gids,
+                                   float* new_errors, uint32_t new_capacity, uint32_t* num_new,
+                                   int32_t* old_gids, float* old_errors, uint32_t old_capacity,
+                                   uint32_t* num_old) {
+  if (!mm || (n && !d_feedback) || !mm->impl.device_ready()) return SVO_ERR_INVALID;
+  return guarded([&] {
+    std::vector<std::pair<int32_t, float>> nw, old;
+    const uint32_t cap = max_new ? max_new : mm->impl.default_max_new_treelets();
+    cudaStream_t s = stream ? (cudaStream_t)stream : mm->impl.render_stream();
+    const int rc = mm->impl.analyse_feedback_device(d_feedback, n, cap, nw, old, s);
+    return export_lists(rc, nw, old, new_gids, new_errors, new_capacity, num_new, old_gids,
+                        old_errors, old_capacity, num_old);
   });
 }
 
@@ -609,11 +634,9 @@ int svo_mm_analysis_step(svo_mm* mm, const svo_frame_params* frame, uint32_t div
     rc = svo::launch_feedback(mm->impl.device_nodes(), mm->impl.incore_nodes(), a, stack_size, d_fb,
                               nullptr, s);
     if (rc != SVO_OK) return rc;
-    std::vector<svo_feedback> h(n);
-    SVO_CUDA_TRY(cudaMemcpyAsync(h.data(), d_fb, n * sizeof(svo_feedback), cudaMemcpyDeviceToHost, s));
-    SVO_CUDA_TRY(cudaStreamSynchronize(s));
+    // the records stay on the GPU; only per-treelet results come back
     std::vector<std::pair<int32_t, float>> nw, old;
-    rc = mm->impl.analyse_feedback(h.data(), n, mm->impl.default_max_new_treelets(), nw, old);
+    rc = mm->impl.analyse_feedback_device(d_fb, n, mm->impl.default_max_new_treelets(), nw, old, s);
     if (num_new) *num_new = (uint32_t)nw.size();
     if (num_old) *num_old = (uint32_t)old.size();
     if (rc != SVO_OK) return rc;

@@ -6,6 +6,7 @@
 #include <cstring>
 #include <deque>
 
+#include "analysis.h"
 #include "errors.h"
 #include "render.h"
 #include "upload.h"
@@ -268,6 +269,11 @@ TreeletMemoryManagerCuda::~TreeletMemoryManagerCuda() {
   cudaFree(d_stats_);
   cudaFree(d_rgba_);
   cudaFree(d_feedback_);
+  cudaFree(d_slot_gid_);
+  cudaFree(d_parent_);
+  cudaFree(d_keys_);
+  if (h_slot_gid_) cudaFreeHost(h_slot_gid_);
+  if (h_keys_) cudaFreeHost(h_keys_);
   for (int i = 0; i < 2; ++i) {
     if (stage_evt_[i]) cudaEventDestroy(stage_evt_[i]);
     if (stage_[i]) cudaFreeHost(stage_[i]);
@@ -554,6 +560,81 @@ int TreeletMemoryManagerCuda::render_to_host_async(const svo_frame_params& p,
 
 int TreeletMemoryManagerCuda::wait_host_frames() {
   if (d2h_stream_) SVO_CUDA_TRY(cudaStreamSynchronize(d2h_stream_));
+  return SVO_OK;
+}
+
+int TreeletMemoryManagerCuda::init_analysis() {
+  if (d_keys_) return SVO_OK;
+  const uint32_t T = num_treelets(), S = num_slots();
+  const size_t key_words = 2 * ((size_t)T + 1) + 1;
+  std::vector<int32_t> parent(T > 0 ? T : 1, 0);
+  for (uint32_t g = 0; g < T; ++g) parent[g] = scene_.treelets[g].parent_gid;
+  int32_t* d_slot = nullptr;
+  int32_t* h_slot = nullptr;
+  int32_t* d_par = nullptr;
+  uint32_t* d_keys = nullptr;
+  uint32_t* h_keys = nullptr;
+  auto fail = [&](cudaError_t e) {
+    cudaFree(d_slot);
+    cudaFree(d_par);
+    cudaFree(d_keys);
+    if (h_slot) cudaFreeHost(h_slot);
+    if (h_keys) cudaFreeHost(h_keys);
+    return cuda_status(e);
+  };
+  cudaError_t e = cudaMalloc(&d_slot, (size_t)S * sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMallocHost(&h_slot, (size_t)S * sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&d_par, parent.size() * sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&d_keys, key_words * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMallocHost(&h_keys, key_words * sizeof(uint32_t));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(d_par, parent.data(), parent.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return fail(e);
+  d_slot_gid_ = d_slot;
+  h_slot_gid_ = h_slot;
+  d_parent_ = d_par;
+  d_keys_ = d_keys;
+  h_keys_ = h_keys;
+  return SVO_OK;
+}
+
+int TreeletMemoryManagerCuda::analyse_feedback_device(
+    const svo_feedback* d_fb, uint64_t n, uint32_t max_new,
+    std::vector<std::pair<int32_t, float>>& out_new, std::vector<std::pair<int32_t, float>>& out_old,
+    cudaStream_t stream) {
+  out_new.clear();
+  out_old.clear();
+  if (n > 0 && !d_fb) return SVO_ERR_INVALID;
+  int rc = init_analysis();
+  if (rc != SVO_OK) return rc;
+  const uint32_t T = num_treelets(), S = num_slots();
+  const size_t words = 2 * ((size_t)T + 1) + 1;
+  uint32_t* d_new = d_keys_;
+  uint32_t* d_old = d_keys_ + (T + 1);
+  uint32_t* d_status = d_keys_ + 2 * ((size_t)T + 1);
+  // the page-locked slot table is free: the previous pass waited for its copy
+  for (uint32_t i = 0; i < S; ++i) h_slot_gid_[i] = slots_[i].treelet_gid;
+  SVO_CUDA_TRY(cudaMemcpyAsync(d_slot_gid_, h_slot_gid_, (size_t)S * sizeof(int32_t),
+                               cudaMemcpyHostToDevice, stream));
+  SVO_CUDA_TRY(cudaMemsetAsync(d_keys_, 0, words * sizeof(uint32_t), stream));
+  rc = launch_analyse(d_fb, n, d_slot_gid_, S, N_, d_parent_, T, d_new, d_old, d_status, stream);
+  if (rc != SVO_OK) return rc;
+  SVO_CUDA_TRY(cudaMemcpyAsync(h_keys_, d_keys_, words * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                               stream));
+  SVO_CUDA_TRY(cudaStreamSynchronize(stream));
+  if (h_keys_[2 * ((size_t)T + 1)] & kAnalyseRejected) return SVO_ERR_RANGE;
+  const uint32_t* h_new = h_keys_;
+  const uint32_t* h_old = h_keys_ + (T + 1);
+  for (uint32_t g = 0; g <= T; ++g) {
+    if (h_new[g]) out_new.emplace_back((int32_t)g, key_error(h_new[g]));
+    if (h_old[g]) out_old.emplace_back((int32_t)g, key_error(h_old[g]));
+  }
+  auto by_error = [](const std::pair<int32_t, float>& a, const std::pair<int32_t, float>& b) {
+    return a.second > b.second;
+  };
+  std::stable_sort(out_new.begin(), out_new.end(), by_error);
+  std::stable_sort(out_old.begin(), out_old.end(), by_error);
+  if (out_new.size() > max_new) out_new.resize(max_new);
   return SVO_OK;
 }
 

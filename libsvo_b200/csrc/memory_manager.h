@@ -146,8 +146,18 @@ class TreeletMemoryManagerCuda : public TreeletMemoryManager {
   int wait_host_frames();
   // Device feedback-record scratch for analysis passes (grown on demand).
   int feedback_scratch(uint64_t records, svo_feedback** out);
+  // analyse_feedback over n records in device memory: the records are folded
+  // on the GPU into per-treelet largest-error arrays (launch_analyse) and
+  // only those come back, 4 bytes per treelet each.  Same lists and statuses
+  // as analyse_feedback on the same records.  Blocks until the lists are on
+  // the host.
+  int analyse_feedback_device(const svo_feedback* d_fb, uint64_t n, uint32_t max_new,
+                              std::vector<std::pair<int32_t, float>>& out_new,
+                              std::vector<std::pair<int32_t, float>>& out_old,
+                              cudaStream_t stream);
 
  private:
+  int init_analysis();
   int stage_copy(void* dst, const void* src, uint64_t bytes);
   int upload_packed(uint32_t* copy_calls);
   void before_host_write() override;
@@ -188,6 +198,14 @@ class TreeletMemoryManagerCuda : public TreeletMemoryManager {
   int img_next_ = 0;
   svo_feedback* d_feedback_ = nullptr;
   uint64_t d_feedback_records_ = 0;
+  // device analysis: the slot -> gid table (refreshed per pass through a
+  // page-locked copy), treelet parents, and the key arrays
+  // [new: T + 1 | old: T + 1 | status] with their page-locked host copy
+  int32_t* d_slot_gid_ = nullptr;
+  int32_t* h_slot_gid_ = nullptr;
+  int32_t* d_parent_ = nullptr;
+  uint32_t* d_keys_ = nullptr;
+  uint32_t* h_keys_ = nullptr;
 };
 
 }  // namespace svo
