@@ -483,7 +483,46 @@ def streaming_run(dev, scene, policy, frames=150, incore_mb=256, size=1024):
             "treelets_inserted": new_total, "resident_slots_at_end": info.num_slots - info.free_slots}
 
 
-def large_shadow_leg(dev, reps=10, cap_gb=60.0, subdivisions=9, depth=14):
+def host_memory_available() -> int:
+    """Bytes this process may still allocate: the host's available memory,
+    capped by the container's memory limit when there is one."""
+    import psutil
+
+    avail = psutil.virtual_memory().available
+    for limit, usage in (("/sys/fs/cgroup/memory.max", "/sys/fs/cgroup/memory.current"),
+                         ("/sys/fs/cgroup/memory/memory.limit_in_bytes",
+                          "/sys/fs/cgroup/memory/memory.usage_in_bytes")):
+        try:
+            lim = Path(limit).read_text().strip()
+            if lim != "max" and int(lim) < (1 << 60):
+                avail = min(avail, int(lim) - int(Path(usage).read_text().strip()))
+        except (OSError, ValueError):
+            pass
+    return avail
+
+
+def large_cpu_baseline(wl, n, seconds=10.0):
+    """The reference's shadow frame compiled for the host over the large
+    pool: the pool is copied to host memory (16 bytes per node), then whole
+    frames are timed on all host threads.  Skipped, with the reason, unless
+    the host has twice the pool's size free."""
+    import types
+
+    need = 16 * n
+    avail = host_memory_available()
+    if avail < 2 * need + (16 << 30):
+        return {"unavailable": f"the pool copy needs {need / 1e9:.1f} GB of host memory, "
+                               f"{avail / 1e9:.1f} GB available"}
+    t0 = time.perf_counter()
+    nodes, attribs = wl.scene.getIncoreBuffer()
+    copy_s = time.perf_counter() - t0
+    one_view = types.SimpleNamespace(cameras=[wl.camera], stack_size=wl.stack_size)
+    out = cpu_reference_frames(one_view, nodes, attribs, seconds=seconds, light=wl.light)
+    out["sample"] += f"; the {need / 1e9:.1f} GB pool copied to host memory first ({copy_s:.1f} s, untimed)"
+    return out
+
+
+def large_shadow_leg(dev, reps=10, cap_gb=60.0, subdivisions=9, depth=14, cpu_baseline=True):
     """The large shadowed workload: the depth-14 icosphere built on the GPU, one
     3840x2160 frame of primary rays plus one shadow ray per hit.  The metric
     counts both kinds of ray."""
@@ -544,6 +583,12 @@ def large_shadow_leg(dev, reps=10, cap_gb=60.0, subdivisions=9, depth=14):
            "roofline": {"algorithmic_bytes_per_frame": algo_bytes, "achieved_gbs": algo_bytes / ms / 1e6,
                         "frac": algo_bytes / ms / 1e6 / peak, "node_reads_per_ray": fetches / rays,
                         "traffic": _profiled_traffic(wl.name)}}
+    del flush, rgba
+    if cpu_baseline:
+        try:
+            out["cpu_baseline"] = large_cpu_baseline(wl, n)
+        except Exception as e:  # the host copy or the CPU run failed: keep the GPU result
+            out["cpu_baseline"] = {"unavailable": f"{type(e).__name__}: {e}"}
     wl.scene.close()
     return out
 
@@ -574,7 +619,8 @@ def main():
                 "served": lambda: served_leg(dev),
                 "large_shadowed": lambda: large_shadow_leg(dev, reps=args.steps,
                                                            subdivisions=args.large_subdivisions,
-                                                           depth=args.large_depth),
+                                                           depth=args.large_depth,
+                                                           cpu_baseline=not args.no_cpu_baseline),
                 "incore_update": lambda: incore_update_leg(dev, make_workload("icosphere").scene),
                 "streaming": lambda: streaming_leg(dev, make_workload("icosphere").scene)}
         print(json.dumps({"leg": args.leg, **legs[args.leg]()}), flush=True)
@@ -736,8 +782,9 @@ def main():
                 except Exception as e:  # a failing extra leg must not lose the primary line
                     line[key] = {"error": f"{type(e).__name__}: {e}"}
         if world == 1 and not args.no_extra:
-            for key, leg in (("batched", batched_leg), ("served", served_leg),
-                             ("large_shadowed", large_shadow_leg)):
+            legs = (("batched", batched_leg), ("served", served_leg),
+                    ("large_shadowed", lambda d: large_shadow_leg(d, cpu_baseline=not args.no_cpu_baseline)))
+            for key, leg in legs:
                 try:
                     line[key] = leg(dev)
                 except Exception as e:  # a failing extra leg must not lose the primary line
