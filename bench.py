@@ -339,9 +339,12 @@ def served_leg(dev, n=400, rates=(4000, 16000, 64000)):
     outs = [torch.empty((c.height, c.width), dtype=torch.int32, device=dev) for _, c in reqs]
     rays = sum(c.width * c.height for _, c in reqs)
 
-    def run(mode, budget, rate_list):
+    def run(mode, budget, rate_list, upload=None):
         srv = L.Server(L.server_cfg(budget, streams=4, max_batch_views=256, mode=mode))
         ids = [srv.add_octree(s) for s in wl.scenes]
+        if upload is not None:
+            for i in ids:
+                srv.set_upload_policy(i, upload)
         rq = [L.request(ids[o], c.frame_params(), t) for (o, c), t in zip(reqs, outs)]
         srv.replay(rq[:64], np.zeros(64), timeout_ms=120000)  # first loads
         res = {}
@@ -363,6 +366,7 @@ def served_leg(dev, n=400, rates=(4000, 16000, 64000)):
     batched = run(L.SERVE_BATCHED, 2 * footprint, all_rates)
     plain = run(L.SERVE_PLAIN, 2 * footprint, all_rates)
     paging = run(L.SERVE_BATCHED, footprint // 2, [16000])
+    paging_pinned = run(L.SERVE_BATCHED, footprint // 2, [16000], upload=L.UPLOAD_PINNED)
     return {"workload": wl.name, "description": wl.description, "requests": n, "rays": rays,
             "scene_build_s": round(build_s, 2), "octree_footprint_gb": footprint / 1e9,
             "budget_note": "the stand-in octrees total far less than the configuration's 40 GB cap; "
@@ -370,7 +374,8 @@ def served_leg(dev, n=400, rates=(4000, 16000, 64000)):
             "batched": batched, "plain": plain,
             "speedup_vs_plain": {k: batched[k]["mrays_s"] / plain[k]["mrays_s"]
                                  for k in batched if k != "paging"},
-            "paging_half_budget": paging}
+            "paging_half_budget": paging,
+            "paging_half_budget_pinned_hosts": paging_pinned}
 
 
 def incore_update_leg(dev, scene, incore_mb=256, frames=20, seed=5):

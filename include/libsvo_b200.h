@@ -602,6 +602,11 @@ void svo_server_destroy(svo_server* s);
 /* Registers an octree (copied) with the given stack size; not resident
  * until a request needs it. */
 int svo_server_add_octree(svo_server* s, const svo_scene* scene, int32_t stack_size, uint32_t* id);
+/* How octree `octree` reaches the device pool (SVO_UPLOAD_*).
+ * SVO_UPLOAD_PINNED page-locks its host copy once, here, so that every
+ * later load is two DMA copies at PCIe speed issued without host copying
+ * (default: staged through a pinned ring, bound by the host memcpy). */
+int svo_server_set_upload_policy(svo_server* s, uint32_t octree, int32_t policy);
 int svo_server_submit(svo_server* s, const svo_request* req, uint64_t* ticket);
 /* Bounded wait: SVO_ERR_TIMEOUT after timeout_ms. */
 int svo_server_wait(svo_server* s, uint64_t ticket, uint32_t timeout_ms, svo_request_result* out);

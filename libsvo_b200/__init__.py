@@ -881,6 +881,7 @@ for _name, (_args, _res) in {
     "svo_server_create": ([_P(svo_server_cfg), _P(_vp)], ctypes.c_int),
     "svo_server_destroy": ([_vp], None),
     "svo_server_add_octree": ([_vp, _vp, _i32, _P(_u32)], ctypes.c_int),
+    "svo_server_set_upload_policy": ([_vp, _u32, _i32], ctypes.c_int),
     "svo_server_submit": ([_vp, _P(svo_request), _P(_u64)], ctypes.c_int),
     "svo_server_wait": ([_vp, _u64, _u32, _P(svo_request_result)], ctypes.c_int),
     "svo_server_poll": ([_vp, _u64, _P(svo_request_result)], ctypes.c_int),
@@ -923,6 +924,11 @@ class Server:
         _check(_L.svo_server_add_octree(self._h, scene._h, stack_size, ctypes.byref(i)),
                "svo_server_add_octree")
         return i.value
+
+    def set_upload_policy(self, octree: int, policy: int):
+        """UPLOAD_PINNED: page-lock the octree's host copy so that its loads
+        are DMA copies straight from it."""
+        _check(_L.svo_server_set_upload_policy(self._h, octree, policy), "svo_server_set_upload_policy")
 
     def submit(self, req: svo_request) -> int:
         t = _u64()

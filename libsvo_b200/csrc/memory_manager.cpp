@@ -302,9 +302,17 @@ int TreeletMemoryManagerCuda::init_transfer() {
 // (TreeletMemoryManagerCl.cpp:106-112)
 int TreeletMemoryManagerCuda::upload_all() {
   const uint64_t n = incore_nodes();
-  int rc = stage_copy(d_nodes_, incore_, n * sizeof(svo_node));
-  if (rc == SVO_OK) rc = stage_copy(d_attribs_, incore_attr_, n * sizeof(svo_attrib));
-  if (rc != SVO_OK) return rc;
+  if (mirror_pinned_) {
+    // page-locked mirror: two DMA copies straight from it, no staging
+    SVO_CUDA_TRY(cudaMemcpyAsync(d_nodes_, incore_, n * sizeof(svo_node), cudaMemcpyHostToDevice,
+                                 copy_stream_));
+    SVO_CUDA_TRY(cudaMemcpyAsync(d_attribs_, incore_attr_, n * sizeof(svo_attrib),
+                                 cudaMemcpyHostToDevice, copy_stream_));
+  } else {
+    int rc = stage_copy(d_nodes_, incore_, n * sizeof(svo_node));
+    if (rc == SVO_OK) rc = stage_copy(d_attribs_, incore_attr_, n * sizeof(svo_attrib));
+    if (rc != SVO_OK) return rc;
+  }
   SVO_CUDA_TRY(cudaEventRecord(upload_done_, copy_stream_));
   upload_pending_ = true;
   upload_.clear();
@@ -400,11 +408,10 @@ int TreeletMemoryManagerCuda::set_upload_policy(int policy) {
   return SVO_OK;
 }
 
-// With the mirror page-locked, the gather kernel reads it directly: a
-// host-side change waits for the gather still in flight.
+// With the mirror page-locked, the gather kernel and whole-pool uploads read
+// it directly: a host-side change waits for the copies still in flight.
 void TreeletMemoryManagerCuda::before_host_write() {
-  if (upload_policy_ == SVO_UPLOAD_PINNED && upload_pending_ && copy_stream_)
-    cudaStreamSynchronize(copy_stream_);
+  if (mirror_pinned_ && upload_pending_ && copy_stream_) cudaStreamSynchronize(copy_stream_);
 }
 
 // Dirty slots packed back to back into a ring half ({nodes, attributes} per

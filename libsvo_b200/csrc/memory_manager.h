@@ -121,7 +121,9 @@ class TreeletMemoryManagerCuda : public TreeletMemoryManager {
   // packed back to back into the pinned ring, one host-to-device copy per
   // 4 MB chunk, and a scatter kernel that moves each slot to its place.
   // SVO_UPLOAD_PINNED: the mirror itself is page-locked and mapped; one
-  // kernel reads the dirty slots from it over PCIe and writes them in place.
+  // kernel reads the dirty slots from it over PCIe and writes them in place,
+  // and whole-pool uploads (init_device_buffer, attach_device_buffers) are
+  // two DMA copies straight from it.
   int set_upload_policy(int policy);
   int upload_policy() const { return upload_policy_; }
   int reset_incore_buffer() override;

@@ -517,6 +517,17 @@ int svo_server_add_octree(svo_server* s, const svo_scene* scene, int32_t stack_s
   return SVO_OK;
 }
 
+int svo_server_set_upload_policy(svo_server* s, uint32_t octree, int32_t policy) {
+  if (!s) return SVO_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (octree >= s->octrees.size()) return SVO_ERR_INVALID;
+  try {
+    return s->octrees[octree].mm->set_upload_policy(policy);
+  } catch (const std::bad_alloc&) {
+    return SVO_ERR_NOMEM;
+  }
+}
+
 int svo_server_submit(svo_server* s, const svo_request* req, uint64_t* ticket) {
   const double submitted = s ? s->now() : 0.0;  // before waiting for the lock
   if (!s || !req || !ticket || !req->d_rgba) return SVO_ERR_INVALID;

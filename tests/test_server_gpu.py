@@ -40,8 +40,10 @@ def footprint(scene):
     return 16 * i.treelet_bytes // 8 * i.num_treelets
 
 
-@pytest.mark.parametrize("mode", [L.SERVE_BATCHED, L.SERVE_PLAIN])
-def test_results_same_alone_and_in_the_mix(workload, cuda, mode):
+@pytest.mark.parametrize("mode,upload", [(L.SERVE_BATCHED, None), (L.SERVE_PLAIN, None),
+                                         (L.SERVE_BATCHED, L.UPLOAD_PINNED)])
+def test_results_same_alone_and_in_the_mix(workload, cuda, mode, upload):
+    """upload: octree loads as DMA copies from page-locked host copies."""
     import torch
 
     reqs = S.serving_requests(40, len(workload.scenes), seed=5, max_wh=(320, 200))
@@ -49,6 +51,9 @@ def test_results_same_alone_and_in_the_mix(workload, cuda, mode):
     budget = int(1.1 * (footprint(workload.scenes[2]) + footprint(workload.scenes[3])))
     srv = L.Server(L.server_cfg(budget, streams=3, max_batch_views=8, mode=mode))
     ids = [srv.add_octree(s) for s in workload.scenes]
+    if upload is not None:
+        for i in ids:
+            srv.set_upload_policy(i, upload)
     outs, rq = [], []
     for o, cam in reqs:
         p = cam.frame_params()

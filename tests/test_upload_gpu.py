@@ -67,3 +67,25 @@ def test_device_pool_follows_host_mirror(cuda, policy, ratio):
         assert np.array_equal(dn, hn), f"cycle {cycle}: node pool differs"
         assert np.array_equal(da, ha), f"cycle {cycle}: attribute pool differs"
     mm.close()
+
+
+@pytest.mark.parametrize("policy", [L.UPLOAD_COALESCED, L.UPLOAD_PINNED])
+def test_whole_pool_upload(cuda, policy):
+    """initDeviceBuffer after insertAll: the whole pool in one upload (staged
+    through the ring, or two DMA copies straight from the page-locked
+    mirror), then host writes that must wait for that upload."""
+    scene = L.Scene.menger(level=4, depth=7, seed=6, treelet_levels=2)
+    mm = L.TreeletMemoryManagerCuda(scene, scene.info.treelet_bytes * scene.info.num_treelets)
+    mm.setUploadPolicy(policy)
+    mm.insertAll()
+    mm.initDeviceBuffer()
+    hn, ha = mm.getIncoreBuffer()
+    dn, da = device_pool(mm)
+    assert np.array_equal(dn, hn) and np.array_equal(da, ha)
+    mm.resetIncoreBuffer()  # rewrites the mirror right after the upload was issued
+    mm.insertAll()
+    mm.updateDeviceMemory()
+    hn2, ha2 = mm.getIncoreBuffer()
+    dn, da = device_pool(mm)
+    assert np.array_equal(dn, hn2) and np.array_equal(da, ha2)
+    mm.close()
