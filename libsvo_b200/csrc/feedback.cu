@@ -25,12 +25,12 @@ constexpr int kThreads = kBlockW * kBlockH;
 
 __global__ void __launch_bounds__(kThreads) feedback_kernel(
     const uint2* __restrict__ nodes, uint64_t num_nodes, const svo_frame_params p, int S,
-    svo_feedback* __restrict__ out, uint32_t* __restrict__ rgba) {
+    svo_feedback* __restrict__ out, uint32_t* __restrict__ rgba, uint32_t y0) {
   extern __shared__ uint2 stack_smem[];
   const int t = threadIdx.x;
   const int warp = t >> 5, lane = t & 31;
   const uint32_t x = blockIdx.x * kBlockW + (warp & 1) * 8 + (lane & 7);
-  const uint32_t y = blockIdx.y * kBlockH + (warp >> 1) * 4 + (lane >> 3);
+  const uint32_t y = y0 + blockIdx.y * kBlockH + (warp >> 1) * 4 + (lane >> 3);
   if (x >= p.width || y >= p.height) return;
   float o[3], dx, dy, dz;
   pixel_ray(p, x, y, o, dx, dy, dz);
@@ -62,11 +62,17 @@ __global__ void __launch_bounds__(kThreads) feedback_kernel(
 int launch_feedback(const svo_node* nodes, uint64_t num_nodes, const svo_frame_params& p, int S,
                     svo_feedback* out, uint32_t* rgba, cudaStream_t stream) {
   if (p.width == 0 || p.height == 0) return SVO_OK;
-  const dim3 grid((p.width + kBlockW - 1) / kBlockW, (p.height + kBlockH - 1) / kBlockH);
+  if (p.height > 0xFFFFFFF0u) return SVO_ERR_RANGE;  // row indices stay below 2^32
   const size_t smem = (size_t)S * kThreads * sizeof(uint2);
-  feedback_kernel<<<grid, kThreads, smem, stream>>>(reinterpret_cast<const uint2*>(nodes), num_nodes,
-                                                     p, S, out, rgba);
-  return cudaGetLastError() == cudaSuccess ? SVO_OK : SVO_ERR_CUDA;
+  constexpr uint32_t kRowsPerLaunch = 65535u * kBlockH;  // grid rows are at most 65535
+  for (uint32_t y0 = 0; y0 < p.height; y0 += kRowsPerLaunch) {
+    const uint32_t rows = p.height - y0 < kRowsPerLaunch ? p.height - y0 : kRowsPerLaunch;
+    const dim3 grid((p.width + kBlockW - 1) / kBlockW, (rows + kBlockH - 1) / kBlockH);
+    feedback_kernel<<<grid, kThreads, smem, stream>>>(reinterpret_cast<const uint2*>(nodes),
+                                                       num_nodes, p, S, out, rgba, y0);
+    if (cudaGetLastError() != cudaSuccess) return SVO_ERR_CUDA;
+  }
+  return SVO_OK;
 }
 
 }  // namespace svo

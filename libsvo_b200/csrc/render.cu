@@ -27,13 +27,14 @@ template <bool kFlat, bool kExt>
 __global__ void __launch_bounds__(kThreads) render_frame_kernel(
     const uint2* __restrict__ nodes, const uint2* __restrict__ attribs, uint64_t num_nodes,
     const svo_frame_params p, int S, uint32_t* __restrict__ rgba, svo_hit* __restrict__ hits,
-    svo_stats* __restrict__ stats) {
+    svo_stats* __restrict__ stats, uint32_t y0) {
   extern __shared__ uint2 stack_smem[];
   const int t = threadIdx.x;
   const int warp = t >> 5, lane = t & 31;
-  // warp w covers pixels [8*(w&1), +8) x [4*(w>>1), +4) of the 16x16 block
+  // warp w covers pixels [8*(w&1), +8) x [4*(w>>1), +4) of the 16x8 block;
+  // rows start at y0 (frames taller than one grid's rows take several launches)
   const uint32_t x = blockIdx.x * kBlockW + (warp % (kBlockW / 8)) * 8 + (lane & 7);
-  const uint32_t y = blockIdx.y * kBlockH + (warp / (kBlockW / 8)) * 4 + (lane >> 3);
+  const uint32_t y = y0 + blockIdx.y * kBlockH + (warp / (kBlockW / 8)) * 4 + (lane >> 3);
   if (x >= p.width || y >= p.height) return;
   float o[3], dx, dy, dz;
   pixel_ray(p, x, y, o, dx, dy, dz);
@@ -58,12 +59,12 @@ __global__ void __launch_bounds__(kThreads) render_shadow_kernel(
     const uint2* __restrict__ nodes, const uint2* __restrict__ attribs, uint64_t num_nodes,
     const svo_frame_params p, const svo_shadow_cfg sc, int S, uint32_t* __restrict__ rgba,
     svo_hit* __restrict__ hits, svo_hit* __restrict__ shadow_hits,
-    svo_stats* __restrict__ stats) {
+    svo_stats* __restrict__ stats, uint32_t y0) {
   extern __shared__ uint2 stack_smem[];
   const int t = threadIdx.x;
   const int warp = t >> 5, lane = t & 31;
   const uint32_t x = blockIdx.x * kBlockW + (warp % (kBlockW / 8)) * 8 + (lane & 7);
-  const uint32_t y = blockIdx.y * kBlockH + (warp / (kBlockW / 8)) * 4 + (lane >> 3);
+  const uint32_t y = y0 + blockIdx.y * kBlockH + (warp / (kBlockW / 8)) * 4 + (lane >> 3);
   if (x >= p.width || y >= p.height) return;
   float o[3], dx, dy, dz;
   pixel_ray(p, x, y, o, dx, dy, dz);
@@ -122,32 +123,29 @@ __global__ void __launch_bounds__(kThreads) trace_rays_kernel(
 
 size_t render_smem_bytes(int S) { return (size_t)S * kThreads * sizeof(uint2); }
 
+// Rows of one launch: a grid has at most 65535 blocks along y.
+constexpr uint32_t kRowsPerLaunch = 65535u * kBlockH;
+
 int launch_render(const svo_node* nodes, const svo_attrib* attribs, uint64_t num_nodes,
                   const svo_frame_params& p, const svo_trace_cfg& cfg, uint32_t* rgba,
                   svo_hit* hits, svo_stats* stats, cudaStream_t stream) {
   if (p.width == 0 || p.height == 0) return SVO_OK;
-  const dim3 grid((p.width + kBlockW - 1) / kBlockW, (p.height + kBlockH - 1) / kBlockH);
+  if (p.height > 0xFFFFFFF0u) return SVO_ERR_RANGE;  // row indices stay below 2^32
   const int S = cfg.stack_size;
   const size_t smem = render_smem_bytes(S);
   const uint2* n2 = reinterpret_cast<const uint2*>(nodes);
   const uint2* a2 = reinterpret_cast<const uint2*>(attribs);
   const bool ext = p.mode == 2 || p.mode == 6 || p.mode == 7;
-  if (cfg.traversal == SVO_TRAVERSAL_FLAT) {
-    if (ext)
-      render_frame_kernel<true, true><<<grid, kThreads, smem, stream>>>(n2, a2, num_nodes, p, S,
-                                                                        rgba, hits, stats);
-    else
-      render_frame_kernel<true, false><<<grid, kThreads, smem, stream>>>(n2, a2, num_nodes, p, S,
-                                                                         rgba, hits, stats);
-  } else {
-    if (ext)
-      render_frame_kernel<false, true><<<grid, kThreads, smem, stream>>>(n2, a2, num_nodes, p, S,
-                                                                         rgba, hits, stats);
-    else
-      render_frame_kernel<false, false><<<grid, kThreads, smem, stream>>>(n2, a2, num_nodes, p, S,
-                                                                          rgba, hits, stats);
+  const bool flat = cfg.traversal == SVO_TRAVERSAL_FLAT;
+  auto* fn = flat ? (ext ? render_frame_kernel<true, true> : render_frame_kernel<true, false>)
+                  : (ext ? render_frame_kernel<false, true> : render_frame_kernel<false, false>);
+  for (uint32_t y0 = 0; y0 < p.height; y0 += kRowsPerLaunch) {
+    const uint32_t rows = p.height - y0 < kRowsPerLaunch ? p.height - y0 : kRowsPerLaunch;
+    const dim3 grid((p.width + kBlockW - 1) / kBlockW, (rows + kBlockH - 1) / kBlockH);
+    fn<<<grid, kThreads, smem, stream>>>(n2, a2, num_nodes, p, S, rgba, hits, stats, y0);
+    if (cudaGetLastError() != cudaSuccess) return SVO_ERR_CUDA;
   }
-  return cudaGetLastError() == cudaSuccess ? SVO_OK : SVO_ERR_CUDA;
+  return SVO_OK;
 }
 
 int launch_render_shadow(const svo_node* nodes, const svo_attrib* attribs, uint64_t num_nodes,
@@ -155,11 +153,16 @@ int launch_render_shadow(const svo_node* nodes, const svo_attrib* attribs, uint6
                          uint32_t* rgba, svo_hit* hits, svo_hit* shadow_hits, svo_stats* stats,
                          cudaStream_t stream) {
   if (p.width == 0 || p.height == 0) return SVO_OK;
-  const dim3 grid((p.width + kBlockW - 1) / kBlockW, (p.height + kBlockH - 1) / kBlockH);
-  render_shadow_kernel<<<grid, kThreads, render_smem_bytes(S), stream>>>(
-      reinterpret_cast<const uint2*>(nodes), reinterpret_cast<const uint2*>(attribs), num_nodes, p,
-      sc, S, rgba, hits, shadow_hits, stats);
-  return cudaGetLastError() == cudaSuccess ? SVO_OK : SVO_ERR_CUDA;
+  if (p.height > 0xFFFFFFF0u) return SVO_ERR_RANGE;  // row indices stay below 2^32
+  for (uint32_t y0 = 0; y0 < p.height; y0 += kRowsPerLaunch) {
+    const uint32_t rows = p.height - y0 < kRowsPerLaunch ? p.height - y0 : kRowsPerLaunch;
+    const dim3 grid((p.width + kBlockW - 1) / kBlockW, (rows + kBlockH - 1) / kBlockH);
+    render_shadow_kernel<<<grid, kThreads, render_smem_bytes(S), stream>>>(
+        reinterpret_cast<const uint2*>(nodes), reinterpret_cast<const uint2*>(attribs), num_nodes,
+        p, sc, S, rgba, hits, shadow_hits, stats, y0);
+    if (cudaGetLastError() != cudaSuccess) return SVO_ERR_CUDA;
+  }
+  return SVO_OK;
 }
 
 int launch_trace_rays(const svo_node* nodes, uint64_t num_nodes, const float* origins,

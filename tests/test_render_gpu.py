@@ -93,6 +93,33 @@ def test_ragged_frame_sizes(menger_mm, w, h):
     assert np.array_equal(rgba, o_rgba)
 
 
+def test_frame_taller_than_one_grid(menger_mm, cuda):
+    """600,001 rows: more than one launch's 65,535 block rows of 8 pixels;
+    the per-frame, shadow and feedback kernels each cover it in several
+    launches."""
+    torch = _torch()
+    p = L.orbit_camera(7, 3, 600001, radius=1.6, fov_deg=80.0).frame_params()
+    rgba, hits = gpu_frame(menger_mm, p)
+    nodes, attribs = menger_mm.getIncoreBuffer()
+    o_rgba, o_hits, _, _ = oracle.render(nodes, attribs, bytes(p))
+    assert_hits_equal(hits, o_hits, "render")
+    assert np.array_equal(rgba, o_rgba)
+    assert o_hits["hit"].sum() > 1000
+    d_nodes, d_attribs, n = menger_mm.getDeviceIncoreBuffer()
+    light = L.seeded_light(3)
+    img = torch.empty((p.height, p.width), dtype=torch.int32, device=cuda)
+    sh = torch.empty(p.width * p.height * 16, dtype=torch.uint8, device=cuda)
+    L.render_shadow(d_nodes, d_attribs, n, p, img, L.shadow_cfg(light), None, sh)
+    fb = torch.empty(p.width * p.height * 16, dtype=torch.uint8, device=cuda)
+    L.feedback_render(d_nodes, n, p, fb)
+    torch.cuda.synchronize()
+    s_rgba, _, s_sh, _, _ = oracle.render_shadow(nodes, attribs, bytes(p), light)
+    assert np.array_equal(img.cpu().numpy().view(np.uint32), s_rgba)
+    assert_hits_equal(_hits_np(sh), s_sh.reshape(-1), "shadow rays")
+    rec, _ = oracle.feedback(nodes, bytes(p))
+    assert np.array_equal(fb.cpu().numpy(), rec.view(np.uint8).reshape(-1))
+
+
 def test_flat_traversal_matches_oracle(menger_scene, cuda):
     torch = _torch()
     nodes, attribs = menger_scene.flatten()
