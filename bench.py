@@ -48,11 +48,12 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the batched, served, large-shadowed and incore-update measurements")
-    ap.add_argument("--leg", choices=["batched", "served", "large_shadowed", "incore_update", "streaming"],
+    ap.add_argument("--leg", choices=["batched", "served", "large_shadowed", "incore_update", "streaming", "flat"],
                     help="run only this measurement on one GPU and print its result: the 64 terrain "
                          "views as one batched launch, the request server, the large shadowed "
-                         "frame, the incore-update policies or the streaming loop on the icosphere "
-                         "scene (--steps sets the timed repetitions of batched and large_shadowed)")
+                         "frame, the incore-update policies, the streaming loop on the icosphere "
+                         "scene, or the flat (CpuRaycasterSingleRay3) traversal of the main view "
+                         "(--steps sets the timed repetitions of batched and large_shadowed)")
     ap.add_argument("--large-only", action="store_true",
                     help="run only the large shadowed measurement (icosphere built on the GPU, 3840x2160 "
                          "primary + shadow frame) and print its result; the same as --leg large_shadowed")
@@ -515,6 +516,76 @@ def host_memory_available() -> int:
     return avail
 
 
+def flat_leg(dev, reps=50, workload="icosphere", seconds=10.0, cpu_baseline=True):
+    """The CpuRaycasterSingleRay3 traversal (flat breadth-first pool with
+    absolute first-child indices, stack = the octree's depth, LOD by tcMax)
+    over the same scene and view as the main step: the pool flattened on the
+    host and uploaded, the frame timed with CUDA events (L2 flushed between
+    frames); the CPU figure is the oracle's restatement of traversSvo (the
+    reference's CPU raycaster does not build without its gloost
+    dependency)."""
+    import torch
+
+    import libsvo_b200 as L
+    import oracle
+
+    wl = make_workload(workload)
+    depth = int(wl.scene.info.max_depth)
+    nodes, attribs = wl.scene.flatten()
+    dn = torch.from_numpy(nodes.view(np.int32)).to(dev)
+    da = torch.from_numpy(attribs.view(np.int32)).to(dev)
+    cfg = L.trace_cfg(L.TRAVERSAL_FLAT, depth)
+    params = [c.frame_params() for c in wl.cameras]
+    outs = [torch.empty((p.height, p.width), dtype=torch.int32, device=dev) for p in params]
+    s = torch.cuda.current_stream()
+    fetches = hits = 0
+    for p, o in zip(params, outs):
+        hb = torch.empty(p.width * p.height * 16, dtype=torch.uint8, device=dev)
+        L.render(dn, da, nodes.shape[0], p, o, hb, cfg=cfg, stream=s)
+        h = hb.cpu().numpy().view(L.HIT_DTYPE)
+        fetches += int(h["fetches"].astype(np.int64).sum())
+        hits += int(h["hit"].astype(np.int64).sum())
+    rays = wl.rays_per_step
+    algo_bytes = 8 * fetches + 8 * hits + 4 * rays
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(reps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(reps)]
+    for _ in range(3):
+        for p, o in zip(params, outs):
+            L.render(dn, da, nodes.shape[0], p, o, cfg=cfg, stream=s)
+    for i in range(reps):
+        flush.fill_(i)
+        starts[i].record(s)
+        for p, o in zip(params, outs):
+            L.render(dn, da, nodes.shape[0], p, o, cfg=cfg, stream=s)
+        ends[i].record(s)
+    torch.cuda.synchronize()
+    ms = statistics.mean(a.elapsed_time(b) for a, b in zip(starts, ends))
+    peak, _ = load_peaks()
+    out = {"workload": wl.name + "_flat", "traversal": f"flat (CpuRaycasterSingleRay3), stack {depth}",
+           "pool_nodes": int(nodes.shape[0]), "rays_per_step": rays, "ms_per_step": ms,
+           "mrays_s": rays / ms / 1e3,
+           "roofline": {"algorithmic_bytes_per_step": algo_bytes, "achieved_gbs": algo_bytes / ms / 1e6,
+                        "frac": algo_bytes / ms / 1e6 / peak, "node_reads_per_ray": fetches / rays}}
+    del flush
+    if cpu_baseline:
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        frames = cast = 0
+        while True:
+            for p in params:
+                oracle.render(nodes, attribs, bytes(p), flat=True, stack_size=depth, threads=threads)
+                cast += p.width * p.height
+            frames += 1
+            el = time.perf_counter() - t0
+            if el >= seconds or frames >= 200:
+                break
+        out["cpu_baseline"] = {"value": cast / el / 1e6, "unit": METRIC, "cores": threads, "kind": "port",
+                               "sample": f"{frames} whole frame(s) ({cast} rays) in {el:.1f} s; the oracle's "
+                                         "restatement of CpuRaycasterSingleRay3::traversSvo"}
+    return out
+
+
 def large_cpu_baseline(wl, n, seconds=10.0):
     """The reference's shadow frame compiled for the host over the large
     pool: the pool is copied to host memory (16 bytes per node), then whole
@@ -636,7 +707,8 @@ def main():
                                                            depth=args.large_depth,
                                                            cpu_baseline=not args.no_cpu_baseline),
                 "incore_update": lambda: incore_update_leg(dev, make_workload("icosphere").scene),
-                "streaming": lambda: streaming_leg(dev, make_workload("icosphere").scene)}
+                "streaming": lambda: streaming_leg(dev, make_workload("icosphere").scene),
+                "flat": lambda: flat_leg(dev, cpu_baseline=not args.no_cpu_baseline)}
         print(json.dumps({"leg": args.leg, **legs[args.leg]()}), flush=True)
         return
     if world > 1:
@@ -800,7 +872,8 @@ def main():
                 except Exception as e:  # a failing extra leg must not lose the primary line
                     line[key] = {"error": f"{type(e).__name__}: {e}"}
         if world == 1 and not args.no_extra:
-            legs = (("batched", batched_leg), ("served", served_leg),
+            legs = (("flat", lambda d: flat_leg(d, cpu_baseline=not args.no_cpu_baseline)),
+                    ("batched", batched_leg), ("served", served_leg),
                     ("large_shadowed", lambda d: large_shadow_leg(d, cpu_baseline=not args.no_cpu_baseline)))
             for key, leg in legs:
                 try:
