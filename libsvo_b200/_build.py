@@ -5,6 +5,12 @@ C++ host sources go through g++, CUDA sources through nvcc for sm_100a only
 (``-fmad=false``; the kernels also use explicit round-to-nearest intrinsics),
 and the shared object links the CUDA runtime statically.  The build needs no
 GPU: nvcc cross-compiles.
+
+``build_sanitized()`` (``--sanitize``) builds a second library,
+``_lib/libsvo_b200_asan.so``, whose host code is compiled with
+AddressSanitizer and UndefinedBehaviorSanitizer (the CUDA objects are the
+regular ones); load it with the sanitizer runtimes preloaded
+(``SANITIZER_PRELOAD``) and ``LIBSVO_B200_LIB`` pointing at it.
 """
 from __future__ import annotations
 
@@ -84,5 +90,59 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     return LIB
 
 
+SAN_DIR = OBJ_DIR / "asan"
+SAN_LIB = LIB_DIR / "libsvo_b200_asan.so"
+SAN_FLAGS = ["-fsanitize=address,undefined", "-fno-omit-frame-pointer", "-fno-sanitize-recover=undefined"]
+
+
+def sanitizer_preload() -> str:
+    """The sanitizer runtimes a host process must preload to load SAN_LIB."""
+    libs = []
+    for name in ("libasan.so", "libubsan.so"):
+        r = subprocess.run(["g++", f"-print-file-name={name}"], capture_output=True, text=True, check=True)
+        libs.append(r.stdout.strip())
+    return " ".join(libs)
+
+
+def build_sanitized(verbose: bool = False) -> Path:
+    """The library with AddressSanitizer/UBSan-instrumented host code."""
+    build(verbose=verbose)  # the CUDA objects
+    SAN_DIR.mkdir(parents=True, exist_ok=True)
+    newest = max((h.stat().st_mtime for h in _headers()), default=0.0)
+    jobs, objs = [], []
+    for src in sorted(CSRC.glob("*.cpp")):
+        obj = SAN_DIR / (src.name + ".o")
+        objs.append(obj)
+        if _stale(obj, src, newest):
+            jobs.append((src, obj))
+
+    def compile_one(job):
+        src, obj = job
+        cmd = ["g++", *CXX_FLAGS, "-O1", "-g", *SAN_FLAGS, "-c", str(src), "-o", str(obj)]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"compile failed: {src.name}\n{r.stdout}\n{r.stderr}")
+
+    if jobs:
+        with ThreadPoolExecutor(max_workers=min(8, len(jobs))) as ex:
+            list(ex.map(compile_one, jobs))
+    cu_objs = [OBJ_DIR / (src.name + ".o") for src in sorted(CSRC.glob("*.cu"))]
+    inputs = objs + cu_objs
+    if jobs or not SAN_LIB.is_file() or any(o.stat().st_mtime > SAN_LIB.stat().st_mtime for o in inputs):
+        cmd = ["g++", "-shared", *SAN_FLAGS, "-o", str(SAN_LIB), *map(str, inputs),
+               f"-L{CUDA_HOME / 'lib64'}", "-lcudart_static", "-lrt", "-ldl", "-pthread"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed\n{r.stdout}\n{r.stderr}")
+    return SAN_LIB
+
+
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))
+    if "--sanitize" in sys.argv:
+        print(build_sanitized(verbose="-v" in sys.argv))
+    else:
+        print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))
