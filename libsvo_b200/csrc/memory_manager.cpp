@@ -5,6 +5,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <deque>
+#include <thread>
 
 #include "analysis.h"
 #include "errors.h"
@@ -309,8 +310,8 @@ int TreeletMemoryManagerCuda::upload_all() {
     SVO_CUDA_TRY(cudaMemcpyAsync(d_attribs_, incore_attr_, n * sizeof(svo_attrib),
                                  cudaMemcpyHostToDevice, copy_stream_));
   } else {
-    int rc = stage_copy(d_nodes_, incore_, n * sizeof(svo_node));
-    if (rc == SVO_OK) rc = stage_copy(d_attribs_, incore_attr_, n * sizeof(svo_attrib));
+    const int rc = stage_copies({{d_nodes_, incore_, n * sizeof(svo_node)},
+                                 {d_attribs_, incore_attr_, n * sizeof(svo_attrib)}});
     if (rc != SVO_OK) return rc;
   }
   SVO_CUDA_TRY(cudaEventRecord(upload_done_, copy_stream_));
@@ -359,20 +360,69 @@ int TreeletMemoryManagerCuda::detach_device_buffers() {
   return SVO_OK;
 }
 
-int TreeletMemoryManagerCuda::stage_copy(void* dst, const void* src, uint64_t bytes) {
-  const char* s = (const char*)src;
-  char* d = (char*)dst;
-  while (bytes) {
-    const uint64_t n = std::min(bytes, kStageBytes);
-    const int h = stage_next_;
-    stage_next_ ^= 1;
-    SVO_CUDA_TRY(cudaEventSynchronize(stage_evt_[h]));
-    std::memcpy(stage_[h], s, (size_t)n);
-    SVO_CUDA_TRY(cudaMemcpyAsync(d, stage_[h], n, cudaMemcpyHostToDevice, copy_stream_));
-    SVO_CUDA_TRY(cudaEventRecord(stage_evt_[h], copy_stream_));
-    s += n;
-    d += n;
-    bytes -= n;
+namespace {
+
+struct HostPiece {
+  char* dst;
+  const char* src;
+  uint64_t bytes;
+};
+
+// Host-to-host copies of `pieces` (`total` bytes) on up to 8 threads, each
+// taking an equal span of the concatenated bytes; serial below 4 MB or when
+// no thread can be started.
+void copy_pieces(const std::vector<HostPiece>& pieces, uint64_t total) {
+  auto span = [&](uint64_t lo, uint64_t hi) {
+    uint64_t off = 0;
+    for (const HostPiece& p : pieces) {
+      const uint64_t a = std::max(lo, off), b = std::min(hi, off + p.bytes);
+      if (a < b) std::memcpy(p.dst + (a - off), p.src + (a - off), (size_t)(b - a));
+      off += p.bytes;
+      if (off >= hi) break;
+    }
+  };
+  static const uint64_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const uint64_t parts = std::min<uint64_t>(std::min<uint64_t>(8, hw), total / (1ull << 20));
+  if (parts <= 1 || total < (4ull << 20)) {
+    span(0, total);
+    return;
+  }
+  std::vector<std::thread> workers;
+  uint64_t started = 1;  // span 0 runs on this thread
+  try {
+    for (; started < parts; ++started)
+      workers.emplace_back(span, total * started / parts, total * (started + 1) / parts);
+  } catch (...) {  // no more threads: the rest runs here
+  }
+  span(0, total / parts);
+  if (started < parts) span(total * started / parts, total);
+  for (std::thread& w : workers) w.join();
+}
+
+}  // namespace
+
+int TreeletMemoryManagerCuda::stage_copies(const std::vector<StagedCopy>& copies) {
+  for (const StagedCopy& c : copies) {
+    char* d = (char*)c.dst;
+    const char* s = (const char*)c.src;
+    uint64_t bytes = c.bytes;
+    while (bytes) {
+      const uint64_t n = std::min(bytes, kStageBytes);
+      const int h = stage_next_;
+      stage_next_ ^= 1;
+      SVO_CUDA_TRY(cudaEventSynchronize(stage_evt_[h]));
+      // small pieces land at the start of a half, which stays in the host's
+      // caches; large ones are copied into it on several threads
+      if (n >= (4ull << 20))
+        copy_pieces({HostPiece{(char*)stage_[h], s, n}}, n);
+      else
+        std::memcpy(stage_[h], s, (size_t)n);
+      SVO_CUDA_TRY(cudaMemcpyAsync(d, stage_[h], n, cudaMemcpyHostToDevice, copy_stream_));
+      SVO_CUDA_TRY(cudaEventRecord(stage_evt_[h], copy_stream_));
+      s += n;
+      d += n;
+      bytes -= n;
+    }
   }
   return SVO_OK;
 }
@@ -487,13 +537,16 @@ int TreeletMemoryManagerCuda::update_device_memory(uint32_t* copy_calls) {
     return SVO_OK;
   }
   const auto ranges = upload_ranges();
+  std::vector<StagedCopy> copies;
+  copies.reserve(2 * ranges.size());
   for (const auto& r : ranges) {
     const uint64_t first = (uint64_t)r.first * N_;
     const uint64_t count = (uint64_t)r.second * N_;
-    int rc = stage_copy(d_nodes_ + first, incore_ + first, count * sizeof(svo_node));
-    if (rc == SVO_OK) rc = stage_copy(d_attribs_ + first, incore_attr_ + first, count * sizeof(svo_attrib));
-    if (rc != SVO_OK) return rc;
+    copies.push_back({d_nodes_ + first, incore_ + first, count * sizeof(svo_node)});
+    copies.push_back({d_attribs_ + first, incore_attr_ + first, count * sizeof(svo_attrib)});
   }
+  const int rc = stage_copies(copies);
+  if (rc != SVO_OK) return rc;
   SVO_CUDA_TRY(cudaEventRecord(upload_done_, copy_stream_));
   upload_pending_ = true;
   if (copy_calls) *copy_calls = (uint32_t)ranges.size();

@@ -160,7 +160,17 @@ class TreeletMemoryManagerCuda : public TreeletMemoryManager {
 
  private:
   int init_analysis();
-  int stage_copy(void* dst, const void* src, uint64_t bytes);
+  // One host-to-device copy through the pinned ring.
+  struct StagedCopy {
+    void* dst;
+    const void* src;
+    uint64_t bytes;
+  };
+  // The copies, in order, through the pinned ring, in pieces of at most one
+  // half: each piece waits for its half's previous copy, is copied into it
+  // (on several host threads from 4 MB up) and goes out with one
+  // cudaMemcpyAsync, so its transfer overlaps the host copy of the next.
+  int stage_copies(const std::vector<StagedCopy>& copies);
   int upload_packed(uint32_t* copy_calls);
   void before_host_write() override;
   int init_transfer();
