@@ -19,8 +19,11 @@ namespace svo {
 
 namespace {
 
-constexpr int kBlockW = 16;
-constexpr int kBlockH = 16;
+// One warp (8x4 pixels) per block: analysis buffers are small (128x128 for
+// a 1024x1024 frame at the reference's divisor 8), and one-warp blocks
+// spread their few rays over all SMs.
+constexpr int kBlockW = 8;
+constexpr int kBlockH = 4;
 constexpr int kThreads = kBlockW * kBlockH;
 
 __global__ void __launch_bounds__(kThreads) feedback_kernel(
@@ -29,8 +32,8 @@ __global__ void __launch_bounds__(kThreads) feedback_kernel(
   extern __shared__ uint2 stack_smem[];
   const int t = threadIdx.x;
   const int warp = t >> 5, lane = t & 31;
-  const uint32_t x = blockIdx.x * kBlockW + (warp & 1) * 8 + (lane & 7);
-  const uint32_t y = y0 + blockIdx.y * kBlockH + (warp >> 1) * 4 + (lane >> 3);
+  const uint32_t x = blockIdx.x * kBlockW + (warp % (kBlockW / 8)) * 8 + (lane & 7);
+  const uint32_t y = y0 + blockIdx.y * kBlockH + (warp / (kBlockW / 8)) * 4 + (lane >> 3);
   if (x >= p.width || y >= p.height) return;
   float o[3], dx, dy, dz;
   pixel_ray(p, x, y, o, dx, dy, dz);
