@@ -180,8 +180,10 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
         tmin = tmax;
         node = e.x;
         tmax = __uint_as_float(e.y);
-        in_pool = (uint64_t)node < num_nodes;
-        if (in_pool) nd = fetch(node);
+        // a stacked node passed the in-pool test before its children were
+        // tested, so the popped one is in the pool
+        in_pool = true;
+        nd = fetch(node);
         // parent centre = child centre -+ the child's sx2 (exact)
         cx = __fadd_rn(cx, (ix & 1u) ? -sx2 : sx2);
         cy = __fadd_rn(cy, (iy & 1u) ? -sx2 : sx2);
@@ -189,8 +191,8 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
         ix >>= 1;
         iy >>= 1;
         iz >>= 1;
+        half = sx2;  // the parent's half child size is the child's size (exact)
         sx2 = __fmul_rn(sx2, 2.0f);
-        half = __fmul_rn(sx2, 0.5f);
       }
       continue;
     }
