@@ -126,9 +126,11 @@ struct StagedFetch {
 // two faces along an axis are the parent's mid plane c and its outer face
 // c +- sx2 (exact dyadic numbers, the values the reference's childCenter +-
 // childSizeHalf produce), so each axis costs the distance to the mid plane,
-// the distance to the outer face and a min and a max that put the near one
-// first.  Rays with an infinite or NaN reciprocal (a direction component of
-// exactly zero) take kSigned = false, the literal compare and swap.
+// the distance to the outer face and the max of the two (the far face); the
+// min (the near face) is taken only for a valid child, the one case that
+// reads tcMin.  Rays with an infinite or NaN reciprocal (a direction
+// component of exactly zero) take kSigned = false, the literal compare and
+// swap.
 template <bool kFlat, bool kSigned, class Fetch>
 __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
                                         const float o[3], float dx, float dy, float dz, float rx,
@@ -147,7 +149,7 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
   uint2 nd = in_pool ? fetch(0u) : make_uint2(0u, 0u);
   uint32_t loops = 0u, fetches = 0u;
 
-  while (scale < S) {
+  for (;;) {  // ends by a return, or by a pop above the root
     ++loops;
     if (loops == max_loops) {
       h.flags = SVO_HITFLAG_CAPPED;
@@ -175,25 +177,24 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
       pop = (tmax < 0.0f) || !(fabsf(__fsub_rn(tmin, tmax)) > eps);
     if (pop) {
       ++scale;
-      if (scale < S) {
-        const uint2 e = stack[(S - 1 - scale) * stride];
-        tmin = tmax;
-        node = e.x;
-        tmax = __uint_as_float(e.y);
-        // a stacked node passed the in-pool test before its children were
-        // tested, so the popped one is in the pool
-        in_pool = true;
-        nd = fetch(node);
-        // parent centre = child centre -+ the child's sx2 (exact)
-        cx = __fadd_rn(cx, (ix & 1u) ? -sx2 : sx2);
-        cy = __fadd_rn(cy, (iy & 1u) ? -sx2 : sx2);
-        cz = __fadd_rn(cz, (iz & 1u) ? -sx2 : sx2);
-        ix >>= 1;
-        iy >>= 1;
-        iz >>= 1;
-        half = sx2;  // the parent's half child size is the child's size (exact)
-        sx2 = __fmul_rn(sx2, 2.0f);
-      }
+      if (scale >= S) break;
+      const uint2 e = stack[(S - 1 - scale) * stride];
+      tmin = tmax;
+      node = e.x;
+      tmax = __uint_as_float(e.y);
+      // a stacked node passed the in-pool test before its children were
+      // tested, so the popped one is in the pool
+      in_pool = true;
+      nd = fetch(node);
+      // parent centre = child centre -+ the child's sx2 (exact)
+      cx = __fadd_rn(cx, (ix & 1u) ? -sx2 : sx2);
+      cy = __fadd_rn(cy, (iy & 1u) ? -sx2 : sx2);
+      cz = __fadd_rn(cz, (iz & 1u) ? -sx2 : sx2);
+      ix >>= 1;
+      iy >>= 1;
+      iz >>= 1;
+      half = sx2;  // the parent's half child size is the child's size (exact)
+      sx2 = __fmul_rn(sx2, 2.0f);
       continue;
     }
     // childEntryPoint = (o + (tMin + eps) d) - centre and its sign test: in
@@ -204,23 +205,21 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
     const bool byp = __fadd_rn(o[1], __fmul_rn(te, dy)) > cy;
     const bool bzp = __fadd_rn(o[2], __fmul_rn(te, dz)) > cz;
     float tx0, tx1, ty0, ty1, tz0, tz1;
+    float mx = 0.0f, my = 0.0f, mz = 0.0f, ox = 0.0f, oy = 0.0f, oz = 0.0f;
     if (kSigned) {
       // The child's faces are the mid plane c and its outer face c +- sx2;
-      // the near one comes first (the mid plane when the child is the far
-      // half along the ray).
-      const float mx = __fadd_rn(__fmul_rn(rx, cx), px);
-      const float my = __fadd_rn(__fmul_rn(ry, cy), py);
-      const float mz = __fadd_rn(__fmul_rn(rz, cz), pz);
-      const float ox = __fadd_rn(__fmul_rn(rx, __fadd_rn(cx, bxp ? sx2 : -sx2)), px);
-      const float oy = __fadd_rn(__fmul_rn(ry, __fadd_rn(cy, byp ? sx2 : -sx2)), py);
-      const float oz = __fadd_rn(__fmul_rn(rz, __fadd_rn(cz, bzp ? sx2 : -sx2)), pz);
-      // the near face is the nearer one: no NaN and no -0 here, so the
-      // hardware min/max give the reference's order bit for bit
-      tx0 = fminf(mx, ox);
+      // the far one is the farther (the near ones, needed only for a valid
+      // child, are taken there).  No NaN and no -0 here, so the hardware
+      // min/max give the reference's order bit for bit.
+      mx = __fadd_rn(__fmul_rn(rx, cx), px);
+      my = __fadd_rn(__fmul_rn(ry, cy), py);
+      mz = __fadd_rn(__fmul_rn(rz, cz), pz);
+      ox = __fadd_rn(__fmul_rn(rx, __fadd_rn(cx, bxp ? sx2 : -sx2)), px);
+      oy = __fadd_rn(__fmul_rn(ry, __fadd_rn(cy, byp ? sx2 : -sx2)), py);
+      oz = __fadd_rn(__fmul_rn(rz, __fadd_rn(cz, bzp ? sx2 : -sx2)), pz);
+      tx0 = ty0 = tz0 = 0.0f;
       tx1 = fmaxf(mx, ox);
-      ty0 = fminf(my, oy);
       ty1 = fmaxf(my, oy);
-      tz0 = fminf(mz, oz);
       tz1 = fmaxf(mz, oz);
     } else {
       // child centre (-0.5 + b) * sx2 + c = c +- half; faces ccx -+ half
@@ -251,8 +250,11 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
     }
     // kSigned: no NaN and no -0 among the distances (see cast_ray), so the
     // hardware min/max equal the reference's max/min bit for bit
-    const float tc_min = kSigned ? fmaxf(tx0, fmaxf(ty0, tz0)) : cl_max(tx0, cl_max(ty0, tz0));
     const float tc_max = kSigned ? fminf(tx1, fminf(ty1, tz1)) : cl_min(tx1, cl_min(ty1, tz1));
+    auto near_max = [&]() {
+      return kSigned ? fmaxf(fminf(mx, ox), fmaxf(fminf(my, oy), fminf(mz, oz)))
+                     : cl_max(tx0, cl_max(ty0, tz0));
+    };
 
     if (!in_pool) {
       h.flags = SVO_HITFLAG_BOUNDS;
@@ -266,6 +268,7 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
     const uint32_t masks = nd.y;
     const uint32_t sh = masks >> ci;  // bit 8: valid, bit 0: leaf
     if (sh & 0x100u) {
+      const float tc_min = near_max();
       const uint32_t below = __popc(masks & ((0x100u << ci) - 0x100u));
       const uint32_t child = (kFlat ? 0u : node) + nd.x + below;
       const bool leaf = sh & 1u;
