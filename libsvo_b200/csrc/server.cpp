@@ -7,8 +7,10 @@
 // at any time; a dispatcher thread admits them against an HBM budget and an
 // in-flight ray budget, pages the treelets of their octrees into one
 // pre-allocated device pool (the octree's TreeletMemoryManagerCuda uploads
-// its slots through its pinned staging ring on its side stream, and the
-// launch waits on the upload event), and launches every admitted request
+// its slots through its pinned staging ring on its side stream -- or, once
+// svo_server_set_upload_policy page-locked its host copy, as two DMA copies
+// straight from it -- and the launch waits on the upload event), and
+// launches every admitted request
 // together as one batch on the next free stream.  Requests that arrive while
 // batches run are launched in further batches on other streams, so their
 // work overlaps on the device (continuous batching).  Octrees no batch uses

@@ -129,8 +129,8 @@ struct StagedFetch {
 // the distance to the outer face and the max of the two (the far face); the
 // min (the near face) is taken only for a valid child, the one case that
 // reads tcMin.  Rays with an infinite or NaN reciprocal (a direction
-// component of exactly zero) take kSigned = false, the literal compare and
-// swap.
+// component of exactly zero) or a -0 origin coordinate (see cast_ray) take
+// kSigned = false, the literal compare and swap.
 template <bool kFlat, bool kSigned, class Fetch>
 __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
                                         const float o[3], float dx, float dy, float dz, float rx,
