@@ -1,13 +1,14 @@
 """Benchmark: primary rays per second of the treelet ray cast on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+                    [--shadow] [--no-extra] [--leg NAME]
 
 One step = one frame of the workload cast over its resident octree.  The
 device-timed ``value`` has the octree resident in HBM and times the render
 kernel with CUDA events (L2 flushed between steps by writing 256 MB).
 ``e2e`` is the same metric through the C ABI call a user makes
-(svo_mm_render_host): kernel plus the copy of the RGBA8 image back to pinned
-host memory, every step.  ``roofline`` relates the kernel's algorithmic bytes
+(svo_mm_render_host_async): kernel plus the copy of the RGBA8 image back to
+pinned host memory, every step, with the L2 flush inside the wall-clock time.  ``roofline`` relates the kernel's algorithmic bytes
 (8 B per parent-node read, 8 B per hit attribute, 4 B per RGBA8 pixel,
 counted by the kernel's own per-ray counters) to the measured HBM copy
 bandwidth.  ``cpu_baseline`` times the reference's own ray cast compiled for
@@ -15,7 +16,10 @@ the host (oracle/_ref; the oracle port when that is absent) on the host cores.
 
 With N > 1 (torchrun), each rank casts the same workload on its own GPU
 (replicas: rays are independent, there is no exchange), and the step time is
-the maximum over ranks.
+the maximum over ranks.  At N = 1 the line also carries the extra legs:
+flat traversal, batched views, serving, the large shadowed frame, incore
+updates and the streaming loop (``--no-extra`` skips them, ``--leg NAME``
+runs one alone).
 """
 from __future__ import annotations
 
