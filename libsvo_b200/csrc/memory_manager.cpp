@@ -672,16 +672,22 @@ int TreeletMemoryManagerCuda::analyse_feedback_device(
   uint32_t* d_new = d_keys_;
   uint32_t* d_old = d_keys_ + (T + 1);
   uint32_t* d_status = d_keys_ + 2 * ((size_t)T + 1);
-  // the page-locked slot table is free: the previous pass waited for its copy
+  // The page-locked slot table is free: every pass, failed ones included,
+  // waits for its copies before it returns.
   for (uint32_t i = 0; i < S; ++i) h_slot_gid_[i] = slots_[i].treelet_gid;
-  SVO_CUDA_TRY(cudaMemcpyAsync(d_slot_gid_, h_slot_gid_, (size_t)S * sizeof(int32_t),
-                               cudaMemcpyHostToDevice, stream));
-  SVO_CUDA_TRY(cudaMemsetAsync(d_keys_, 0, words * sizeof(uint32_t), stream));
-  rc = launch_analyse(d_fb, n, d_slot_gid_, S, N_, d_parent_, T, d_new, d_old, d_status, stream);
+  cudaError_t e = cudaMemcpyAsync(d_slot_gid_, h_slot_gid_, (size_t)S * sizeof(int32_t),
+                                  cudaMemcpyHostToDevice, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_keys_, 0, words * sizeof(uint32_t), stream);
+  if (e == cudaSuccess) {
+    rc = launch_analyse(d_fb, n, d_slot_gid_, S, N_, d_parent_, T, d_new, d_old, d_status, stream);
+    if (rc == SVO_OK)
+      e = cudaMemcpyAsync(h_keys_, d_keys_, words * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                          stream);
+  }
+  const cudaError_t waited = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return cuda_status(e);
   if (rc != SVO_OK) return rc;
-  SVO_CUDA_TRY(cudaMemcpyAsync(h_keys_, d_keys_, words * sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                               stream));
-  SVO_CUDA_TRY(cudaStreamSynchronize(stream));
+  if (waited != cudaSuccess) return cuda_status(waited);
   if (h_keys_[2 * ((size_t)T + 1)] & kAnalyseRejected) return SVO_ERR_RANGE;
   const uint32_t* h_new = h_keys_;
   const uint32_t* h_old = h_keys_ + (T + 1);
