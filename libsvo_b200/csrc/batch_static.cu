@@ -16,6 +16,10 @@
 // keeps the last call's contents: each call rewrites the tables and zeroes
 // the counter before its launch, and calls whose work overlaps on the GPU
 // (other streams or host threads) race on the array.
+//
+// The tables reach the array as the parameter of a small loader kernel
+// (passed by value, so no host memory is read after the call returns), and
+// the batch kernel launched right after it on the same stream reads them.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -41,12 +45,38 @@ static_assert(kViewOffset % 16 == 0, "descriptor alignment");
 // cudaGetSymbolAddress, looked up once per device.
 static __device__ __align__(256) unsigned char g_batch_scratch[kScratchBytes];
 
+// The call's descriptor tables, passed to the loader kernel by value
+// (29,192 bytes, within the 32,764-byte kernel-parameter limit).
+struct StaticTables {
+  BatchOctree octrees[kStaticMaxOctrees];
+  BatchView views[kStaticMaxViews];
+  uint32_t num_octrees;
+  uint32_t num_views;
+};
+static_assert(sizeof(StaticTables) <= 32764, "kernel parameter limit");
+
+// Copies the used part of the tables into the scratch array and zeroes the
+// tile counter; one block.
+__global__ void load_static_tables(const __grid_constant__ StaticTables t, unsigned char* scratch) {
+  const uint32_t* oct = reinterpret_cast<const uint32_t*>(t.octrees);
+  const uint32_t* view = reinterpret_cast<const uint32_t*>(t.views);
+  uint32_t* d_oct = reinterpret_cast<uint32_t*>(scratch + kOctreeOffset);
+  uint32_t* d_view = reinterpret_cast<uint32_t*>(scratch + kViewOffset);
+  const uint32_t oct_words = t.num_octrees * (uint32_t)(sizeof(BatchOctree) / 4);
+  const uint32_t view_words = t.num_views * (uint32_t)(sizeof(BatchView) / 4);
+  for (uint32_t i = threadIdx.x; i < oct_words; i += blockDim.x) d_oct[i] = oct[i];
+  for (uint32_t i = threadIdx.x; i < view_words; i += blockDim.x) d_view[i] = view[i];
+  if (threadIdx.x == 0) *reinterpret_cast<unsigned long long*>(scratch) = 0ull;
+}
+
 constexpr int kMaxDevices = 64;
 void* g_scratch_address[kMaxDevices] = {};
 std::mutex g_scratch_mutex;
 
 // Device address of g_batch_scratch on the current device.  The first call
-// on a device does the lookup with that device current.
+// on a device does the lookup with that device current and keeps it for the
+// life of the process (a cudaDeviceReset would move the array; the library
+// is not used across one).
 int scratch_address(unsigned char** out) {
   int dev = 0;
   SVO_CUDA_TRY(cudaGetDevice(&dev));
@@ -73,9 +103,13 @@ extern "C" int svo_render_batch_static(const svo_octree_desc* octrees, uint32_t 
   if (!octrees || !views || num_views == 0 || num_octrees == 0) return SVO_ERR_INVALID;
   if (num_views > kStaticMaxViews || num_octrees > kStaticMaxOctrees) return SVO_ERR_RANGE;
   if (!batch_tile_supported(tile_w, tile_h)) return SVO_ERR_NOTSUP;
-  // descriptor tables are laid out on the host stack: nothing is allocated
-  BatchView host_views[kStaticMaxViews];
-  BatchOctree host_octrees[kStaticMaxOctrees];
+  // the tables are built in a host-stack struct and handed to the loader
+  // kernel by value: nothing is allocated
+  StaticTables tables;
+  tables.num_octrees = num_octrees;
+  tables.num_views = num_views;
+  BatchView* host_views = tables.views;
+  BatchOctree* host_octrees = tables.octrees;
   const uint64_t tiles = layout_views(views, num_views, num_octrees, tile_w, tile_h, host_views);
   if (tiles == 0) return SVO_ERR_INVALID;
   int max_s = 2;
@@ -95,12 +129,8 @@ extern "C" int svo_render_batch_static(const svo_octree_desc* octrees, uint32_t 
   int rc = scratch_address(&scratch);
   if (rc != SVO_OK) return rc;
   cudaStream_t s = (cudaStream_t)stream;
-  // pageable sources: each copy returns once the host data has been staged
-  SVO_CUDA_TRY(cudaMemcpyAsync(scratch + kOctreeOffset, host_octrees,
-                               num_octrees * sizeof(BatchOctree), cudaMemcpyHostToDevice, s));
-  SVO_CUDA_TRY(cudaMemcpyAsync(scratch + kViewOffset, host_views, num_views * sizeof(BatchView),
-                               cudaMemcpyHostToDevice, s));
-  SVO_CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(unsigned long long), s));
+  load_static_tables<<<1, 256, 0, s>>>(tables, scratch);
+  SVO_CUDA_TRY(cudaGetLastError());
   BatchLaunch L;
   L.views = reinterpret_cast<const BatchView*>(scratch + kViewOffset);
   L.num_views = num_views;
