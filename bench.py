@@ -191,6 +191,44 @@ def cpu_reference_frames(wl, nodes, attribs, seconds=10.0, max_frames=200, light
                       + ("; primary + shadow rays" if light is not None else "")}
 
 
+def reference_parity(nodes, attribs, params, gpu_rgba, gpu_hits, light=None, gpu_shadow_hits=None,
+                     config=""):
+    """Compares one GPU frame with the reference's own renderToBuffer compiled
+    for the host (oracle/_ref): every pixel's RGBA8, and per ray the node
+    index, depth, hit flag and loop count of the reference's sample() (primary
+    rays; with `light`, the shadow rays of the shadow frame).  The oracle
+    restatement stands in when the reference build is absent."""
+    import oracle
+
+    p = bytes(params)
+    w, h = (int(v) for v in np.frombuffer(p[:8], dtype=np.uint32))
+    ref = oracle.reference_lib() is not None
+    fields = ("node", "depth", "hit", "loops")
+    out = {"config": config, "pixels": w * h, "against": "reference" if ref else "oracle restatement"}
+    if light is None:
+        if ref:
+            ref_rgba = oracle.to_rgba8(oracle.reference_render(nodes, attribs, p))
+            o, d = oracle.pixel_rays(p)
+            ref_hits = oracle.reference_sample_rays(nodes, o, d, params.t_scale_ratio)
+        else:
+            ref_rgba, ref_hits, _, _ = oracle.render(nodes, attribs, p)
+        rays_ref, rays_gpu = ref_hits.reshape(-1), gpu_hits.reshape(-1)
+        out["rays"] = w * h
+    else:
+        if ref:
+            rgbaf, ref_shadow = oracle.reference_render_shadow(nodes, attribs, p, light)
+            ref_rgba = oracle.to_rgba8(rgbaf)
+        else:
+            ref_rgba, _, ref_shadow, _, _ = oracle.render_shadow(nodes, attribs, p, light)
+        rays_ref, rays_gpu = ref_shadow.reshape(-1), gpu_shadow_hits.reshape(-1)
+        out["rays"] = int(rays_gpu["hit"].size)
+        out["rays_compared"] = "shadow rays (one per primary hit; zero records elsewhere)"
+    out["mismatched_rgba"] = int((gpu_rgba.reshape(-1) != ref_rgba.reshape(-1)).sum())
+    out["mismatched_rays"] = int(np.any(np.stack([rays_gpu[k] != rays_ref[k] for k in fields]), axis=0).sum())
+    out["mismatched"] = out["mismatched_rgba"] + out["mismatched_rays"]
+    return out
+
+
 def run_reference(args, wl):
     """The reference arm: the reference's renderToBuffer compiled for the host
     (oracle/_ref; the oracle port if that is absent), all host threads, on
@@ -353,8 +391,8 @@ def served_leg(dev, n=400, rates=(4000, 16000, 64000)):
     outs = [torch.empty((c.height, c.width), dtype=torch.int32, device=dev) for _, c in reqs]
     rays = sum(c.width * c.height for _, c in reqs)
 
-    def run(mode, budget, rate_list, upload=None):
-        srv = L.Server(L.server_cfg(budget, streams=4, max_batch_views=256, mode=mode))
+    def run(mode, budget, rate_list, upload=None, streams=4):
+        srv = L.Server(L.server_cfg(budget, streams=streams, max_batch_views=256, mode=mode))
         ids = [srv.add_octree(s) for s in wl.scenes]
         if upload is not None:
             for i in ids:
@@ -379,17 +417,25 @@ def served_leg(dev, n=400, rates=(4000, 16000, 64000)):
     all_rates = list(rates) + [0]
     batched = run(L.SERVE_BATCHED, 2 * footprint, all_rates)
     plain = run(L.SERVE_PLAIN, 2 * footprint, all_rates)
+    # the ungated plain baseline: every admitted request's per-frame kernel
+    # launched at once, round robin over 8 streams, completion by events
+    ungated = run(L.SERVE_PLAIN_STREAMED, 2 * footprint, all_rates, streams=8)
     paging = run(L.SERVE_BATCHED, footprint // 2, [16000])
     paging_pinned = run(L.SERVE_BATCHED, footprint // 2, [16000], upload=L.UPLOAD_PINNED)
+    paging_ungated = run(L.SERVE_PLAIN_STREAMED, footprint // 2, [16000], streams=8)
+    paging_ungated_pinned = run(L.SERVE_PLAIN_STREAMED, footprint // 2, [16000], upload=L.UPLOAD_PINNED,
+                                streams=8)
+    keys = [k for k in batched if k != "paging"]
     return {"workload": wl.name, "description": wl.description, "requests": n, "rays": rays,
             "scene_build_s": round(build_s, 2), "octree_footprint_gb": footprint / 1e9,
             "budget_note": "the stand-in octrees total far less than the configuration's 40 GB cap; "
-                           "the paging run caps the pool at half their footprint",
-            "batched": batched, "plain": plain,
-            "speedup_vs_plain": {k: batched[k]["mrays_s"] / plain[k]["mrays_s"]
-                                 for k in batched if k != "paging"},
-            "paging_half_budget": paging,
-            "paging_half_budget_pinned_hosts": paging_pinned}
+                           "the paging runs cap the pool at half their footprint",
+            "batched": batched, "plain_one_stream": plain, "plain_ungated": ungated,
+            "speedup_vs_plain_ungated": {k: batched[k]["mrays_s"] / ungated[k]["mrays_s"] for k in keys},
+            "speedup_vs_plain_one_stream": {k: batched[k]["mrays_s"] / plain[k]["mrays_s"] for k in keys},
+            "paging_half_budget": {"batched": paging, "batched_pinned_hosts": paging_pinned,
+                                   "plain_ungated": paging_ungated,
+                                   "plain_ungated_pinned_hosts": paging_ungated_pinned}}
 
 
 def incore_update_leg(dev, scene, incore_mb=256, frames=20, seed=5):
@@ -594,21 +640,22 @@ def large_cpu_baseline(wl, n, seconds=10.0):
     """The reference's shadow frame compiled for the host over the large
     pool: the pool is copied to host memory (16 bytes per node), then whole
     frames are timed on all host threads.  Skipped, with the reason, unless
-    the host has twice the pool's size free."""
+    the host has twice the pool's size free.  Returns the baseline and the
+    host copy of the pool (None when skipped)."""
     import types
 
     need = 16 * n
     avail = host_memory_available()
     if avail < 2 * need + (16 << 30):
         return {"unavailable": f"the pool copy needs {need / 1e9:.1f} GB of host memory, "
-                               f"{avail / 1e9:.1f} GB available"}
+                               f"{avail / 1e9:.1f} GB available"}, None
     t0 = time.perf_counter()
     nodes, attribs = wl.scene.getIncoreBuffer()
     copy_s = time.perf_counter() - t0
     one_view = types.SimpleNamespace(cameras=[wl.camera], stack_size=wl.stack_size)
     out = cpu_reference_frames(one_view, nodes, attribs, seconds=seconds, light=wl.light)
     out["sample"] += f"; the {need / 1e9:.1f} GB pool copied to host memory first ({copy_s:.1f} s, untimed)"
-    return out
+    return out, (nodes, attribs)
 
 
 def large_shadow_leg(dev, reps=10, cap_gb=60.0, subdivisions=9, depth=14, cpu_baseline=True):
@@ -641,6 +688,7 @@ def large_shadow_leg(dev, reps=10, cap_gb=60.0, subdivisions=9, depth=14, cpu_ba
     torch.cuda.synchronize()
     h = hb.cpu().numpy().view(L.HIT_DTYPE)
     sh = sb.cpu().numpy().view(L.HIT_DTYPE)
+    gpu_rgba = rgba.cpu().numpy().view(np.uint32).copy()
     del hb, sb
     primary_hits = int(h["hit"].astype(np.int64).sum())
     shadow_rays = primary_hits  # one per hit (all hits lie in the pool)
@@ -675,7 +723,11 @@ def large_shadow_leg(dev, reps=10, cap_gb=60.0, subdivisions=9, depth=14, cpu_ba
     del flush, rgba
     if cpu_baseline:
         try:
-            out["cpu_baseline"] = large_cpu_baseline(wl, n)
+            out["cpu_baseline"], pool = large_cpu_baseline(wl, n)
+            if pool is not None:
+                out["parity"] = reference_parity(pool[0], pool[1], p, gpu_rgba, h, light=wl.light,
+                                                 gpu_shadow_hits=sh, config=wl.name)
+                del pool
         except Exception as e:  # the host copy or the CPU run failed: keep the GPU result
             out["cpu_baseline"] = {"unavailable": f"{type(e).__name__}: {e}"}
     wl.scene.close()
@@ -738,6 +790,7 @@ def main():
     # algorithmic bytes of one step, from the kernel's own per-ray counters
     fetches = hits = 0
     shadow = L.shadow_cfg(L.seeded_light(1)) if args.shadow else None
+    parity_frame = None  # the first view's GPU image and records, for the parity check
     with torch.cuda.stream(stream):
         for p, o in zip(params, outs):
             hb = torch.empty(p.width * p.height * 16, dtype=torch.uint8, device=dev)
@@ -750,8 +803,11 @@ def main():
             h = hb.cpu().numpy().view(L.HIT_DTYPE)
             fetches += int(h["fetches"].astype(np.int64).sum())
             hits += int(h["hit"].astype(np.int64).sum())
+            sh = sb.cpu().numpy().view(L.HIT_DTYPE) if shadow else None
             if shadow:
-                fetches += int(sb.cpu().numpy().view(L.HIT_DTYPE)["fetches"].astype(np.int64).sum())
+                fetches += int(sh["fetches"].astype(np.int64).sum())
+            if parity_frame is None:
+                parity_frame = (p, o.cpu().numpy().view(np.uint32).copy(), h, sh)
             del hb, sb
     algo_bytes = 8 * fetches + 8 * hits + 4 * rays
     primary_rays = rays
@@ -868,6 +924,10 @@ def main():
             nodes, attribs = mm.getIncoreBuffer()
             line["cpu_baseline"] = cpu_reference_frames(wl, nodes, attribs,
                                                         light=L.seeded_light(1) if shadow else None)
+            pp, p_rgba, p_hits, p_shadow = parity_frame
+            line["parity"] = reference_parity(nodes, attribs, pp, p_rgba, p_hits,
+                                              light=L.seeded_light(1) if shadow else None,
+                                              gpu_shadow_hits=p_shadow, config=line["config"]["workload"])
         mm.close()
         if world == 1 and not args.no_extra and args.workload == "icosphere":
             for key, leg in (("incore_update", incore_update_leg), ("streaming", streaming_leg)):

@@ -79,6 +79,10 @@ def lib():
         L.oracle_feedback.restype = None
         L.oracle_render_shadow.argtypes = [vp, vp, u64, vp, i32, vp, f32, f32, vp, vp, vp, vp, i32]
         L.oracle_render_shadow.restype = u64
+        u32 = ctypes.c_uint32
+        L.oracle_render_shadow_rows.argtypes = [vp, vp, u64, vp, i32, vp, f32, f32, u32, u32, vp, vp, vp,
+                                                vp, i32]
+        L.oracle_render_shadow_rows.restype = u64
         assert L.oracle_hit_record_size() == 16
         _lib = L
     return _lib
@@ -103,6 +107,9 @@ def reference_lib():
         L.ref_feedback.restype = None
         L.ref_render_shadow.argtypes = [vp, vp, vp, vp, f32, f32, vp, vp, i32]
         L.ref_render_shadow.restype = None
+        L.ref_render_shadow_rows.argtypes = [vp, vp, vp, vp, f32, f32, ctypes.c_uint32, ctypes.c_uint32,
+                                             vp, vp, i32]
+        L.ref_render_shadow_rows.restype = None
         assert L.ref_hit_record_size() == 16
         _ref = L
     return _ref
@@ -236,39 +243,44 @@ def default_light():
 
 def render_shadow(nodes, attribs, params: bytes, light, shadow_tsr: float = 0.001,
                   offset: float = 0.01, stack_size: int = 13,
-                  want_rgbaf: bool = False, threads=None):
+                  want_rgbaf: bool = False, threads=None, rows=None):
     """Primary plus shadow rays on the CPU.  Returns (rgba8 [H, W], hits [H, W],
-    shadow_hits [H, W], node_fetches, rgbaf or None)."""
+    shadow_hits [H, W], node_fetches, rgbaf or None); with ``rows`` = (y0, y1)
+    only those rows, as arrays of y1 - y0 rows."""
     nodes = np.ascontiguousarray(nodes, dtype=np.uint32)
     attribs = np.ascontiguousarray(attribs, dtype=np.uint32)
     light = np.ascontiguousarray(light, dtype=np.float32)
-    w, h = np.frombuffer(params[:8], dtype=np.uint32)
+    w, h = (int(v) for v in np.frombuffer(params[:8], dtype=np.uint32))
+    y0, y1 = (0, h) if rows is None else (int(rows[0]), min(h, int(rows[1])))
+    n = max(0, y1 - y0)
     pbuf = np.frombuffer(bytearray(params), dtype=np.uint8)
-    rgba = np.zeros((h, w), dtype=np.uint32)
-    hits = np.zeros((h, w), dtype=HIT_DTYPE)
-    shits = np.zeros((h, w), dtype=HIT_DTYPE)
-    rgbaf = np.zeros((h, w, 4), dtype=np.float32) if want_rgbaf else None
-    fetches = lib().oracle_render_shadow(
+    rgba = np.zeros((n, w), dtype=np.uint32)
+    hits = np.zeros((n, w), dtype=HIT_DTYPE)
+    shits = np.zeros((n, w), dtype=HIT_DTYPE)
+    rgbaf = np.zeros((n, w, 4), dtype=np.float32) if want_rgbaf else None
+    fetches = lib().oracle_render_shadow_rows(
         _ptr(nodes), _ptr(attribs), nodes.shape[0], _ptr(pbuf), int(stack_size), _ptr(light),
-        float(shadow_tsr), float(offset), _ptr(rgba),
+        float(shadow_tsr), float(offset), y0, y1, _ptr(rgba),
         _ptr(rgbaf) if want_rgbaf else None, _ptr(hits), _ptr(shits), _threads(threads))
     return rgba, hits, shits, int(fetches), rgbaf
 
 
 def reference_render_shadow(nodes, attribs, params: bytes, light, shadow_tsr: float = 0.001,
-                            offset: float = 0.01, threads=None):
+                            offset: float = 0.01, threads=None, rows=None):
     """The shadow shading over the reference's own sample(): (rgbaf [H, W, 4],
-    shadow_hits [H, W])."""
+    shadow_hits [H, W]); with ``rows`` = (y0, y1) only those rows."""
     L = reference_lib()
     if L is None:
         return None
     nodes = np.ascontiguousarray(nodes, dtype=np.uint32)
     attribs = np.ascontiguousarray(attribs, dtype=np.uint32)
     light = np.ascontiguousarray(light, dtype=np.float32)
-    w, h = np.frombuffer(params[:8], dtype=np.uint32)
-    out = np.zeros((h, w, 4), dtype=np.float32)
-    shits = np.zeros((h, w), dtype=HIT_DTYPE)
+    w, h = (int(v) for v in np.frombuffer(params[:8], dtype=np.uint32))
+    y0, y1 = (0, h) if rows is None else (int(rows[0]), min(h, int(rows[1])))
+    n = max(0, y1 - y0)
+    out = np.zeros((n, w, 4), dtype=np.float32)
+    shits = np.zeros((n, w), dtype=HIT_DTYPE)
     pbuf = np.frombuffer(bytearray(params), dtype=np.uint8)
-    L.ref_render_shadow(_ptr(nodes), _ptr(attribs), _ptr(pbuf), _ptr(light), float(shadow_tsr),
-                        float(offset), _ptr(out), _ptr(shits), _threads(threads))
+    L.ref_render_shadow_rows(_ptr(nodes), _ptr(attribs), _ptr(pbuf), _ptr(light), float(shadow_tsr),
+                             float(offset), y0, y1, _ptr(out), _ptr(shits), _threads(threads))
     return out, shits

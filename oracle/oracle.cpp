@@ -749,16 +749,22 @@ uint64_t oracle_render(const uint32_t* nodes, const uint32_t* attribs, uint64_t 
 // light: the unit direction toward the light, used as given.  Outputs as in
 // oracle_render, plus shadow_hits (zeros where no shadow ray was cast).
 // Returns the node fetches of both ray kinds.
-uint64_t oracle_render_shadow(const uint32_t* nodes, const uint32_t* attribs, uint64_t num_nodes,
-                              const void* params, int S, const float* light, float shadow_tsr,
-                              float offset, uint32_t* rgba8, float* rgbaf,
-                              void* hits, void* shadow_hits, int threads) {
+// Rows [y0, y1) of the frame only: the outputs hold (y1 - y0) * W entries,
+// row y at (y - y0) * W.
+uint64_t oracle_render_shadow_rows(const uint32_t* nodes, const uint32_t* attribs,
+                                   uint64_t num_nodes, const void* params, int S,
+                                   const float* light, float shadow_tsr, float offset, uint32_t y0,
+                                   uint32_t y1, uint32_t* rgba8, float* rgbaf, void* hits,
+                                   void* shadow_hits, int threads) {
   const FrameParams& fp = *(const FrameParams*)params;
   std::atomic<uint64_t> total{0};
   Hit* hrec = (Hit*)hits;
   Hit* srec = (Hit*)shadow_hits;
   const V3 l{light[0], light[1], light[2]};
-  parallel_lines(fp.height, 4, threads, [&](uint32_t y) {
+  if (y1 > fp.height) y1 = fp.height;
+  if (y0 >= y1) return 0;
+  parallel_lines(y1 - y0, 4, threads, [&](uint32_t yr) {
+    const uint32_t y = y0 + yr;
     RayCount rc;
     for (uint32_t x = 0; x < fp.width; ++x) {
       V3 o, d;
@@ -783,7 +789,7 @@ uint64_t oracle_render_shadow(const uint32_t* nodes, const uint32_t* attribs, ui
         for (int i = 0; i < 3; ++i) c[i] = col[i] * ndl * (1.0f - shadow) + col[i] * 0.2f;
         c[3] = 1.0f;
       }
-      const uint64_t pix = (uint64_t)y * fp.width + x;
+      const uint64_t pix = (uint64_t)yr * fp.width + x;
       if (hrec) hrec[pix] = h;
       if (srec) srec[pix] = sh;
       if (rgba8) rgba8[pix] = pack_rgba8(c[0], c[1], c[2], c[3]);
@@ -792,6 +798,15 @@ uint64_t oracle_render_shadow(const uint32_t* nodes, const uint32_t* attribs, ui
     total.fetch_add(rc.fetches, std::memory_order_relaxed);
   });
   return total.load();
+}
+
+uint64_t oracle_render_shadow(const uint32_t* nodes, const uint32_t* attribs, uint64_t num_nodes,
+                              const void* params, int S, const float* light, float shadow_tsr,
+                              float offset, uint32_t* rgba8, float* rgbaf,
+                              void* hits, void* shadow_hits, int threads) {
+  const FrameParams& fp = *(const FrameParams*)params;
+  return oracle_render_shadow_rows(nodes, attribs, num_nodes, params, S, light, shadow_tsr, offset,
+                                   0, fp.height, rgba8, rgbaf, hits, shadow_hits, threads);
 }
 
 // Casts an explicit list of rays (origins and directions, 3 floats each).
