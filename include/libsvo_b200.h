@@ -539,10 +539,14 @@ int svo_batcher_size(svo_batcher* b, uint64_t* tiles, uint64_t* rays);
  * by every GPU that loads it until the process exits.  At most 256 views and
  * 16 octrees per call (SVO_ERR_RANGE otherwise); tile 8x4, 16x2, 4x8 or 32x1;
  * 256-thread persistent blocks.  The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress) with that device current;
- * make that first call before any stream capture.  All calls share the one
- * array, which keeps the last call's contents; each call rewrites it and
- * zeroes its counter, and calls whose work overlaps on the GPU race. */
+ * array's device address (cudaGetSymbolAddress) with that device current
+ * and keeps it for the life of the process (do not use the library across a
+ * cudaDeviceReset); make that first call before any stream capture.  The
+ * descriptor tables reach the array as the by-value parameter of a small
+ * loader kernel launched on `stream` before the cast, so no host memory of
+ * the call is read after it returns.  All calls share the one array, which
+ * keeps the last call's contents; each call rewrites it and zeroes its
+ * counter, and calls whose work overlaps on the GPU race. */
 int svo_render_batch_static(const svo_octree_desc* octrees, uint32_t num_octrees,
                             const svo_view_desc* views, uint32_t num_views, uint32_t tile_w,
                             uint32_t tile_h, svo_stats* d_stats, void* stream);
@@ -561,6 +565,10 @@ int svo_render_batch_static(const svo_octree_desc* octrees, uint32_t num_octrees
  * that arrives while other batches run overlaps with them on the device. */
 #define SVO_SERVE_BATCHED 0 /* batched launches on `streams` streams       */
 #define SVO_SERVE_PLAIN 1   /* one per-frame kernel per request, one stream */
+/* One per-frame kernel per request, launched as soon as it is admitted,
+ * round robin over `streams` streams, completion by polled CUDA events: no
+ * launch slots and no host callback gate the plain kernel. */
+#define SVO_SERVE_PLAIN_STREAMED 2
 
 typedef struct svo_server_cfg {
   uint64_t hbm_budget_bytes;  /* device pool for octree node+attribute pools */
@@ -600,8 +608,24 @@ int svo_server_create(const svo_server_cfg* cfg, svo_server** out);
 /* Cancels requests not yet launched, waits for running ones, frees all. */
 void svo_server_destroy(svo_server* s);
 /* Registers an octree (copied) with the given stack size; not resident
- * until a request needs it. */
+ * until a request needs it.  An octree whose node and attribute pools
+ * together exceed the whole budget is registered as by
+ * svo_server_add_octree_paged with half the budget as its region. */
 int svo_server_add_octree(svo_server* s, const svo_scene* scene, int32_t stack_size, uint32_t* id);
+/* Registers an octree served by treelet paging: it holds `region_bytes` of
+ * the pool (node and attribute halves: region_bytes / (2 * treelet_bytes)
+ * slots, at least 2, at most one per treelet) for the server's life, starting
+ * with its root treelet alone, and a worker thread of its own serves its
+ * requests in arrival order.  Per request the worker runs analysis passes
+ * over the request's view at full resolution (svo_mm_analysis_step: the
+ * treelets it sees paged in, invisible ones evicted) until a pass places no
+ * new treelet, at most 48 passes, then casts the frame; when the treelets
+ * the view needs fit the region, the image is the fully resident octree's.
+ * The reference's out-of-core loop (src/TreeletMemoryManager.cpp:393-548,
+ * src/RenderPassAnalyse.cpp:218-356) applied per request.  SVO_ERR_BUSY if
+ * the pool cannot give the region now. */
+int svo_server_add_octree_paged(svo_server* s, const svo_scene* scene, int32_t stack_size,
+                                uint64_t region_bytes, uint32_t* id);
 /* How octree `octree` reaches the device pool (SVO_UPLOAD_*).
  * SVO_UPLOAD_PINNED page-locks its host copy once, here, so that every
  * later load is two DMA copies at PCIe speed issued without host copying

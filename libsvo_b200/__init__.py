@@ -851,6 +851,7 @@ def render_batch_static(octrees, views, tile=(8, 4), d_stats=None, stream=None):
 # ---- serving -------------------------------------------------------------------
 SERVE_BATCHED = 0
 SERVE_PLAIN = 1
+SERVE_PLAIN_STREAMED = 2
 
 
 class svo_server_cfg(ctypes.Structure):
@@ -881,6 +882,7 @@ for _name, (_args, _res) in {
     "svo_server_create": ([_P(svo_server_cfg), _P(_vp)], ctypes.c_int),
     "svo_server_destroy": ([_vp], None),
     "svo_server_add_octree": ([_vp, _vp, _i32, _P(_u32)], ctypes.c_int),
+    "svo_server_add_octree_paged": ([_vp, _vp, _i32, _u64, _P(_u32)], ctypes.c_int),
     "svo_server_set_upload_policy": ([_vp, _u32, _i32], ctypes.c_int),
     "svo_server_submit": ([_vp, _P(svo_request), _P(_u64)], ctypes.c_int),
     "svo_server_wait": ([_vp, _u64, _u32, _P(svo_request_result)], ctypes.c_int),
@@ -923,6 +925,13 @@ class Server:
         i = _u32()
         _check(_L.svo_server_add_octree(self._h, scene._h, stack_size, ctypes.byref(i)),
                "svo_server_add_octree")
+        return i.value
+
+    def add_octree_paged(self, scene: Scene, region_bytes: int, stack_size=13) -> int:
+        """An octree served by treelet paging inside a fixed region of the pool."""
+        i = _u32()
+        _check(_L.svo_server_add_octree_paged(self._h, scene._h, stack_size, int(region_bytes),
+                                              ctypes.byref(i)), "svo_server_add_octree_paged")
         return i.value
 
     def set_upload_policy(self, octree: int, policy: int):

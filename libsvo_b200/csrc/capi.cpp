@@ -611,45 +611,8 @@ int svo_mm_analysis_step(svo_mm* mm, const svo_frame_params* frame, uint32_t div
   if (!mm || !frame || divisor == 0 || !mm->impl.device_ready()) return SVO_ERR_INVALID;
   if (stack_size < 2 || stack_size > 24) return SVO_ERR_RANGE;
   return guarded([&] {
-    cudaStream_t s = stream ? (cudaStream_t)stream : mm->impl.render_stream();
-    // analysis buffer and its one-pixel far-plane vectors
-    // (RenderPassAnalyse.cpp:168-193): same frustum, coarser pixels
-    svo_frame_params a = *frame;
-    a.width = std::max(1u, frame->width / divisor);
-    a.height = std::max(1u, frame->height / divisor);
-    const double sx = (double)frame->width / a.width, sy = (double)frame->height / a.height;
-    for (int k = 0; k < 3; ++k) {
-      a.pixel_far_h[k] = (float)(frame->pixel_far_h[k] * sx);
-      a.pixel_far_v[k] = (float)(frame->pixel_far_v[k] * sy);
-      a.far_lower_left[k] = (float)(frame->far_lower_left[k] +
-                                    jitter_x * (double)divisor * frame->pixel_far_h[k] * 0.5 +
-                                    jitter_y * (double)divisor * frame->pixel_far_v[k] * 0.5);
-    }
-    const uint64_t n = (uint64_t)a.width * a.height;
-    svo_feedback* d_fb = nullptr;
-    int rc = mm->impl.feedback_scratch(n, &d_fb);
-    if (rc != SVO_OK) return rc;
-    rc = mm->impl.wait_uploads(s);
-    if (rc != SVO_OK) return rc;
-    rc = svo::launch_feedback(mm->impl.device_nodes(), mm->impl.incore_nodes(), a, stack_size, d_fb,
-                              nullptr, s);
-    if (rc != SVO_OK) return rc;
-    // the records stay on the GPU; only per-treelet results come back
-    std::vector<std::pair<int32_t, float>> nw, old;
-    rc = mm->impl.analyse_feedback_device(d_fb, n, mm->impl.default_max_new_treelets(), nw, old, s);
-    if (num_new) *num_new = (uint32_t)nw.size();
-    if (num_old) *num_old = (uint32_t)old.size();
-    if (rc != SVO_OK) return rc;
-    std::vector<int32_t> ng(nw.size()), og(old.size());
-    std::vector<float> ne(nw.size());
-    for (size_t i = 0; i < nw.size(); ++i) ng[i] = nw[i].first, ne[i] = nw[i].second;
-    for (size_t i = 0; i < old.size(); ++i) og[i] = old[i].first;
-    uint32_t placed = 0;
-    rc = mm->impl.update_client_side(ng.data(), ne.data(), (uint32_t)ng.size(), og.data(),
-                                     (uint32_t)og.size(), true, &placed);
-    if (num_new) *num_new = placed;
-    const int up = mm->impl.update_device_memory(nullptr);
-    return rc != SVO_OK ? rc : up;
+    return mm->impl.analysis_step(*frame, divisor, jitter_x, jitter_y, stack_size, (cudaStream_t)stream,
+                                  num_new, num_old);
   });
 }
 

@@ -9,6 +9,7 @@
 
 #include "analysis.h"
 #include "errors.h"
+#include "feedback.h"
 #include "render.h"
 #include "upload.h"
 
@@ -714,6 +715,54 @@ int TreeletMemoryManagerCuda::feedback_scratch(uint64_t records, svo_feedback** 
   }
   *out = d_feedback_;
   return SVO_OK;
+}
+
+int TreeletMemoryManagerCuda::analysis_step(const svo_frame_params& frame, uint32_t divisor,
+                                            float jitter_x, float jitter_y, int32_t stack_size,
+                                            cudaStream_t stream, uint32_t* num_new,
+                                            uint32_t* num_old) {
+  if (num_new) *num_new = 0;
+  if (num_old) *num_old = 0;
+  if (divisor == 0 || !device_ready()) return SVO_ERR_INVALID;
+  if (stack_size < 2 || stack_size > 24) return SVO_ERR_RANGE;
+  cudaStream_t s = stream ? stream : render_stream_;
+  // analysis buffer and its one-pixel far-plane vectors
+  // (RenderPassAnalyse.cpp:168-193): same frustum, coarser pixels
+  svo_frame_params a = frame;
+  a.width = std::max(1u, frame.width / divisor);
+  a.height = std::max(1u, frame.height / divisor);
+  const double sx = (double)frame.width / a.width, sy = (double)frame.height / a.height;
+  for (int k = 0; k < 3; ++k) {
+    a.pixel_far_h[k] = (float)(frame.pixel_far_h[k] * sx);
+    a.pixel_far_v[k] = (float)(frame.pixel_far_v[k] * sy);
+    a.far_lower_left[k] = (float)(frame.far_lower_left[k] +
+                                  jitter_x * (double)divisor * frame.pixel_far_h[k] * 0.5 +
+                                  jitter_y * (double)divisor * frame.pixel_far_v[k] * 0.5);
+  }
+  const uint64_t n = (uint64_t)a.width * a.height;
+  svo_feedback* d_fb = nullptr;
+  int rc = feedback_scratch(n, &d_fb);
+  if (rc != SVO_OK) return rc;
+  rc = wait_uploads(s);
+  if (rc != SVO_OK) return rc;
+  rc = launch_feedback(device_nodes(), incore_nodes(), a, stack_size, d_fb, nullptr, s);
+  if (rc != SVO_OK) return rc;
+  // the records stay on the GPU; only per-treelet results come back
+  std::vector<std::pair<int32_t, float>> nw, old;
+  rc = analyse_feedback_device(d_fb, n, default_max_new_treelets(), nw, old, s);
+  if (num_new) *num_new = (uint32_t)nw.size();
+  if (num_old) *num_old = (uint32_t)old.size();
+  if (rc != SVO_OK) return rc;
+  std::vector<int32_t> ng(nw.size()), og(old.size());
+  std::vector<float> ne(nw.size());
+  for (size_t i = 0; i < nw.size(); ++i) ng[i] = nw[i].first, ne[i] = nw[i].second;
+  for (size_t i = 0; i < old.size(); ++i) og[i] = old[i].first;
+  uint32_t placed = 0;
+  rc = update_client_side(ng.data(), ne.data(), (uint32_t)ng.size(), og.data(), (uint32_t)og.size(),
+                          true, &placed);
+  if (num_new) *num_new = placed;
+  const int up = update_device_memory(nullptr);
+  return rc != SVO_OK ? rc : up;
 }
 
 }  // namespace svo

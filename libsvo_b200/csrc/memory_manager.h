@@ -157,6 +157,17 @@ class TreeletMemoryManagerCuda : public TreeletMemoryManager {
                               std::vector<std::pair<int32_t, float>>& out_new,
                               std::vector<std::pair<int32_t, float>>& out_old,
                               cudaStream_t stream);
+  // One dynamic-loading step of the reference's frame loop
+  // (raycast_serialized_opencl.cpp:684-716; RenderPassAnalyse::
+  // performAnalysePass, src/RenderPassAnalyse.cpp:150-369): the analysis
+  // rays over `frame` at 1/divisor resolution with the far plane jittered by
+  // (jitter_x, jitter_y) * divisor / 2 frame pixels, the records analysed on
+  // the GPU, treelets inserted (new ones that find no slot are skipped, as
+  // the reference ignores its insertion results) and the dirty slots
+  // uploaded.  *num_new: treelets placed; *num_old: visible resident ones.
+  int analysis_step(const svo_frame_params& frame, uint32_t divisor, float jitter_x,
+                    float jitter_y, int32_t stack_size, cudaStream_t stream, uint32_t* num_new,
+                    uint32_t* num_old);
 
  private:
   int init_analysis();

@@ -17,8 +17,21 @@
 // are evicted least recently used first when the pool is full.  A host
 // callback on each batch's stream timestamps completion.
 //
+// An octree whose pools do not fit the whole budget (or one registered with
+// svo_server_add_octree_paged) is not made resident whole: it keeps a fixed
+// region of treelet slots in the pool and a worker thread of its own, which
+// serves its requests one by one, each after analysis passes over the
+// request's view at full resolution until no new treelet is placed
+// (treelets paged in and out of the region by visibility, the reference's
+// out-of-core loop), so a request whose visible treelets fit the region gets
+// the image of the fully resident octree.
+//
 // In SVO_SERVE_PLAIN mode the same loop launches the per-frame kernel once
-// per request on a single stream instead: the plain baseline.
+// per request on a single stream instead: the plain baseline.  In
+// SVO_SERVE_PLAIN_STREAMED mode the dispatcher launches each admitted
+// request's per-frame kernel at once, round robin over `streams` streams,
+// with no launch slots and no host callback: a CUDA event recorded after
+// each launch is polled for its completion (the ungated plain baseline).
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -28,6 +41,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <system_error>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -91,6 +105,15 @@ class DevicePool {
   std::map<uint64_t, uint64_t> free_;
 };
 
+// Serves the requests of one treelet-paged octree, in arrival order.
+struct PagedWorker {
+  std::thread thread;
+  cudaStream_t stream = nullptr;
+  std::deque<uint64_t> queue;  // tickets, guarded by the server's mutex
+  std::condition_variable cv;
+  bool stop = false;
+};
+
 struct ServedOctree {
   std::unique_ptr<svo::TreeletMemoryManagerCuda> mm;
   int32_t stack_size = 13;
@@ -99,7 +122,13 @@ struct ServedOctree {
   uint64_t pool_off = 0;
   uint32_t refs = 0;  // batches in flight that read it
   uint64_t last_use = 0;
+  bool paged = false;  // a fixed region of slots, paged by its worker
+  std::unique_ptr<PagedWorker> worker;
 };
+
+// Analysis passes before a paged request gives up converging and renders
+// with what is resident.
+constexpr uint32_t kMaxPagingSteps = 48;
 
 struct Request {
   svo_request r{};
@@ -146,6 +175,18 @@ struct svo_server {
   std::atomic<uint64_t> callbacks_launched{0};
   std::atomic<uint64_t> callbacks_exited{0};
 
+  // SVO_SERVE_PLAIN_STREAMED: launches in flight, each with the event
+  // recorded after it, and recycled events
+  struct Streamed {
+    uint64_t ticket;
+    cudaEvent_t done;
+    uint32_t octree;
+    uint64_t rays;
+  };
+  std::vector<Streamed> streamed;
+  std::vector<cudaEvent_t> spare_events;
+  uint32_t next_stream = 0;
+
   uint64_t inflight_rays = 0;
   bool blocked = false;  // admission stopped on a limit; cleared by completions
   uint64_t use_clock = 0;
@@ -173,17 +214,15 @@ void CUDART_CB on_slot_done(void* p) {
 
 // Makes octree `id` resident, evicting idle octrees if the pool is full.
 // Called by the dispatcher with `mu` held.
-int ensure_resident(svo_server* s, uint32_t id) {
-  ServedOctree& o = s->octrees[id];
-  o.last_use = ++s->use_clock;
-  if (o.resident) return SVO_OK;
-  const uint64_t need = 2 * ((o.node_bytes + 255) & ~255ull);
-  uint64_t off = 0;
-  while (!s->pool.alloc(need, &off)) {
+// Allocates `need` bytes of the pool, evicting idle whole-resident octrees
+// (least recently used first, never `keep` or a paged octree's region).
+// Called with `mu` held.
+int alloc_evicting(svo_server* s, uint64_t need, int keep, uint64_t* off) {
+  while (!s->pool.alloc(need, off)) {
     int victim = -1;
     for (uint32_t i = 0; i < s->octrees.size(); ++i) {
       const ServedOctree& c = s->octrees[i];
-      if (i == id || !c.resident || c.refs) continue;
+      if ((int)i == keep || c.paged || !c.resident || c.refs) continue;
       if (victim < 0 || c.last_use < s->octrees[victim].last_use) victim = (int)i;
     }
     if (victim < 0) return need > s->pool.size() ? SVO_ERR_RANGE : SVO_ERR_BUSY;
@@ -196,6 +235,17 @@ int ensure_resident(svo_server* s, uint32_t id) {
     s->stats.resident_octrees--;
     s->stats.resident_bytes -= 2 * v.node_bytes;
   }
+  return SVO_OK;
+}
+
+int ensure_resident(svo_server* s, uint32_t id) {
+  ServedOctree& o = s->octrees[id];
+  o.last_use = ++s->use_clock;
+  if (o.resident) return SVO_OK;
+  const uint64_t need = 2 * ((o.node_bytes + 255) & ~255ull);
+  uint64_t off = 0;
+  const int arc = alloc_evicting(s, need, (int)id, &off);
+  if (arc != SVO_OK) return arc;
   char* base = s->pool.base() + off;
   const uint64_t attr_off = (o.node_bytes + 255) & ~255ull;
   const int rc = o.mm->attach_device_buffers(reinterpret_cast<svo_node*>(base),
@@ -212,6 +262,80 @@ int ensure_resident(svo_server* s, uint32_t id) {
   s->stats.resident_octrees++;
   s->stats.resident_bytes += 2 * o.node_bytes;
   return SVO_OK;
+}
+
+// A paged octree's worker: per request, analysis passes over the request's
+// view at full resolution until a pass places no new treelet (at most
+// kMaxPagingSteps), then the per-frame kernel, waited for on the worker's
+// stream.
+void paged_worker_loop(svo_server* s, uint32_t id) {
+  PagedWorker* w = nullptr;
+  svo::TreeletMemoryManagerCuda* mm = nullptr;
+  int32_t S = 13;
+  uint64_t slot_bytes = 0;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    w = s->octrees[id].worker.get();
+    mm = s->octrees[id].mm.get();
+    S = s->octrees[id].stack_size;
+    slot_bytes = 2ull * mm->treelet_bytes();
+  }
+  for (;;) {
+    uint64_t t = 0;
+    svo_request r{};
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      w->cv.wait(lk, [&] { return w->stop || !w->queue.empty(); });
+      if (w->stop) return;  // queued requests are cancelled by the destroyer
+      t = w->queue.front();
+      w->queue.pop_front();
+      Request& q = s->requests[t];
+      q.res.launch_s = s->now();
+      q.res.batch = s->batch_seq++;
+      s->stats.batches++;
+      r = q.r;
+    }
+    uint32_t placed = 0;
+    int rc = SVO_OK;
+    for (uint32_t step = 0; step < kMaxPagingSteps; ++step) {
+      uint32_t nw = 0, old = 0;
+      rc = mm->analysis_step(r.params, 1, 0.0f, 0.0f, S, w->stream, &nw, &old);
+      if (rc != SVO_OK || nw == 0) break;
+      placed += nw;
+    }
+    if (rc == SVO_OK) rc = mm->wait_uploads(w->stream);
+    if (rc == SVO_OK) {
+      const svo_trace_cfg tc{SVO_TRAVERSAL_TREELET, S};
+      rc = svo::launch_render(mm->device_nodes(), mm->device_attribs(), mm->incore_nodes(), r.params, tc,
+                              r.d_rgba, nullptr, nullptr, w->stream);
+    }
+    if (rc == SVO_OK) rc = svo::cuda_status(cudaStreamSynchronize(w->stream));
+    std::lock_guard<std::mutex> lk(s->mu);
+    Request& q = s->requests[t];
+    q.res.done_s = s->now();
+    q.res.status = rc;
+    q.done = true;
+    s->stats.requests_done++;
+    s->stats.rays_done += (uint64_t)r.params.width * r.params.height;
+    s->stats.treelets_paged_in += placed;
+    s->stats.bytes_uploaded += placed * slot_bytes;
+    s->cv_user.notify_all();
+  }
+}
+
+// Hands pending requests on paged octrees to their workers.  Called with
+// `mu` held.
+void route_paged(svo_server* s) {
+  for (auto it = s->pending.begin(); it != s->pending.end();) {
+    ServedOctree& o = s->octrees[s->requests[*it].r.octree];
+    if (!o.paged) {
+      ++it;
+      continue;
+    }
+    o.worker->queue.push_back(*it);
+    o.worker->cv.notify_one();
+    it = s->pending.erase(it);
+  }
 }
 
 void finish_slot(svo_server* s, svo_server::Slot& slot) {
@@ -304,6 +428,7 @@ void dispatch_loop(svo_server* s) {
       s->blocked = false;
       s->cv_user.notify_all();
     }
+    route_paged(s);
     bool busy_any = false;
     for (auto& sl : s->slots) busy_any |= sl.busy;
     if (s->stop && s->pending.empty() && !busy_any) return;
@@ -401,6 +526,149 @@ void dispatch_loop(svo_server* s) {
   }
 }
 
+// SVO_SERVE_PLAIN_STREAMED: one per-frame kernel per request, launched as
+// soon as the request is admitted (residency and the in-flight ray budget as
+// in the other modes), round robin over the slots' streams; completions are
+// found by polling the event recorded after each launch, every 20 us while
+// launches are in flight.  Called with `mu` held by the dispatcher.
+int streamed_launch(svo_server* s, uint64_t t) {
+  Request& q = s->requests[t];
+  ServedOctree& o = s->octrees[q.r.octree];
+  svo_server::Slot& slot = s->slots[s->next_stream];
+  s->next_stream = (s->next_stream + 1) % (uint32_t)s->slots.size();
+  int rc = o.mm->wait_uploads(slot.stream);
+  if (rc != SVO_OK) return rc;
+  q.res.launch_s = s->now();
+  q.res.batch = s->batch_seq++;
+  s->stats.batches++;
+  const svo_trace_cfg tc{SVO_TRAVERSAL_TREELET, o.stack_size};
+  rc = svo::launch_render(o.mm->device_nodes(), o.mm->device_attribs(), o.mm->incore_nodes(),
+                          q.r.params, tc, q.r.d_rgba, nullptr, nullptr, slot.stream);
+  if (rc != SVO_OK) return rc;
+  cudaEvent_t ev = nullptr;
+  if (!s->spare_events.empty()) {
+    ev = s->spare_events.back();
+    s->spare_events.pop_back();
+  } else {
+    SVO_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  }
+  const cudaError_t e = cudaEventRecord(ev, slot.stream);
+  if (e != cudaSuccess) {
+    s->spare_events.push_back(ev);
+    return svo::cuda_status(e);
+  }
+  const uint64_t rays = (uint64_t)q.r.params.width * q.r.params.height;
+  o.refs++;
+  s->inflight_rays += rays;
+  s->streamed.push_back(svo_server::Streamed{t, ev, q.r.octree, rays});
+  return SVO_OK;
+}
+
+void dispatch_loop_streamed(svo_server* s) {
+  std::unique_lock<std::mutex> lk(s->mu);
+  for (;;) {
+    if (s->streamed.empty()) {
+      s->cv_dispatch.wait_for(lk, std::chrono::microseconds(200), [&] {
+        return s->stop || (!s->pending.empty() && !s->blocked);
+      });
+    } else {
+      lk.unlock();
+      std::this_thread::sleep_for(std::chrono::microseconds(20));
+      lk.lock();
+    }
+    // completions, in any order
+    bool any_done = false;
+    for (size_t i = 0; i < s->streamed.size();) {
+      svo_server::Streamed& f = s->streamed[i];
+      const cudaError_t e = cudaEventQuery(f.done);
+      if (e == cudaErrorNotReady) {
+        ++i;
+        continue;
+      }
+      Request& q = s->requests[f.ticket];
+      q.res.done_s = s->now();
+      q.res.status = e == cudaSuccess ? SVO_OK : svo::cuda_status(e);
+      q.done = true;
+      s->stats.requests_done++;
+      s->stats.rays_done += f.rays;
+      s->octrees[f.octree].refs--;
+      s->inflight_rays -= f.rays;
+      s->spare_events.push_back(f.done);
+      f = s->streamed.back();
+      s->streamed.pop_back();
+      any_done = true;
+    }
+    if (any_done) {
+      s->blocked = false;
+      s->cv_user.notify_all();
+    }
+    route_paged(s);
+    if (s->stop && s->pending.empty() && s->streamed.empty()) return;
+    if (s->fatal != SVO_OK) continue;
+    // admission in arrival order, requests on resident octrees first (as in
+    // the batched mode); the oldest request pages its octree in when nothing
+    // else can go, or when it has waited longer than 50 ms
+    constexpr double kMaxWait = 0.05;
+    auto fits = [&](const Request& q) {
+      const uint64_t rays = (uint64_t)q.r.params.width * q.r.params.height;
+      return s->inflight_rays == 0 || s->inflight_rays + rays <= s->cfg.max_inflight_rays;
+    };
+    bool launched = true;
+    while (launched && !s->pending.empty()) {
+      launched = false;
+      const bool starving = s->now() - s->requests[s->pending.front()].res.submit_s > kMaxWait;
+      if (!starving) {
+        for (auto it = s->pending.begin(); it != s->pending.end();) {
+          const Request& q = s->requests[*it];
+          if (!fits(q)) break;
+          if (!s->octrees[q.r.octree].resident) {
+            ++it;
+            continue;
+          }
+          s->octrees[q.r.octree].last_use = ++s->use_clock;
+          const uint64_t t = *it;
+          const int rc = streamed_launch(s, t);
+          if (rc != SVO_OK) {
+            s->fatal = rc;
+            break;
+          }
+          it = s->pending.erase(it);
+          launched = true;
+        }
+      }
+      if (s->fatal != SVO_OK || s->pending.empty()) break;
+      Request& q = s->requests[s->pending.front()];
+      if (!fits(q)) break;
+      const int rc = ensure_resident(s, q.r.octree);
+      if (rc == SVO_ERR_BUSY) break;  // the pool is held by launches in flight
+      if (rc != SVO_OK) {
+        s->pending.pop_front();
+        q.res.status = rc;
+        q.done = true;
+        s->cv_user.notify_all();
+        launched = true;
+        continue;
+      }
+      const int lrc = streamed_launch(s, s->pending.front());
+      if (lrc != SVO_OK) {
+        s->fatal = lrc;
+        break;
+      }
+      s->pending.pop_front();
+      launched = true;
+    }
+    if (s->fatal != SVO_OK) {
+      for (uint64_t t : s->pending) {
+        s->requests[t].res.status = s->fatal;
+        s->requests[t].done = true;
+      }
+      s->pending.clear();
+      s->cv_user.notify_all();
+    }
+    s->blocked = !s->pending.empty() && !s->streamed.empty();
+  }
+}
+
 // The pool, the slots' streams and batchers, and the dispatcher thread.
 int start_server(svo_server* s, const svo_server_cfg* cfg) {
   int rc = s->pool.init(cfg->hbm_budget_bytes);
@@ -421,7 +689,7 @@ int start_server(svo_server* s, const svo_server_cfg* cfg) {
       rc = svo_batcher_create(cfg->max_batch_views, 64, &sl.batcher);
   }
   if (rc != SVO_OK) return rc;
-  s->dispatcher = std::thread(dispatch_loop, s);
+  s->dispatcher = std::thread(cfg->mode == SVO_SERVE_PLAIN_STREAMED ? dispatch_loop_streamed : dispatch_loop, s);
   return SVO_OK;
 }
 
@@ -435,7 +703,9 @@ int svo_server_create(const svo_server_cfg* cfg, svo_server** out) {
   if (cfg->streams == 0 || cfg->streams > 16 || cfg->max_batch_views == 0 ||
       cfg->max_batch_views > 4096 || cfg->max_inflight_rays == 0)
     return SVO_ERR_RANGE;
-  if (cfg->mode != SVO_SERVE_BATCHED && cfg->mode != SVO_SERVE_PLAIN) return SVO_ERR_NOTSUP;
+  if (cfg->mode != SVO_SERVE_BATCHED && cfg->mode != SVO_SERVE_PLAIN &&
+      cfg->mode != SVO_SERVE_PLAIN_STREAMED)
+    return SVO_ERR_NOTSUP;
   auto* s = new (std::nothrow) svo_server;
   if (!s) return SVO_ERR_NOMEM;
   s->cfg = *cfg;
@@ -474,9 +744,31 @@ void svo_server_destroy(svo_server* s) {
     s->cv_dispatch.notify_one();
     s->dispatcher.join();
   }
+  // paged octrees' workers: requests still queued end as cancelled
+  for (auto& o : s->octrees) {
+    if (!o.worker) continue;
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      o.worker->stop = true;
+      for (uint64_t t : o.worker->queue) {
+        s->requests[t].res.status = SVO_ERR_CANCELED;
+        s->requests[t].done = true;
+      }
+      o.worker->queue.clear();
+    }
+    o.worker->cv.notify_one();
+    if (o.worker->thread.joinable()) o.worker->thread.join();
+    if (o.worker->stream) {
+      cudaStreamSynchronize(o.worker->stream);
+      cudaStreamDestroy(o.worker->stream);
+    }
+  }
+  s->cv_user.notify_all();
   // plain mode: all slots share slot 0's stream, destroyed once at the end
   for (auto& sl : s->slots)
     if (sl.stream) cudaStreamSynchronize(sl.stream);
+  for (auto& f : s->streamed) cudaEventDestroy(f.done);  // (none left after a clean stop)
+  for (cudaEvent_t e : s->spare_events) cudaEventDestroy(e);
   for (uint32_t i = 0; i < s->slots.size(); ++i) {
     auto& sl = s->slots[i];
     if (sl.batcher) svo_batcher_destroy(sl.batcher);
@@ -494,29 +786,91 @@ void svo_server_destroy(svo_server* s) {
   delete s;
 }
 
-int svo_server_add_octree(svo_server* s, const svo_scene* scene, int32_t stack_size, uint32_t* id) {
+}  // extern "C"
+
+namespace {
+
+// Registers an octree: whole-resident on demand, or treelet-paged in a
+// region of `region_bytes` (node and attribute halves) when `paged`.
+int add_octree(svo_server* s, const svo_scene* scene, int32_t stack_size, bool paged,
+               uint64_t region_bytes, uint32_t* id) {
   if (!s || !scene || !id || scene->treelets.empty()) return SVO_ERR_INVALID;
   if (stack_size < 2 || stack_size > 24) return SVO_ERR_RANGE;
   try {
     ServedOctree o;
     o.mm.reset(new svo::TreeletMemoryManagerCuda(nullptr));
     svo_scene copy = *scene;
-    const uint64_t incore = (uint64_t)scene->treelet_bytes * scene->treelets.size();
-    int rc = o.mm->init(std::move(copy), incore);
+    const uint64_t tb = scene->treelet_bytes;
+    const uint64_t whole = 2 * ((tb * scene->treelets.size() + 255) & ~255ull);
+    if (!paged && whole > s->pool.size()) {  // does not fit whole: paged in half the budget
+      paged = true;
+      region_bytes = s->pool.size() / 2;
+    }
+    uint64_t slots = scene->treelets.size();
+    if (paged) {
+      slots = std::min<uint64_t>(slots, (region_bytes / 2) / tb);
+      if (slots < 2) return SVO_ERR_RANGE;  // the root and one more treelet at least
+    }
+    int rc = o.mm->init(std::move(copy), slots * tb);
     if (rc != SVO_OK) return rc;
-    uint32_t n = 0;
-    rc = o.mm->insert_all(&n);
-    if (rc != SVO_OK) return rc;
+    if (!paged) {
+      uint32_t n = 0;
+      rc = o.mm->insert_all(&n);
+      if (rc != SVO_OK) return rc;
+    }
     o.stack_size = stack_size;
     o.node_bytes = o.mm->incore_nodes() * sizeof(svo_node);
-    std::lock_guard<std::mutex> lk(s->mu);
+    o.paged = paged;
+    std::unique_lock<std::mutex> lk(s->mu);
     if (s->octrees.size() >= 64) return SVO_ERR_RANGE;
+    if (paged) {
+      // the region is held for the server's life; only the root treelet is
+      // resident at first
+      const uint64_t need = 2 * ((o.node_bytes + 255) & ~255ull);
+      uint64_t off = 0;
+      rc = alloc_evicting(s, need, -1, &off);
+      if (rc != SVO_OK) return rc;
+      char* base = s->pool.base() + off;
+      rc = o.mm->attach_device_buffers(reinterpret_cast<svo_node*>(base),
+                                       reinterpret_cast<svo_attrib*>(base + need / 2));
+      if (rc == SVO_OK) rc = o.mm->wait_uploads(nullptr);
+      if (rc == SVO_OK) rc = svo::cuda_status(cudaStreamSynchronize(nullptr));
+      if (rc != SVO_OK) {
+        s->pool.release(off, need);
+        return rc;
+      }
+      o.pool_off = off;
+      o.resident = true;
+      o.worker.reset(new PagedWorker);
+      rc = svo::cuda_status(cudaStreamCreateWithFlags(&o.worker->stream, cudaStreamNonBlocking));
+      if (rc != SVO_OK) {
+        s->pool.release(off, need);
+        return rc;
+      }
+      s->stats.resident_bytes += need;
+    }
     s->octrees.push_back(std::move(o));
     *id = (uint32_t)s->octrees.size() - 1;
+    if (paged) s->octrees.back().worker->thread = std::thread(paged_worker_loop, s, *id);
   } catch (const std::bad_alloc&) {
+    return SVO_ERR_NOMEM;
+  } catch (const std::system_error&) {  // the worker thread could not start
     return SVO_ERR_NOMEM;
   }
   return SVO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int svo_server_add_octree(svo_server* s, const svo_scene* scene, int32_t stack_size, uint32_t* id) {
+  return add_octree(s, scene, stack_size, false, 0, id);
+}
+
+int svo_server_add_octree_paged(svo_server* s, const svo_scene* scene, int32_t stack_size,
+                                uint64_t region_bytes, uint32_t* id) {
+  return add_octree(s, scene, stack_size, true, region_bytes, id);
 }
 
 int svo_server_set_upload_policy(svo_server* s, uint32_t octree, int32_t policy) {

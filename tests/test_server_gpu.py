@@ -41,7 +41,7 @@ def footprint(scene):
 
 
 @pytest.mark.parametrize("mode,upload", [(L.SERVE_BATCHED, None), (L.SERVE_PLAIN, None),
-                                         (L.SERVE_BATCHED, L.UPLOAD_PINNED)])
+                                         (L.SERVE_PLAIN_STREAMED, None), (L.SERVE_BATCHED, L.UPLOAD_PINNED)])
 def test_results_same_alone_and_in_the_mix(workload, cuda, mode, upload):
     """upload: octree loads as DMA copies from page-locked host copies."""
     import torch
@@ -112,24 +112,78 @@ def test_cancel_wait_timeout_and_errors(workload, cuda):
         srv.submit(L.request(99, cam.frame_params(), out))
     assert e.value.code == L.SVO_ERR_INVALID
     srv.close()
-    # an octree larger than the whole budget fails its requests instead of hanging
-    tiny = L.Server(L.server_cfg(1 << 20, streams=1))
-    big = tiny.add_octree(workload.scenes[3])
-    t = tiny.submit(L.request(big, cam.frame_params(), out))
-    assert tiny.wait(t, timeout_ms=5000).status == L.SVO_ERR_RANGE
+    # a budget too small for even two treelet slots of an octree: registration fails
+    scene = workload.scenes[3]
+    tiny = L.Server(L.server_cfg(2 * scene.info.treelet_bytes, streams=1))
+    with pytest.raises(L.SvoError) as e:
+        tiny.add_octree(scene)
+    assert e.value.code == L.SVO_ERR_RANGE
     tiny.close()
 
 
-def test_repeated_create_serve_destroy(workload, cuda):
+def test_octree_larger_than_the_budget_is_paged(workload, cuda):
+    """An octree whose pools exceed the whole budget is no longer refused: it
+    is served by treelet paging in half the budget, and a distant view (few
+    treelets at its level of detail) converges to the fully resident image."""
+    import torch
+
+    scene = workload.scenes[2]
+    srv = L.Server(L.server_cfg(footprint(scene) // 2, streams=2))
+    oid = srv.add_octree(scene)
+    cams = [L.orbit_camera(k, 96, 64, radius=2.4) for k in range(3)]
+    outs = [torch.full((c.height, c.width), -1, dtype=torch.int32, device=cuda) for c in cams]
+    res = srv.replay([L.request(oid, c.frame_params(), t) for c, t in zip(cams, outs)], np.zeros(len(cams)),
+                     timeout_ms=60000)
+    assert all(r.status == L.SVO_OK for r in res)
+    st = srv.stats()
+    assert st.treelets_paged_in > 0 and st.octree_loads == 0
+    torch.cuda.synchronize()
+    for c, t in zip(cams, outs):
+        assert np.array_equal(t.cpu().numpy(), alone(scene, c, cuda))
+    srv.close()
+
+
+@pytest.mark.parametrize("mode", [L.SERVE_BATCHED, L.SERVE_PLAIN_STREAMED])
+def test_treelet_paged_octree_same_alone_and_in_the_mix(workload, cuda, mode):
+    """The largest octree served by treelet paging in a region of 3/4 of its
+    footprint, the others whole and paged in and out under the rest of the
+    budget: every request's image equals its fully resident render, bit for
+    bit (the paged requests' analysis passes run to convergence)."""
+    import torch
+
+    sizes = [footprint(s) for s in workload.scenes]
+    big = int(np.argmax(sizes))
+    others = sorted(sizes[i] for i in range(len(sizes)) if i != big)
+    region = 3 * sizes[big] // 4
+    budget = region + int(1.1 * (others[-1] + others[-2])) + (1 << 20)
+    srv = L.Server(L.server_cfg(budget, streams=3, max_batch_views=8, mode=mode))
+    ids = [srv.add_octree_paged(s, region) if i == big else srv.add_octree(s)
+           for i, s in enumerate(workload.scenes)]
+    reqs = S.serving_requests(36, len(workload.scenes), seed=21, max_wh=(256, 160))
+    assert sum(o == big for o, _ in reqs) >= 5
+    outs = [torch.full((c.height, c.width), -1, dtype=torch.int32, device=cuda) for _, c in reqs]
+    rq = [L.request(ids[o], c.frame_params(), t) for (o, c), t in zip(reqs, outs)]
+    res = srv.replay(rq, S.poisson_arrivals(len(rq), 1000.0, seed=2), timeout_ms=60000)
+    assert all(r.status == L.SVO_OK for r in res)
+    st = srv.stats()
+    assert st.requests_done == len(rq) and st.treelets_paged_in > 0
+    torch.cuda.synchronize()
+    for (o, cam), t in zip(reqs, outs):
+        assert np.array_equal(t.cpu().numpy(), alone(workload.scenes[o], cam, cuda)), f"octree {o}"
+    srv.close()
+
+
+@pytest.mark.parametrize("mode", [L.SERVE_BATCHED, L.SERVE_PLAIN_STREAMED])
+def test_repeated_create_serve_destroy(workload, cuda, mode):
     """Teardown right after the last completion, many times over: the server
-    must outlive its stream callbacks."""
+    must outlive its stream callbacks (batched) and its events (streamed)."""
     import torch
 
     total = sum(footprint(s) for s in workload.scenes)
     cams = [L.orbit_camera(k, 48 + 8 * k, 40, radius=1.6) for k in range(12)]
     outs = [torch.empty((c.height, c.width), dtype=torch.int32, device=cuda) for c in cams]
     for cycle in range(15):
-        srv = L.Server(L.server_cfg(total, streams=4, max_batch_views=3))
+        srv = L.Server(L.server_cfg(total, streams=4, max_batch_views=3, mode=mode))
         oid = srv.add_octree(workload.scenes[cycle % len(workload.scenes)])
         res = srv.replay([L.request(oid, c.frame_params(), t) for c, t in zip(cams, outs)],
                          np.zeros(len(cams)), timeout_ms=20000)
