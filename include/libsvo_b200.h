@@ -174,6 +174,15 @@ int svo_device_scene_copy(const svo_device_scene* scene, uint64_t first, uint64_
 int svo_device_scene_counts(const svo_device_scene* scene, uint64_t* octree_nodes,
                             uint64_t* overlaps);
 void svo_device_scene_destroy(svo_device_scene* scene);
+/* Undoes svo_mm_insert_all: a fully resident incore pool (treelet g in slot
+ * g, num_slots slots of treelet_bytes, every sub-treelet attached by the
+ * patch of insertTreeletIntoIncoreBuffer, src/TreeletMemoryManager.cpp:
+ * 518-545) back into the treelets and headers of the treelet file
+ * (src/Treelet.cpp:403-419, src/Treelet.h:194-203).  SVO_ERR_INVALID on a
+ * pool that is not such a pool. */
+int svo_scene_from_pool(const svo_node* h_nodes, const svo_attrib* h_attribs, uint32_t num_slots,
+                        uint32_t treelet_bytes, uint32_t max_depth, uint64_t leaf_voxels,
+                        svo_scene** out);
 
 /* svo_scene_build_mesh / svo_device_scene_build_mesh with per-vertex normals
  * and colours (num_vertices x 3 floats each, colours in [0, 1]; both or
@@ -286,6 +295,15 @@ int svo_mm_create(const char* svo_path_base, uint64_t incore_bytes, void* stream
 /* Same, from an in-memory scene (copied; the scene stays owned by the caller). */
 int svo_mm_create_from_scene(const svo_scene* scene, uint64_t incore_bytes, void* stream,
                              svo_mm** out);
+/* A manager over a GPU-built octree whose incore buffer may be far smaller
+ * than the octree: the device pool is copied to host memory in pieces of
+ * about 256 MB and turned back into treelets and their headers (as
+ * svo_scene_from_pool), which become the manager's host copy, paged into an
+ * incore buffer of incore_bytes by insertion or the analysis pass like an
+ * octree read with svo_mm_create.  The device scene is left as it is.
+ * Blocking. */
+int svo_mm_create_from_device_scene(const svo_device_scene* scene, uint64_t incore_bytes,
+                                    void* stream, svo_mm** out);
 void svo_mm_destroy(svo_mm* mm);
 
 /* initClBuffer (src/TreeletMemoryManagerCl.cpp:101-113): allocates the
@@ -599,7 +617,10 @@ typedef struct svo_server_stats {
   uint64_t requests_done, rays_done, batches;
   uint64_t octree_loads, octree_evictions, treelets_paged_in, bytes_uploaded;
   uint64_t resident_bytes;
-  uint32_t resident_octrees, reserved;
+  uint32_t resident_octrees;
+  uint32_t paged_unconverged; /* paged requests cast after the last analysis
+                                 pass still placed treelets (region too small
+                                 for the view)                                */
 } svo_server_stats;
 
 typedef struct svo_server svo_server;

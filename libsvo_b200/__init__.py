@@ -427,6 +427,18 @@ class Scene:
         _check(_L.svo_scene_read(str(path_base).encode(), ctypes.byref(h)), "svo_scene_read")
         return cls(h.value)
 
+    @classmethod
+    def from_pool(cls, nodes: np.ndarray, attribs: np.ndarray, num_slots: int, treelet_bytes: int,
+                  max_depth: int, leaf_voxels: int = 0) -> "Scene":
+        """A fully resident incore pool (treelet g in slot g, as insertAll
+        leaves it) back into its treelets (svo_scene_from_pool)."""
+        n = np.ascontiguousarray(nodes, dtype=np.uint32)
+        a = np.ascontiguousarray(attribs, dtype=np.uint32)
+        h = ctypes.c_void_p()
+        _check(_L.svo_scene_from_pool(_np_ptr(n), _np_ptr(a), num_slots, treelet_bytes, max_depth, leaf_voxels,
+                                      ctypes.byref(h)), "svo_scene_from_pool")
+        return cls(h.value)
+
     def write(self, path_base: str):
         _check(_L.svo_scene_write(self._h, str(path_base).encode()), "svo_scene_write")
 
@@ -533,11 +545,16 @@ class TreeletMemoryManagerCuda:
     MAX_VISIBILITY = 8
 
     def __init__(self, scene_or_path, incore_bytes: int, stream=None):
+        """scene_or_path: a Scene, a DeviceScene (its pool turned back into
+        treelets, svo_mm_create_from_device_scene) or a treelet file base."""
         h = ctypes.c_void_p()
         sp = _stream_ptr(stream)
         if isinstance(scene_or_path, Scene):
             _check(_L.svo_mm_create_from_scene(scene_or_path._h, incore_bytes, sp, ctypes.byref(h)),
                    "svo_mm_create_from_scene")
+        elif isinstance(scene_or_path, DeviceScene):
+            _check(_L.svo_mm_create_from_device_scene(scene_or_path._h, incore_bytes, sp, ctypes.byref(h)),
+                   "svo_mm_create_from_device_scene")
         else:
             _check(_L.svo_mm_create(str(scene_or_path).encode(), incore_bytes, sp, ctypes.byref(h)),
                    "svo_mm_create")
@@ -875,7 +892,7 @@ class svo_server_stats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in ("requests_done", "rays_done", "batches", "octree_loads",
                                                 "octree_evictions", "treelets_paged_in",
                                                 "bytes_uploaded", "resident_bytes")] + \
-               [("resident_octrees", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+               [("resident_octrees", ctypes.c_uint32), ("paged_unconverged", ctypes.c_uint32)]
 
 
 for _name, (_args, _res) in {
@@ -883,6 +900,8 @@ for _name, (_args, _res) in {
     "svo_server_destroy": ([_vp], None),
     "svo_server_add_octree": ([_vp, _vp, _i32, _P(_u32)], ctypes.c_int),
     "svo_server_add_octree_paged": ([_vp, _vp, _i32, _u64, _P(_u32)], ctypes.c_int),
+    "svo_scene_from_pool": ([_vp, _vp, _u32, _u32, _u32, _u64, _P(_vp)], ctypes.c_int),
+    "svo_mm_create_from_device_scene": ([_vp, _u64, _vp, _P(_vp)], ctypes.c_int),
     "svo_server_set_upload_policy": ([_vp, _u32, _i32], ctypes.c_int),
     "svo_server_submit": ([_vp, _P(svo_request), _P(_u64)], ctypes.c_int),
     "svo_server_wait": ([_vp, _u64, _u32, _P(svo_request_result)], ctypes.c_int),

@@ -2,11 +2,14 @@
 //
 // Every entry point validates its arguments, turns C++ exceptions (allocation
 // failures) into status codes, and never terminates the process.
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <new>
 #include <string>
 #include <vector>
+#include <thread>
+#include <atomic>
 
 #include "../../include/libsvo_b200.h"
 #include "errors.h"
@@ -219,6 +222,73 @@ int svo_device_scene_counts(const svo_device_scene* scene, uint64_t* octree_node
 }
 
 void svo_device_scene_destroy(svo_device_scene* scene) { delete scene; }
+
+int svo_scene_from_pool(const svo_node* h_nodes, const svo_attrib* h_attribs, uint32_t num_slots,
+                        uint32_t treelet_bytes, uint32_t max_depth, uint64_t leaf_voxels,
+                        svo_scene** out) {
+  if (!out || !h_nodes || !h_attribs) return SVO_ERR_INVALID;
+  *out = nullptr;
+  return guarded([&] {
+    std::unique_ptr<svo_scene> s(new svo_scene);
+    const int rc = svo::scene_from_pool(h_nodes, h_attribs, num_slots, treelet_bytes, max_depth,
+                                        leaf_voxels, *s);
+    if (rc != SVO_OK) return rc;
+    *out = s.release();
+    return SVO_OK;
+  });
+}
+
+int svo_mm_create_from_device_scene(const svo_device_scene* scene, uint64_t incore_bytes, void* stream,
+                                    svo_mm** out) {
+  if (!out || !scene) return SVO_ERR_INVALID;
+  *out = nullptr;
+  return guarded([&] {
+    const svo::DeviceScene& d = scene->impl;
+    const uint64_t N = d.nodes_per_slot;
+    svo_scene s;
+    s.treelet_bytes = (uint32_t)(N * 8);
+    s.max_depth = d.depth;
+    s.leaf_voxels = d.leaf_voxels;
+    s.treelets.resize(d.num_treelets);
+    // the pool comes to the host in pieces of about 256 MB and is turned into
+    // treelets piece by piece: the host never holds a second copy of it
+    const uint64_t per = std::max<uint64_t>(1, (256ull << 20) / (N * sizeof(svo_node)));
+    std::vector<svo_node> hn(per * N);
+    std::vector<svo_attrib> ha(per * N);
+    cudaStream_t st = (cudaStream_t)stream;
+    for (uint64_t g0 = 0; g0 < d.num_treelets; g0 += per) {
+      const uint64_t k = std::min<uint64_t>(per, d.num_treelets - g0);
+      SVO_CUDA_TRY(cudaMemcpyAsync(hn.data(), d.d_nodes + g0 * N, k * N * sizeof(svo_node),
+                                   cudaMemcpyDeviceToHost, st));
+      SVO_CUDA_TRY(cudaMemcpyAsync(ha.data(), d.d_attribs + g0 * N, k * N * sizeof(svo_attrib),
+                                   cudaMemcpyDeviceToHost, st));
+      SVO_CUDA_TRY(cudaStreamSynchronize(st));
+      // slots are independent (a slot writes its own treelet and the headers
+      // of its sub-treelets, each of which has one parent): host threads
+      // take them in turn
+      std::atomic<uint64_t> next{0};
+      std::atomic<int> status{SVO_OK};
+      auto work = [&] {
+        for (uint64_t i = next.fetch_add(1); i < k; i = next.fetch_add(1)) {
+          const int rc = svo::unpatch_slot((uint32_t)(g0 + i), N, d.num_treelets, hn.data() + i * N,
+                                           ha.data() + i * N, s);
+          if (rc != SVO_OK) status.store(rc);
+        }
+      };
+      const unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+      std::vector<std::thread> pool;
+      for (unsigned t = 1; t < nt; ++t) pool.emplace_back(work);
+      work();
+      for (auto& th : pool) th.join();
+      if (status.load() != SVO_OK) return status.load();
+    }
+    std::unique_ptr<svo_mm> mm(new svo_mm(st));
+    const int rc = mm->impl.init(std::move(s), incore_bytes);
+    if (rc != SVO_OK) return rc;
+    *out = mm.release();
+    return SVO_OK;
+  });
+}
 
 int svo_scene_write(const svo_scene* scene, const char* path_base) {
   if (!scene || !path_base) return SVO_ERR_INVALID;

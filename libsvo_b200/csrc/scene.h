@@ -83,6 +83,16 @@ int read_scene(const std::string& base, svo_scene& s);
 int flatten_scene(const svo_scene& s, std::vector<svo_node>* nodes, std::vector<svo_attrib>* attribs,
                   uint64_t* count);
 
+// A fully resident incore pool (treelet g in slot g, sub-treelets attached)
+// back to the treelets and headers it was filled from (pool_scene.cpp).
+// unpatch_slot fills scene.treelets[g] from slot g's N records and the
+// headers of the sub-treelets that slot links to.
+int unpatch_slot(uint32_t g, uint64_t N, uint32_t num_slots, const svo_node* nodes,
+                 const svo_attrib* attribs, svo_scene& scene);
+int scene_from_pool(const svo_node* nodes, const svo_attrib* attribs, uint32_t num_slots,
+                    uint32_t treelet_bytes, uint32_t max_depth, uint64_t leaf_voxels,
+                    svo_scene& out);
+
 // Colour/normal packing (gloost's compressAsColor / compressAsNormal are not
 // part of the reference; these are the inverses of the kernel's unpacking,
 // opencl/treeletRenderer_rgba.cl:183-195, 388-404).
