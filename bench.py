@@ -52,7 +52,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the batched, served, large-shadowed and incore-update measurements")
-    ap.add_argument("--leg", choices=["batched", "served", "large_shadowed", "incore_update", "streaming", "flat"],
+    ap.add_argument("--leg", choices=["batched", "served", "large_shadowed", "incore_update", "streaming", "flat",
+                                      "large_streaming"],
                     help="run only this measurement on one GPU and print its result: the 64 terrain "
                          "views as one batched launch, the request server, the large shadowed "
                          "frame, the incore-update policies, the streaming loop on the icosphere "
@@ -63,6 +64,8 @@ def parse():
                          "primary + shadow frame) and print its result; the same as --leg large_shadowed")
     ap.add_argument("--large-subdivisions", type=int, default=9)
     ap.add_argument("--large-depth", type=int, default=14)
+    ap.add_argument("--legs-json", default=None,
+                    help="also write the full records of the extra measurements to this file")
     ap.add_argument("--shadow", action="store_true",
                     help="cast one shadow ray per hit as well (svo_mm_render_shadow, seeded light); "
                          "the metric then counts primary and shadow rays")
@@ -410,7 +413,8 @@ def served_leg(dev, n=400, rates=(4000, 16000, 64000)):
                 "p99_ms": float(np.percentile(lat, 99)), "launches": len({x.batch for x in r})}
         st = srv.stats()
         res["paging"] = {"octree_loads": st.octree_loads, "evictions": st.octree_evictions,
-                         "treelets_paged_in": st.treelets_paged_in, "gb_uploaded": st.bytes_uploaded / 1e9}
+                         "treelets_paged_in": st.treelets_paged_in, "gb_uploaded": st.bytes_uploaded / 1e9,
+                         "paged_unconverged": st.paged_unconverged}
         srv.close()
         return res
 
@@ -425,6 +429,14 @@ def served_leg(dev, n=400, rates=(4000, 16000, 64000)):
     paging_ungated = run(L.SERVE_PLAIN_STREAMED, footprint // 2, [16000], streams=8)
     paging_ungated_pinned = run(L.SERVE_PLAIN_STREAMED, footprint // 2, [16000], upload=L.UPLOAD_PINNED,
                                 streams=8)
+    # a budget below the largest octree's footprint: that octree is served by
+    # treelet paging in half the budget (svo_server_add_octree decides), the
+    # others page in and out whole under the rest
+    sizes = [16 * s.info.treelet_bytes // 8 * s.info.num_treelets for s in wl.scenes]
+    tp_budget = int(0.9 * max(sizes))
+    treelet_paged = {"budget_gb": tp_budget / 1e9, "largest_octree_gb": max(sizes) / 1e9,
+                     "batched": run(L.SERVE_BATCHED, tp_budget, [16000]),
+                     "plain_ungated": run(L.SERVE_PLAIN_STREAMED, tp_budget, [16000], streams=8)}
     keys = [k for k in batched if k != "paging"]
     return {"workload": wl.name, "description": wl.description, "requests": n, "rays": rays,
             "scene_build_s": round(build_s, 2), "octree_footprint_gb": footprint / 1e9,
@@ -435,7 +447,8 @@ def served_leg(dev, n=400, rates=(4000, 16000, 64000)):
             "speedup_vs_plain_one_stream": {k: batched[k]["mrays_s"] / plain[k]["mrays_s"] for k in keys},
             "paging_half_budget": {"batched": paging, "batched_pinned_hosts": paging_pinned,
                                    "plain_ungated": paging_ungated,
-                                   "plain_ungated_pinned_hosts": paging_ungated_pinned}}
+                                   "plain_ungated_pinned_hosts": paging_ungated_pinned},
+            "treelet_paged": treelet_paged}
 
 
 def incore_update_leg(dev, scene, incore_mb=256, frames=20, seed=5):
@@ -734,6 +747,158 @@ def large_shadow_leg(dev, reps=10, cap_gb=60.0, subdivisions=9, depth=14, cpu_ba
     return out
 
 
+def _r(x, nd=3):
+    """x rounded to `nd` significant digits (None stays None)."""
+    if x is None or isinstance(x, (bool, str)):
+        return x
+    if x == 0:
+        return 0
+    return float(f"{x:.{nd}g}")
+
+
+def summarize_legs(legs: dict) -> dict:
+    """The extra measurements as short summary numbers (Mrays/s, ms, Hz;
+    full records with --legs-json)."""
+    out = {}
+    for key, v in legs.items():
+        if "error" in v:
+            out[key] = {"error": v["error"][:120]}
+            continue
+        if key == "flat":
+            out[key] = {"mrays_s": _r(v["mrays_s"]), "frac": _r(v["roofline"]["frac"]),
+                        "cpu_mrays_s": _r(v.get("cpu_baseline", {}).get("value"))}
+        elif key == "batched":
+            out[key] = {"per_view_mrays_s": _r(v["per_view_launches_mrays_s"]),
+                        "batched_mrays_s": _r(v["batched_mrays_s"]), "speedup": _r(v["speedup"]),
+                        "tile": v["autotuned"]["tile"], "threads": v["autotuned"]["block_threads"]}
+        elif key == "served":
+            rates = {}
+            for k in v["speedup_vs_plain_ungated"]:
+                b, u = v["batched"][k], v["plain_ungated"][k]
+                rates[k] = {"batched": [_r(b["mrays_s"]), _r(b["p50_ms"]), _r(b["p99_ms"])],
+                            "plain_ungated": [_r(u["mrays_s"]), _r(u["p50_ms"]), _r(u["p99_ms"])],
+                            "x": _r(v["speedup_vs_plain_ungated"][k])}
+            pg = {}
+            for k, r in v["paging_half_budget"].items():
+                q = r["16000"]
+                pg[k] = [_r(q["mrays_s"]), _r(q["p50_ms"]), _r(q["p99_ms"])]
+            out[key] = {"cols": "Mrays/s, p50 ms, p99 ms", "rates": rates, "half_budget_16000": pg}
+            if "treelet_paged" in v:
+                t = v["treelet_paged"]
+                out[key]["treelet_paged_16000"] = {
+                    k: [_r(t[k]["16000"]["mrays_s"]), _r(t[k]["16000"]["p50_ms"]), _r(t[k]["16000"]["p99_ms"]),
+                        t[k]["paging"]["paged_unconverged"]]
+                    for k in ("batched", "plain_ungated") if k in t}
+        elif key == "large_shadowed":
+            out[key] = {"mrays_s": _r(v["mrays_s"]), "ms": _r(v["ms_per_frame"]),
+                        "frac": _r(v["roofline"]["frac"]),
+                        "cpu_mrays_s": _r(v.get("cpu_baseline", {}).get("value")),
+                        "parity_mismatched": v.get("parity", {}).get("mismatched")}
+        elif key == "large_streaming":
+            cp = v["converged_parity"]
+            out[key] = {"cap_gb": v["residency_cap_gb"], "hz": _r(v["hz_mean"]), "p50_ms": _r(v["ms_p50"]),
+                        "p99_ms": _r(v["ms_p99"]), "gb_paged": _r(v["gb_paged_in"]),
+                        "parity_mismatched": cp["mismatched"], "converged": cp["converged"]}
+        elif key == "incore_update":
+            out[key] = {k: _r(r["ms_mean"]) for k, r in v.items() if isinstance(r, dict) and "ms_mean" in r}
+        elif key == "streaming":
+            out[key] = {k: {"hz": _r(r["hz_mean"]), "p99_ms": _r(r["ms_p99"])}
+                        for k, r in v.items() if isinstance(r, dict)}
+        else:
+            out[key] = {k: _r(x) for k, x in v.items() if isinstance(x, (int, float))}
+    return out
+
+
+def large_streaming_leg(dev, cap_gb=16.0, frames=60, subdivisions=9, depth=14, upload="pinned"):
+    """The large shadowed workload under a residency cap: the depth-14
+    icosphere built on the GPU, its pool turned back into treelets on the host
+    (svo_mm_create_from_device_scene), and 3840x2160 primary + shadow frames
+    cast through a manager whose incore buffer (nodes and attributes) holds
+    cap_gb -- well below the 40 GB pool.  Each frame runs the analysis pass at
+    1/8 resolution with a jittered far plane (the reference's dynamic loading:
+    treelets paged in by visibility, evicted when the buffer is full) and
+    then the frame; the camera moves in along the orbit from radius 2.5 to
+    1.2.  Then the last view is converged by analysis passes at full
+    resolution and its primary-ray frame compared with the same frame over the
+    fully resident pool (RGBA8 and, per ray, hit, depth, t and loop count;
+    node indices differ between the two pools)."""
+    import torch
+
+    import libsvo_b200 as L
+    from libsvo_b200 import scenes as S
+
+    t0 = time.perf_counter()
+    wl = S.large_shadowed(subdivisions=subdivisions, depth=depth)
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    info = wl.scene.info
+    slot_bytes = 2 * info.treelet_bytes
+    incore = int(cap_gb * 1e9) // slot_bytes * info.treelet_bytes  # node pool; attributes as much again
+    t0 = time.perf_counter()
+    s = torch.cuda.current_stream()
+    mm = L.TreeletMemoryManagerCuda(wl.scene, incore, stream=s)
+    host_s = time.perf_counter() - t0
+    if upload == "pinned":
+        mm.setUploadPolicy(L.UPLOAD_PINNED)
+    mm.initDeviceBuffer()
+    cfg = L.trace_cfg(L.TRAVERSAL_TREELET, wl.stack_size)
+    sc = L.shadow_cfg(wl.light)
+    cam = wl.camera
+    out = torch.empty((cam.height, cam.width), dtype=torch.int32, device=dev)
+    rng = np.random.default_rng(7)
+    ms, placed = [], 0
+    for f in range(frames):
+        r = 2.5 - 1.3 * f / max(1, frames - 1)
+        p = S.orbit_pose(r, 40.0 + 3.0 * f, 15.0, cam.width, cam.height, 25.0).frame_params()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        new, _ = mm.performAnalysePass(p, divisor=8, jitter=tuple(rng.uniform(-1, 1, 2)),
+                                       stack_size=wl.stack_size, stream=s)
+        mm.render_shadow(p, out, sc, cfg=cfg, stream=s)
+        s.synchronize()
+        ms.append((time.perf_counter() - t1) * 1e3)
+        placed += new
+    st = mm.sync(s)
+    steady = ms[5:]
+    primary = cam.width * cam.height
+    res = {"workload": wl.name + "_streamed", "scene_build_s": round(build_s, 2),
+           "host_treelets_s": round(host_s, 2), "pool_gb": 16 * info.num_treelets * info.nodes_per_treelet / 1e9,
+           "residency_cap_gb": cap_gb, "slots": mm.info.num_slots, "treelets": int(info.num_treelets),
+           "upload": upload, "frames": frames, "hz_mean": 1e3 / statistics.mean(steady),
+           "ms_p50": statistics.median(steady), "ms_p99": float(np.percentile(steady, 99)),
+           "ms_first": ms[0], "treelets_paged_in": placed,
+           "gb_paged_in": placed * slot_bytes / 1e9, "primary_mrays_s_mean": primary / statistics.mean(steady) / 1e3,
+           "capped_rays": st.capped_rays, "bounds_errors": st.bounds_errors}
+    # converged view: full-resolution analysis passes until nothing new is placed
+    steps, new = 0, 1
+    while new and steps < 80:
+        new, _ = mm.performAnalysePass(p, divisor=1, stack_size=wl.stack_size, stream=s)
+        steps += 1
+    hb = torch.empty(primary * 16, dtype=torch.uint8, device=dev)
+    mm.render(p, out, hb, cfg=cfg, stream=s)
+    s.synchronize()
+    got_rgba = out.cpu().numpy().view(np.uint32).copy()
+    got = hb.cpu().numpy().view(L.HIT_DTYPE).copy()
+    mm.close()
+    d_nodes, d_attribs, n = wl.scene.buffers()
+    L.render(d_nodes, d_attribs, n, p, out, hb, cfg=cfg, stream=s)
+    s.synchronize()
+    want = hb.cpu().numpy().view(L.HIT_DTYPE)
+    bad = np.zeros(primary, dtype=bool)
+    for k in ("hit", "depth", "loops"):
+        bad |= got[k] != want[k]
+    bad |= got["t"].view(np.uint32) != want["t"].view(np.uint32)
+    res["converged_parity"] = {"view": "the last frame's camera (radius 1.2), primary rays", "analysis_passes": steps,
+                               "converged": new == 0, "pixels": primary,
+                               "mismatched_rgba": int((got_rgba.reshape(-1) != out.cpu().numpy().view(np.uint32).reshape(-1)).sum()),
+                               "mismatched_rays": int(bad.sum())}
+    res["converged_parity"]["mismatched"] = (res["converged_parity"]["mismatched_rgba"]
+                                             + res["converged_parity"]["mismatched_rays"])
+    del hb, out
+    wl.scene.close()
+    return res
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -764,7 +929,9 @@ def main():
                                                            cpu_baseline=not args.no_cpu_baseline),
                 "incore_update": lambda: incore_update_leg(dev, make_workload("icosphere").scene),
                 "streaming": lambda: streaming_leg(dev, make_workload("icosphere").scene),
-                "flat": lambda: flat_leg(dev, cpu_baseline=not args.no_cpu_baseline)}
+                "flat": lambda: flat_leg(dev, cpu_baseline=not args.no_cpu_baseline),
+                "large_streaming": lambda: large_streaming_leg(dev, subdivisions=args.large_subdivisions,
+                                                               depth=args.large_depth)}
         print(json.dumps({"leg": args.leg, **legs[args.leg]()}), flush=True)
         return
     if world > 1:
@@ -929,21 +1096,29 @@ def main():
                                               light=L.seeded_light(1) if shadow else None,
                                               gpu_shadow_hits=p_shadow, config=line["config"]["workload"])
         mm.close()
+        legs = {}
         if world == 1 and not args.no_extra and args.workload == "icosphere":
             for key, leg in (("incore_update", incore_update_leg), ("streaming", streaming_leg)):
                 try:
-                    line[key] = leg(dev, wl.scene)
+                    legs[key] = leg(dev, wl.scene)
                 except Exception as e:  # a failing extra leg must not lose the primary line
-                    line[key] = {"error": f"{type(e).__name__}: {e}"}
+                    legs[key] = {"error": f"{type(e).__name__}: {e}"}
         if world == 1 and not args.no_extra:
-            legs = (("flat", lambda d: flat_leg(d, cpu_baseline=not args.no_cpu_baseline)),
-                    ("batched", batched_leg), ("served", served_leg),
-                    ("large_shadowed", lambda d: large_shadow_leg(d, cpu_baseline=not args.no_cpu_baseline)))
-            for key, leg in legs:
+            extra = (("flat", lambda d: flat_leg(d, cpu_baseline=not args.no_cpu_baseline)),
+                     ("batched", batched_leg), ("served", served_leg),
+                     ("large_shadowed", lambda d: large_shadow_leg(d, cpu_baseline=not args.no_cpu_baseline)),
+                     ("large_streaming", large_streaming_leg))
+            for key, leg in extra:
                 try:
-                    line[key] = leg(dev)
+                    legs[key] = leg(dev)
                 except Exception as e:  # a failing extra leg must not lose the primary line
-                    line[key] = {"error": f"{type(e).__name__}: {e}"}
+                    legs[key] = {"error": f"{type(e).__name__}: {e}"}
+        if legs:
+            if args.legs_json:
+                Path(args.legs_json).write_text(json.dumps(legs, indent=1))
+            # the compact summary goes last, so that a reader keeping only the
+            # end of the line still sees every leg
+            line["legs"] = summarize_legs(legs)
         print(json.dumps(line), flush=True)
     mm.close()
     if world > 1:

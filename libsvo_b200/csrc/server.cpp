@@ -297,10 +297,15 @@ void paged_worker_loop(svo_server* s, uint32_t id) {
     }
     uint32_t placed = 0;
     int rc = SVO_OK;
+    bool converged = false;
     for (uint32_t step = 0; step < kMaxPagingSteps; ++step) {
       uint32_t nw = 0, old = 0;
       rc = mm->analysis_step(r.params, 1, 0.0f, 0.0f, S, w->stream, &nw, &old);
-      if (rc != SVO_OK || nw == 0) break;
+      if (rc != SVO_OK) break;
+      if (nw == 0) {
+        converged = true;
+        break;
+      }
       placed += nw;
     }
     if (rc == SVO_OK) rc = mm->wait_uploads(w->stream);
@@ -319,6 +324,7 @@ void paged_worker_loop(svo_server* s, uint32_t id) {
     s->stats.rays_done += (uint64_t)r.params.width * r.params.height;
     s->stats.treelets_paged_in += placed;
     s->stats.bytes_uploaded += placed * slot_bytes;
+    if (rc == SVO_OK && !converged) s->stats.paged_unconverged++;
     s->cv_user.notify_all();
   }
 }
