@@ -9,13 +9,15 @@ configurations name:
                    from a seeded camera outside the cube, 60 degree fov.
 * ``icosphere`` -- icosphere subdivided 6 times (81,920 triangles), radius
                    0.4 displaced radially by 3-octave value noise of amplitude
-                   0.05, depth-11 octree cut into 6-level treelets, leaf normal
-                   and colour interpolated from seeded per-vertex attributes as
-                   the reference's attribute generator does; one 1920x1080 view
-                   from an orbit of radius
-                   2.5.  The configuration names no field of view; 25 degrees
-                   (vertical) makes the sphere fill the frame height, so most
-                   rays enter the octree.
+                   0.05, depth-11 octree cut into 6-level treelets, leaf colour
+                   from the face normal (colour = normal * 0.5 + 0.5 of the
+                   normalised sum of the overlapping faces' normals, as the
+                   configuration asks; ``colour="vertex"`` interpolates seeded
+                   per-vertex attributes as the reference's attribute
+                   generator does instead); one 1920x1080 view from an orbit of
+                   radius 2.5.  The configuration names no field of view; 25
+                   degrees (vertical) makes the sphere fill the frame height, so
+                   most rays enter the octree.
 * ``terrain``   -- 1024 x 1024 height-field grid (2,093,058 triangles), heights
                    from 6-octave fBm in [-0.45, -0.15] (0.3 of the extent),
                    depth-12 octree cut into 6-level treelets; 64 square views
@@ -68,16 +70,20 @@ def orbit_pose(radius: float, angle_deg: float, elevation_deg: float, width: int
 
 
 def icosphere(subdivisions=6, depth=11, treelet_levels=6, seed=1, width=1920, height=1080,
-              fov_deg=25.0, radius=2.5) -> Workload:
+              fov_deg=25.0, radius=2.5, colour="face") -> Workload:
     v, t = icosphere_mesh(subdivisions, radius=0.4, octaves=3, amplitude=0.05, frequency=2.0, seed=seed)
-    n, c = vertex_attributes(v, t, seed)
-    scene = Scene.from_mesh(v, t, depth, treelet_levels=treelet_levels, normals=n, colors=c)
+    if colour == "face":
+        scene = Scene.from_mesh(v, t, depth, treelet_levels=treelet_levels)
+    else:
+        n, c = vertex_attributes(v, t, seed)
+        scene = Scene.from_mesh(v, t, depth, treelet_levels=treelet_levels, normals=n, colors=c)
     rng = np.random.default_rng(seed)
     cam = orbit_pose(radius, float(rng.uniform(0, 360)), float(rng.uniform(-30, 30)), width, height,
                      fov_deg)
     return Workload(f"icosphere_s{subdivisions}_d{depth}_{width}x{height}", scene, [cam],
                     description=f"icosphere {subdivisions}x subdivided ({t.shape[0]} triangles), 3-octave "
-                                f"noise 0.05, depth {depth}, {treelet_levels}-level treelets, {width}x{height}, "
+                                f"noise 0.05, depth {depth}, {treelet_levels}-level treelets, colour from the "
+                                f"{'face normal' if colour == 'face' else 'vertex attributes'}, {width}x{height}, "
                                 f"orbit radius {radius}, fov {fov_deg}")
 
 

@@ -64,7 +64,7 @@ def test_rendering_the_device_pool(cuda):
 
     from libsvo_b200 import scenes
 
-    wl = scenes.icosphere(subdivisions=4, depth=9, treelet_levels=5, width=320, height=200)
+    wl = scenes.icosphere(subdivisions=4, depth=9, treelet_levels=5, width=320, height=200, colour="vertex")
     v, t = L.icosphere(4)  # the mesh scenes.icosphere builds, with its vertex attributes
     vn, vc = L.vertex_attributes(v, t, 1)
     ds = L.DeviceScene(v, t, 9, treelet_levels=5, normals=vn, colors=vc)
