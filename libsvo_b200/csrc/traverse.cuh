@@ -110,6 +110,17 @@ struct StagedFetch {
   }
 };
 
+// A saved traversal state for the cycle search of long rays (descend):
+// frame node, scale and tMin bits, the stacked frames, and the loop and fetch
+// counts when it was saved.  Lives in local memory; only rays that run
+// kCycleFrom iterations or more touch it (volatile keeps every field in
+// local memory, so the hot loop's registers are not spent on it).
+constexpr uint32_t kCycleFrom = 64;
+struct CycleMark {
+  uint32_t node, scale, tmin, loops, fetches, next_save;
+  uint32_t stack[2 * kMaxStack];  // {node, tMax bits} per stacked frame
+};
+
 // The descent loop.  kFlat selects the CpuRaycasterSingleRay3 rules; S is
 // the stack size (treelet) or the octree depth (flat).  `stack` points at
 // this thread's column of the shared-memory stack, `stride` words apart.
@@ -148,27 +159,82 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
   bool in_pool = num_nodes > 0u;
   uint2 nd = in_pool ? fetch(0u) : make_uint2(0u, 0u);
   uint32_t loops = 0u, fetches = 0u;
+  // pools hold at most 2^32 nodes, so the in-pool test of a 32-bit index is
+  // one 32-bit compare against the last index
+  const uint32_t last_node = num_nodes ? (uint32_t)(num_nodes - 1u) : 0u;
+  uint2* sp = stack;  // the next free stack word: level S-1-scale
+  // Iterations from kCycleFrom on take the cold path below, which looks for
+  // a repeating state; before that only the watchdog's test runs.
+  uint32_t check_at = max_loops < kCycleFrom ? max_loops : kCycleFrom;
+  volatile CycleMark mark;
+
+  auto capped = [&]() {
+    h.flags = SVO_HITFLAG_CAPPED;
+    h.loops = loops;
+    h.fetches = fetches;
+    if (!kFlat) {  // sample() reports the current node as a hit (:268-277)
+      h.hit = 1u;
+      h.node = node;
+      h.depth = (uint32_t)(S - scale);
+      h.t = tmin;
+      h.cx = cx;
+      h.cy = cy;
+      h.cz = cz;
+      // quality = scale_exp2 - tScaleRatio * tMin, as for a leaf
+      h.tc_min = tmin;
+      h.sx2 = sx2;
+      h.leaf = 1u;
+    }
+  };
 
   for (;;) {  // ends by a return, or by a pop above the root
     ++loops;
-    if (loops == max_loops) {
-      h.flags = SVO_HITFLAG_CAPPED;
-      h.loops = loops;
-      h.fetches = fetches;
-      if (!kFlat) {  // sample() reports the current node as a hit (:268-277)
-        h.hit = 1u;
-        h.node = node;
-        h.depth = (uint32_t)(S - scale);
-        h.t = tmin;
-        h.cx = cx;
-        h.cy = cy;
-        h.cz = cz;
-        // quality = scale_exp2 - tScaleRatio * tMin, as for a leaf
-        h.tc_min = tmin;
-        h.sx2 = sx2;
-        h.leaf = 1u;
+    if (loops >= check_at) {
+      if (loops == max_loops) {
+        capped();
+        return;
       }
-      return;
+      // Cold path (long rays only).  The state at the start of an iteration
+      // is the frame's node, scale and tMin and the stacked frames: a frame's
+      // tMax depends only on its box and the ray, and the box on the nodes
+      // stacked above it.  Once that state recurs, the ray repeats the same
+      // iterations with period p until the watchdog, so whole periods are
+      // skipped (loop and fetch counts advanced by them) and the iterations
+      // left run as usual: the watchdog then stops the ray in the state, and
+      // with the counts, the reference reaches.  States are saved at
+      // iterations kCycleFrom, 2 kCycleFrom, 4 kCycleFrom, ... (Brent's cycle
+      // search) and compared with every later iteration.
+      check_at = loops + 1u;
+      const uint32_t depth = (uint32_t)(S - 1 - scale);
+      bool same = loops > kCycleFrom && mark.node == node && mark.scale == (uint32_t)scale &&
+                  mark.tmin == __float_as_uint(tmin);
+      for (uint32_t j = 0; same && j < depth; ++j) {
+        const uint2 a = stack[j * stride];
+        same = a.x == mark.stack[2 * j] && a.y == mark.stack[2 * j + 1];
+      }
+      if (same) {
+        const uint32_t period = loops - mark.loops;
+        const uint32_t skip = (max_loops - loops) / period;
+        fetches += skip * (fetches - mark.fetches);
+        loops += skip * period;
+        check_at = max_loops;
+        if (loops == max_loops) {
+          capped();
+          return;
+        }
+      } else if (loops == kCycleFrom || loops == mark.next_save) {
+        mark.node = node;
+        mark.scale = (uint32_t)scale;
+        mark.tmin = __float_as_uint(tmin);
+        mark.loops = loops;
+        mark.fetches = fetches;
+        mark.next_save = 2u * loops;
+        for (uint32_t j = 0; j < depth; ++j) {
+          const uint2 a = stack[j * stride];
+          mark.stack[2 * j] = a.x;
+          mark.stack[2 * j + 1] = a.y;
+        }
+      }
     }
     bool pop;
     if (kFlat)
@@ -178,7 +244,8 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
     if (pop) {
       ++scale;
       if (scale >= S) break;
-      const uint2 e = stack[(S - 1 - scale) * stride];
+      sp -= stride;
+      const uint2 e = *sp;
       tmin = tmax;
       node = e.x;
       tmax = __uint_as_float(e.y);
@@ -296,10 +363,11 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
         return;
       }
       // push: the current frame's tMin becomes tc_max (recovered on pop)
-      stack[(S - 1 - scale) * stride] = make_uint2(node, __float_as_uint(tmax));
+      *sp = make_uint2(node, __float_as_uint(tmax));
+      sp += stride;
       --scale;
       node = child;
-      in_pool = (uint64_t)node < num_nodes;
+      in_pool = node <= last_node;
       if (in_pool) nd = fetch(node);
       tmin = tc_min;
       tmax = tc_max;

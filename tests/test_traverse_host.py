@@ -91,3 +91,25 @@ def test_icosphere_frame(host_lib):
     p = wl.cameras[0].frame_params()
     o, d = oracle.pixel_rays(bytes(p))
     check(host_lib, nodes, o, d, p.t_scale_ratio)
+
+
+def test_long_and_watchdog_rays(host_lib):
+    """Rays of 64 iterations and more take the cold path that looks for a
+    repeating traversal state and skips whole periods up to the watchdog:
+    every long ray of a 960x540 icosphere frame (one of them capped at
+    (S+1)^2*5 iterations) must still match the oracle in node, t, depth,
+    flags, loop and fetch counts."""
+    from libsvo_b200 import scenes
+
+    wl = scenes.icosphere(subdivisions=5, depth=9, treelet_levels=4, width=960, height=540)
+    info = wl.scene.info
+    mm = L.TreeletMemoryManagerCuda(wl.scene, info.treelet_bytes * info.num_treelets)
+    mm.insertAll()
+    nodes, _ = mm.getIncoreBuffer()
+    p = wl.cameras[0].frame_params()
+    o, d = oracle.pixel_rays(bytes(p))
+    want, _ = oracle.cast_rays(nodes, o, d, p.t_scale_ratio)
+    long_rays = np.nonzero(want["loops"] >= 60)[0]
+    assert long_rays.size > 1000 and (want["flags"][long_rays] & L.HITFLAG_CAPPED).sum() >= 1
+    got = check(host_lib, nodes, o[long_rays], d[long_rays], p.t_scale_ratio)
+    assert (got["flags"] & L.HITFLAG_CAPPED).sum() == (want["flags"][long_rays] & L.HITFLAG_CAPPED).sum()
