@@ -720,9 +720,10 @@ int TreeletMemoryManagerCuda::feedback_scratch(uint64_t records, svo_feedback** 
 int TreeletMemoryManagerCuda::analysis_step(const svo_frame_params& frame, uint32_t divisor,
                                             float jitter_x, float jitter_y, int32_t stack_size,
                                             cudaStream_t stream, uint32_t* num_new,
-                                            uint32_t* num_old) {
+                                            uint32_t* num_old, uint32_t* num_requested) {
   if (num_new) *num_new = 0;
   if (num_old) *num_old = 0;
+  if (num_requested) *num_requested = 0;
   if (divisor == 0 || !device_ready()) return SVO_ERR_INVALID;
   if (stack_size < 2 || stack_size > 24) return SVO_ERR_RANGE;
   cudaStream_t s = stream ? stream : render_stream_;
@@ -752,6 +753,7 @@ int TreeletMemoryManagerCuda::analysis_step(const svo_frame_params& frame, uint3
   rc = analyse_feedback_device(d_fb, n, default_max_new_treelets(), nw, old, s);
   if (num_new) *num_new = (uint32_t)nw.size();
   if (num_old) *num_old = (uint32_t)old.size();
+  if (num_requested) *num_requested = (uint32_t)nw.size();
   if (rc != SVO_OK) return rc;
   std::vector<int32_t> ng(nw.size()), og(old.size());
   std::vector<float> ne(nw.size());

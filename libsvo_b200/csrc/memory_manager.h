@@ -164,10 +164,12 @@ class TreeletMemoryManagerCuda : public TreeletMemoryManager {
   // (jitter_x, jitter_y) * divisor / 2 frame pixels, the records analysed on
   // the GPU, treelets inserted (new ones that find no slot are skipped, as
   // the reference ignores its insertion results) and the dirty slots
-  // uploaded.  *num_new: treelets placed; *num_old: visible resident ones.
+  // uploaded.  *num_new: treelets placed; *num_old: visible resident ones;
+  // *num_requested (optional): newly visible treelets the pass asked for,
+  // placed or not (0 once the view needs nothing that is not resident).
   int analysis_step(const svo_frame_params& frame, uint32_t divisor, float jitter_x,
                     float jitter_y, int32_t stack_size, cudaStream_t stream, uint32_t* num_new,
-                    uint32_t* num_old);
+                    uint32_t* num_old, uint32_t* num_requested = nullptr);
 
  private:
   int init_analysis();

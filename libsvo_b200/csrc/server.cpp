@@ -128,7 +128,7 @@ struct ServedOctree {
 
 // Analysis passes before a paged request gives up converging and renders
 // with what is resident.
-constexpr uint32_t kMaxPagingSteps = 48;
+constexpr uint32_t kMaxPagingSteps = 64;
 
 struct Request {
   svo_request r{};
@@ -299,14 +299,18 @@ void paged_worker_loop(svo_server* s, uint32_t id) {
     int rc = SVO_OK;
     bool converged = false;
     for (uint32_t step = 0; step < kMaxPagingSteps; ++step) {
-      uint32_t nw = 0, old = 0;
-      rc = mm->analysis_step(r.params, 1, 0.0f, 0.0f, S, w->stream, &nw, &old);
+      // converged when the pass asks for nothing new; a pass may also place
+      // nothing because the region is full of treelets still marked visible
+      // from earlier views, whose visibility runs down pass by pass until
+      // they can be evicted
+      uint32_t nw = 0, old = 0, asked = 0;
+      rc = mm->analysis_step(r.params, 1, 0.0f, 0.0f, S, w->stream, &nw, &old, &asked);
       if (rc != SVO_OK) break;
-      if (nw == 0) {
+      placed += nw;
+      if (asked == 0) {
         converged = true;
         break;
       }
-      placed += nw;
     }
     if (rc == SVO_OK) rc = mm->wait_uploads(w->stream);
     if (rc == SVO_OK) {

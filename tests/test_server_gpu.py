@@ -123,20 +123,21 @@ def test_cancel_wait_timeout_and_errors(workload, cuda):
 
 def test_octree_larger_than_the_budget_is_paged(workload, cuda):
     """An octree whose pools exceed the whole budget is no longer refused: it
-    is served by treelet paging in half the budget, and a distant view (few
-    treelets at its level of detail) converges to the fully resident image."""
+    is served by treelet paging in half the budget (a quarter of the octree's
+    treelets), and close views of a small patch of it converge to the fully
+    resident image."""
     import torch
 
     scene = workload.scenes[2]
     srv = L.Server(L.server_cfg(footprint(scene) // 2, streams=2))
     oid = srv.add_octree(scene)
-    cams = [L.orbit_camera(k, 96, 64, radius=2.4) for k in range(3)]
+    cams = [L.orbit_camera(k, 96, 64, radius=0.75, fov_deg=20.0) for k in range(3)]
     outs = [torch.full((c.height, c.width), -1, dtype=torch.int32, device=cuda) for c in cams]
     res = srv.replay([L.request(oid, c.frame_params(), t) for c, t in zip(cams, outs)], np.zeros(len(cams)),
                      timeout_ms=60000)
     assert all(r.status == L.SVO_OK for r in res)
     st = srv.stats()
-    assert st.treelets_paged_in > 0 and st.octree_loads == 0
+    assert st.treelets_paged_in > 0 and st.octree_loads == 0 and st.paged_unconverged == 0
     torch.cuda.synchronize()
     for c, t in zip(cams, outs):
         assert np.array_equal(t.cpu().numpy(), alone(scene, c, cuda))
@@ -166,7 +167,7 @@ def test_treelet_paged_octree_same_alone_and_in_the_mix(workload, cuda, mode):
     res = srv.replay(rq, S.poisson_arrivals(len(rq), 1000.0, seed=2), timeout_ms=60000)
     assert all(r.status == L.SVO_OK for r in res)
     st = srv.stats()
-    assert st.requests_done == len(rq) and st.treelets_paged_in > 0
+    assert st.requests_done == len(rq) and st.treelets_paged_in > 0 and st.paged_unconverged == 0
     torch.cuda.synchronize()
     for (o, cam), t in zip(reqs, outs):
         assert np.array_equal(t.cpu().numpy(), alone(workload.scenes[o], cam, cuda)), f"octree {o}"
