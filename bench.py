@@ -404,13 +404,22 @@ def served_leg(dev, n=400, rates=(4000, 16000, 64000)):
         srv.replay(rq[:64], np.zeros(64), timeout_ms=120000)  # first loads
         res = {}
         for rate in rate_list:
+            t_run = time.perf_counter()
             arr = S.poisson_arrivals(n, rate, seed=11) if rate else np.zeros(n)
-            r = srv.replay(rq, arr, timeout_ms=120000)
-            lat = np.array([x.done_s - x.submit_s for x in r]) * 1e3
-            span = max(x.done_s for x in r) - min(x.submit_s for x in r)
+            try:
+                r = srv.replay(rq, arr, timeout_ms=60000)
+            except L.SvoError:  # some requests failed: their results carry the status
+                r = srv.last_replay_results
+            ok = [x for x in r if x.status == L.SVO_OK]
+            served_rays = sum(q.params.width * q.params.height for q, x in zip(rq, r) if x.status == L.SVO_OK)
+            lat = np.array([x.done_s - x.submit_s for x in ok]) * 1e3 if ok else np.zeros(1)
+            span = (max(x.done_s for x in ok) - min(x.submit_s for x in r)) if ok else float("inf")
             res[str(rate) if rate else "burst"] = {
-                "mrays_s": rays / span / 1e6, "p50_ms": float(np.percentile(lat, 50)),
-                "p99_ms": float(np.percentile(lat, 99)), "launches": len({x.batch for x in r})}
+                "mrays_s": served_rays / span / 1e6, "p50_ms": float(np.percentile(lat, 50)),
+                "p99_ms": float(np.percentile(lat, 99)), "launches": len({x.batch for x in ok}),
+                "failed": len(r) - len(ok)}
+            print(f"[bench] served mode {mode} budget {budget / 1e9:.2f} GB rate {rate}: "
+                  f"{time.perf_counter() - t_run:.1f} s", file=sys.stderr, flush=True)
         st = srv.stats()
         res["paging"] = {"octree_loads": st.octree_loads, "evictions": st.octree_evictions,
                          "treelets_paged_in": st.treelets_paged_in, "gb_uploaded": st.bytes_uploaded / 1e9,
@@ -429,9 +438,10 @@ def served_leg(dev, n=400, rates=(4000, 16000, 64000)):
     paging_ungated = run(L.SERVE_PLAIN_STREAMED, footprint // 2, [16000], streams=8)
     paging_ungated_pinned = run(L.SERVE_PLAIN_STREAMED, footprint // 2, [16000], upload=L.UPLOAD_PINNED,
                                 streams=8)
-    # a budget below the largest octree's footprint: that octree is served by
-    # treelet paging in half the budget (svo_server_add_octree decides), the
-    # others page in and out whole under the rest
+    # a budget below the largest octree's footprint: octrees taking more than
+    # half of it (the two largest) are served by treelet paging, each in a
+    # quarter of the budget (svo_server_add_octree decides), the others page
+    # in and out whole under the rest
     sizes = [16 * s.info.treelet_bytes // 8 * s.info.num_treelets for s in wl.scenes]
     tp_budget = int(0.9 * max(sizes))
     treelet_paged = {"budget_gb": tp_budget / 1e9, "largest_octree_gb": max(sizes) / 1e9,
@@ -1099,20 +1109,24 @@ def main():
         legs = {}
         if world == 1 and not args.no_extra and args.workload == "icosphere":
             for key, leg in (("incore_update", incore_update_leg), ("streaming", streaming_leg)):
+                t_leg = time.perf_counter()
                 try:
                     legs[key] = leg(dev, wl.scene)
                 except Exception as e:  # a failing extra leg must not lose the primary line
                     legs[key] = {"error": f"{type(e).__name__}: {e}"}
+                print(f"[bench] leg {key}: {time.perf_counter() - t_leg:.1f} s", file=sys.stderr, flush=True)
         if world == 1 and not args.no_extra:
             extra = (("flat", lambda d: flat_leg(d, cpu_baseline=not args.no_cpu_baseline)),
                      ("batched", batched_leg), ("served", served_leg),
                      ("large_shadowed", lambda d: large_shadow_leg(d, cpu_baseline=not args.no_cpu_baseline)),
                      ("large_streaming", large_streaming_leg))
             for key, leg in extra:
+                t_leg = time.perf_counter()
                 try:
                     legs[key] = leg(dev)
                 except Exception as e:  # a failing extra leg must not lose the primary line
                     legs[key] = {"error": f"{type(e).__name__}: {e}"}
+                print(f"[bench] leg {key}: {time.perf_counter() - t_leg:.1f} s", file=sys.stderr, flush=True)
         if legs:
             if args.legs_json:
                 Path(args.legs_json).write_text(json.dumps(legs, indent=1))

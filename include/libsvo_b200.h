@@ -630,8 +630,10 @@ int svo_server_create(const svo_server_cfg* cfg, svo_server** out);
 void svo_server_destroy(svo_server* s);
 /* Registers an octree (copied) with the given stack size; not resident
  * until a request needs it.  An octree whose node and attribute pools
- * together exceed the whole budget is registered as by
- * svo_server_add_octree_paged with half the budget as its region. */
+ * together take more than half the budget is registered as by
+ * svo_server_add_octree_paged with a quarter of the budget as its region.
+ * A request whose octree cannot be made resident even with every idle
+ * octree evicted (paged regions hold the space) ends with SVO_ERR_RANGE. */
 int svo_server_add_octree(svo_server* s, const svo_scene* scene, int32_t stack_size, uint32_t* id);
 /* Registers an octree served by treelet paging: it holds `region_bytes` of
  * the pool (node and attribute halves: region_bytes / (2 * treelet_bytes)

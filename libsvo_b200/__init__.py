@@ -989,7 +989,10 @@ class Server:
         ra = (svo_request * n)(*reqs)
         ta = (ctypes.c_double * n)(*[float(a) for a in arrival_s])
         out = (svo_request_result * n)()
-        _check(_L.svo_server_replay(self._h, ra, ta, n, timeout_ms, out), "svo_server_replay")
+        rc = _L.svo_server_replay(self._h, ra, ta, n, timeout_ms, out)
+        # kept when a wait timed out, so callers can see which requests finished
+        self.last_replay_results = list(out)
+        _check(rc, "svo_server_replay")
         return list(out)
 
     def close(self):

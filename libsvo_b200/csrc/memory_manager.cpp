@@ -124,7 +124,7 @@ int TreeletMemoryManager::free_incore_position() {
     if (s.visibility < 0 && s.treelet_gid != -1) {
       const int32_t parent = scene_.treelets[s.treelet_gid].parent_gid;
       const int32_t ps = slot_of_[parent];
-      if (ps >= 0 && slots_[ps].visibility < 0) {
+      if (ps >= 0 && (evict_any_invisible_ || slots_[ps].visibility < 0)) {
         freeable = s.treelet_gid;
         break;
       }

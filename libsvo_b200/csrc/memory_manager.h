@@ -73,6 +73,13 @@ class TreeletMemoryManager {
                        std::vector<std::pair<int32_t, float>>& out_old) const;
   // 12 MB worth of treelets (RenderPassAnalyse.cpp:340).
   uint32_t default_max_new_treelets() const;
+  // freeIncorePosition evicts a treelet only when it and its parent are both
+  // invisible (src/TreeletMemoryManager.cpp:571-579); since the root's slot
+  // never ages, the root's own sub-treelets then stay for good.  With `any`
+  // set, an invisible treelet goes whatever its parent's visibility (its
+  // subtree with it), so that a small region serving views that jump across
+  // the octree can always make room.  Off by default (the reference's rule).
+  void set_evict_any_invisible(bool any) { evict_any_invisible_ = any; }
 
   // Slot ranges the reference's updateDeviceMemory would copy
   // (TreeletMemoryManagerCl.cpp:177-236), as (first slot, slot count).  A
@@ -102,6 +109,7 @@ class TreeletMemoryManager {
   std::set<uint32_t> upload_;
   uint32_t search_pos_ = 1;
   float upload_ratio_ = 0.6f;
+  bool evict_any_invisible_ = false;
 };
 
 class TreeletMemoryManagerCuda : public TreeletMemoryManager {

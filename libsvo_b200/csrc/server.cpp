@@ -17,8 +17,8 @@
 // are evicted least recently used first when the pool is full.  A host
 // callback on each batch's stream timestamps completion.
 //
-// An octree whose pools do not fit the whole budget (or one registered with
-// svo_server_add_octree_paged) is not made resident whole: it keeps a fixed
+// An octree whose pools take more than half the budget (or one registered
+// with svo_server_add_octree_paged) is not made resident whole: it keeps a fixed
 // region of treelet slots in the pool and a worker thread of its own, which
 // serves its requests one by one, each after analysis passes over the
 // request's view at full resolution until no new treelet is placed
@@ -220,12 +220,19 @@ void CUDART_CB on_slot_done(void* p) {
 int alloc_evicting(svo_server* s, uint64_t need, int keep, uint64_t* off) {
   while (!s->pool.alloc(need, off)) {
     int victim = -1;
+    bool in_flight = false;  // an octree pinned by running work will free up later
     for (uint32_t i = 0; i < s->octrees.size(); ++i) {
       const ServedOctree& c = s->octrees[i];
-      if ((int)i == keep || c.paged || !c.resident || c.refs) continue;
+      if ((int)i == keep || c.paged || !c.resident) continue;
+      if (c.refs) {
+        in_flight = true;
+        continue;
+      }
       if (victim < 0 || c.last_use < s->octrees[victim].last_use) victim = (int)i;
     }
-    if (victim < 0) return need > s->pool.size() ? SVO_ERR_RANGE : SVO_ERR_BUSY;
+    // nothing to evict and nothing that will be released: the space is held
+    // by paged regions for good, so waiting would not help
+    if (victim < 0) return (need > s->pool.size() || !in_flight) ? SVO_ERR_RANGE : SVO_ERR_BUSY;
     ServedOctree& v = s->octrees[victim];
     int rc = v.mm->detach_device_buffers();
     if (rc != SVO_OK) return rc;
@@ -812,9 +819,9 @@ int add_octree(svo_server* s, const svo_scene* scene, int32_t stack_size, bool p
     svo_scene copy = *scene;
     const uint64_t tb = scene->treelet_bytes;
     const uint64_t whole = 2 * ((tb * scene->treelets.size() + 255) & ~255ull);
-    if (!paged && whole > s->pool.size()) {  // does not fit whole: paged in half the budget
+    if (!paged && whole > s->pool.size() / 2) {  // too large to page whole: a quarter of the budget
       paged = true;
-      region_bytes = s->pool.size() / 2;
+      region_bytes = s->pool.size() / 4;
     }
     uint64_t slots = scene->treelets.size();
     if (paged) {
@@ -827,6 +834,9 @@ int add_octree(svo_server* s, const svo_scene* scene, int32_t stack_size, bool p
       uint32_t n = 0;
       rc = o.mm->insert_all(&n);
       if (rc != SVO_OK) return rc;
+    } else {
+      // requests look anywhere: any treelet their views no longer see may go
+      o.mm->set_evict_any_invisible(true);
     }
     o.stack_size = stack_size;
     o.node_bytes = o.mm->incore_nodes() * sizeof(svo_node);

@@ -123,8 +123,8 @@ def test_cancel_wait_timeout_and_errors(workload, cuda):
 
 def test_octree_larger_than_the_budget_is_paged(workload, cuda):
     """An octree whose pools exceed the whole budget is no longer refused: it
-    is served by treelet paging in half the budget (a quarter of the octree's
-    treelets), and close views of a small patch of it converge to the fully
+    is served by treelet paging in a quarter of the budget (an eighth of the
+    octree), and close views of a small patch of it converge to the fully
     resident image."""
     import torch
 

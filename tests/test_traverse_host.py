@@ -94,11 +94,9 @@ def test_icosphere_frame(host_lib):
 
 
 def test_long_and_watchdog_rays(host_lib):
-    """Rays of 64 iterations and more take the cold path that looks for a
-    repeating traversal state and skips whole periods up to the watchdog:
-    every long ray of a 960x540 icosphere frame (one of them capped at
-    (S+1)^2*5 iterations) must still match the oracle in node, t, depth,
-    flags, loop and fetch counts."""
+    """Every long ray (60 iterations or more) of a 960x540 icosphere frame,
+    one of them stopped by the watchdog at (S+1)^2*5 iterations, matches the
+    oracle in node, t, depth, flags, loop and fetch counts."""
     from libsvo_b200 import scenes
 
     wl = scenes.icosphere(subdivisions=5, depth=9, treelet_levels=4, width=960, height=540)
