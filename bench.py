@@ -157,11 +157,13 @@ def cpu_reference_frames(wl, nodes, attribs, seconds=10.0, max_frames=200, light
     """Times the reference's renderToBuffer compiled for the host (or the
     oracle port) over whole frames of the workload, all host threads.  With
     `light`, the primary + shadow frame (the shadow shading over the
-    reference's own sample()); shadow rays count as rays."""
+    reference's own sample()); shadow rays count as rays.  The reference's
+    kernel has MAX_STACK_SIZE 13 compiled in, so octrees deeper than 12 levels
+    take the oracle port with their own stack size."""
     import oracle
 
     threads = os.cpu_count() or 1
-    ref = oracle.reference_lib() is not None
+    ref = oracle.reference_lib() is not None and wl.stack_size == 13
     params = [bytes(c.frame_params()) for c in wl.cameras]
     # shadow rays per frame = primary hits (counted once, outside the timing)
     shadow_rays = [int(oracle.render(nodes, attribs, p, stack_size=wl.stack_size, threads=threads)[1]["hit"].sum())
@@ -195,17 +197,18 @@ def cpu_reference_frames(wl, nodes, attribs, seconds=10.0, max_frames=200, light
 
 
 def reference_parity(nodes, attribs, params, gpu_rgba, gpu_hits, light=None, gpu_shadow_hits=None,
-                     config=""):
+                     config="", stack_size=13):
     """Compares one GPU frame with the reference's own renderToBuffer compiled
     for the host (oracle/_ref): every pixel's RGBA8, and per ray the node
     index, depth, hit flag and loop count of the reference's sample() (primary
     rays; with `light`, the shadow rays of the shadow frame).  The oracle
-    restatement stands in when the reference build is absent."""
+    restatement (pinned to the reference at its stack of 13) stands in when
+    the reference build is absent or the octree needs a deeper stack."""
     import oracle
 
     p = bytes(params)
     w, h = (int(v) for v in np.frombuffer(p[:8], dtype=np.uint32))
-    ref = oracle.reference_lib() is not None
+    ref = oracle.reference_lib() is not None and stack_size == 13
     fields = ("node", "depth", "hit", "loops")
     out = {"config": config, "pixels": w * h, "against": "reference" if ref else "oracle restatement"}
     if light is None:
@@ -214,7 +217,7 @@ def reference_parity(nodes, attribs, params, gpu_rgba, gpu_hits, light=None, gpu
             o, d = oracle.pixel_rays(p)
             ref_hits = oracle.reference_sample_rays(nodes, o, d, params.t_scale_ratio)
         else:
-            ref_rgba, ref_hits, _, _ = oracle.render(nodes, attribs, p)
+            ref_rgba, ref_hits, _, _ = oracle.render(nodes, attribs, p, stack_size=stack_size)
         rays_ref, rays_gpu = ref_hits.reshape(-1), gpu_hits.reshape(-1)
         out["rays"] = w * h
     else:
@@ -222,7 +225,7 @@ def reference_parity(nodes, attribs, params, gpu_rgba, gpu_hits, light=None, gpu
             rgbaf, ref_shadow = oracle.reference_render_shadow(nodes, attribs, p, light)
             ref_rgba = oracle.to_rgba8(rgbaf)
         else:
-            ref_rgba, _, ref_shadow, _, _ = oracle.render_shadow(nodes, attribs, p, light)
+            ref_rgba, _, ref_shadow, _, _ = oracle.render_shadow(nodes, attribs, p, light, stack_size=stack_size)
         rays_ref, rays_gpu = ref_shadow.reshape(-1), gpu_shadow_hits.reshape(-1)
         out["rays"] = int(rays_gpu["hit"].size)
         out["rays_compared"] = "shadow rays (one per primary hit; zero records elsewhere)"
@@ -438,10 +441,10 @@ def served_leg(dev, n=400, rates=(4000, 16000, 64000)):
     paging_ungated = run(L.SERVE_PLAIN_STREAMED, footprint // 2, [16000], streams=8)
     paging_ungated_pinned = run(L.SERVE_PLAIN_STREAMED, footprint // 2, [16000], upload=L.UPLOAD_PINNED,
                                 streams=8)
-    # a budget below the largest octree's footprint: octrees taking more than
-    # half of it (the two largest) are served by treelet paging, each in a
-    # quarter of the budget (svo_server_add_octree decides), the others page
-    # in and out whole under the rest
+    # a budget below the largest octree's footprint: octrees larger than it
+    # (the two largest) are served by treelet paging, each in a quarter of the
+    # budget (svo_server_add_octree decides), the others page in and out whole
+    # under the rest
     sizes = [16 * s.info.treelet_bytes // 8 * s.info.num_treelets for s in wl.scenes]
     tp_budget = int(0.9 * max(sizes))
     treelet_paged = {"budget_gb": tp_budget / 1e9, "largest_octree_gb": max(sizes) / 1e9,
@@ -749,7 +752,7 @@ def large_shadow_leg(dev, reps=10, cap_gb=60.0, subdivisions=9, depth=14, cpu_ba
             out["cpu_baseline"], pool = large_cpu_baseline(wl, n)
             if pool is not None:
                 out["parity"] = reference_parity(pool[0], pool[1], p, gpu_rgba, h, light=wl.light,
-                                                 gpu_shadow_hits=sh, config=wl.name)
+                                                 gpu_shadow_hits=sh, config=wl.name, stack_size=wl.stack_size)
                 del pool
         except Exception as e:  # the host copy or the CPU run failed: keep the GPU result
             out["cpu_baseline"] = {"unavailable": f"{type(e).__name__}: {e}"}
@@ -828,7 +831,8 @@ def large_streaming_leg(dev, cap_gb=16.0, frames=60, subdivisions=9, depth=14, u
     1/8 resolution with a jittered far plane (the reference's dynamic loading:
     treelets paged in by visibility, evicted when the buffer is full) and
     then the frame; the camera moves in along the orbit from radius 2.5 to
-    1.2.  Then the last view is converged by analysis passes at full
+    1.2; a pass may place 256 MB of treelets (the reference's 12 MB cap is
+    paced for PCIe 2).  Then the last view is converged by analysis passes at full
     resolution and its primary-ray frame compared with the same frame over the
     fully resident pool (RGBA8 and, per ray, hit, depth, t and loop count;
     node indices differ between the two pools)."""
@@ -850,6 +854,9 @@ def large_streaming_leg(dev, cap_gb=16.0, frames=60, subdivisions=9, depth=14, u
     host_s = time.perf_counter() - t0
     if upload == "pinned":
         mm.setUploadPolicy(L.UPLOAD_PINNED)
+    # the reference places 12 MB of treelets per pass (paced for PCIe 2);
+    # 256 MB per pass is about 6 ms of the page-locked gather here
+    mm.setAnalysisBudget(256 << 20)
     mm.initDeviceBuffer()
     cfg = L.trace_cfg(L.TRAVERSAL_TREELET, wl.stack_size)
     sc = L.shadow_cfg(wl.light)
@@ -881,7 +888,7 @@ def large_streaming_leg(dev, cap_gb=16.0, frames=60, subdivisions=9, depth=14, u
            "capped_rays": st.capped_rays, "bounds_errors": st.bounds_errors}
     # converged view: full-resolution analysis passes until nothing new is placed
     steps, new = 0, 1
-    while new and steps < 80:
+    while new and steps < 200:
         new, _ = mm.performAnalysePass(p, divisor=1, stack_size=wl.stack_size, stream=s)
         steps += 1
     hb = torch.empty(primary * 16, dtype=torch.uint8, device=dev)
@@ -1104,7 +1111,8 @@ def main():
             pp, p_rgba, p_hits, p_shadow = parity_frame
             line["parity"] = reference_parity(nodes, attribs, pp, p_rgba, p_hits,
                                               light=L.seeded_light(1) if shadow else None,
-                                              gpu_shadow_hits=p_shadow, config=line["config"]["workload"])
+                                              gpu_shadow_hits=p_shadow, config=line["config"]["workload"],
+                                              stack_size=wl.stack_size)
         mm.close()
         legs = {}
         if world == 1 and not args.no_extra and args.workload == "icosphere":

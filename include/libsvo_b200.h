@@ -487,6 +487,11 @@ int svo_mm_analyse_feedback_device(svo_mm* mm, const svo_feedback* d_feedback, u
  * reference's updateClientSideIncoreBuffer, the step skips new treelets that
  * find no slot under memory pressure (the next step asks for them again).
  * *num_old: visible resident treelets. */
+/* The bytes of newly visible treelets one analysis step may place: the
+ * reference's pass is capped at 12 MB (maxTreeletsToPropergate,
+ * src/RenderPassAnalyse.cpp:340), paced for PCIe 2; 0 restores that cap.
+ * SVO_ERR_RANGE below one treelet. */
+int svo_mm_set_analysis_budget(svo_mm* mm, uint64_t bytes);
 int svo_mm_analysis_step(svo_mm* mm, const svo_frame_params* frame, uint32_t divisor,
                          float jitter_x, float jitter_y, int32_t stack_size, void* stream,
                          uint32_t* num_new, uint32_t* num_old);
@@ -630,7 +635,7 @@ int svo_server_create(const svo_server_cfg* cfg, svo_server** out);
 void svo_server_destroy(svo_server* s);
 /* Registers an octree (copied) with the given stack size; not resident
  * until a request needs it.  An octree whose node and attribute pools
- * together take more than half the budget is registered as by
+ * together exceed the budget is registered as by
  * svo_server_add_octree_paged with a quarter of the budget as its region.
  * A request whose octree cannot be made resident even with every idle
  * octree evicted (paged regions hold the space) ends with SVO_ERR_RANGE. */

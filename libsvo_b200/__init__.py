@@ -901,6 +901,7 @@ for _name, (_args, _res) in {
     "svo_server_add_octree": ([_vp, _vp, _i32, _P(_u32)], ctypes.c_int),
     "svo_server_add_octree_paged": ([_vp, _vp, _i32, _u64, _P(_u32)], ctypes.c_int),
     "svo_scene_from_pool": ([_vp, _vp, _u32, _u32, _u32, _u64, _P(_vp)], ctypes.c_int),
+    "svo_mm_set_analysis_budget": ([_vp, _u64], ctypes.c_int),
     "svo_mm_create_from_device_scene": ([_vp, _u64, _vp, _P(_vp)], ctypes.c_int),
     "svo_server_set_upload_policy": ([_vp, _u32, _i32], ctypes.c_int),
     "svo_server_submit": ([_vp, _P(svo_request), _P(_u64)], ctypes.c_int),
@@ -1080,6 +1081,14 @@ def _perform_analyse_pass(self, frame: svo_frame_params, divisor=8, jitter=(0.0,
 TreeletMemoryManagerCuda.analyseFeedback = _analyse_feedback
 TreeletMemoryManagerCuda.analyseFeedbackDevice = _analyse_feedback_device
 TreeletMemoryManagerCuda.performAnalysePass = _perform_analyse_pass
+
+
+def _set_analysis_budget(self, nbytes: int):
+    """Bytes of new treelets one analysis pass may place (0: the reference's 12 MB)."""
+    _check(_L.svo_mm_set_analysis_budget(self._h, int(nbytes)), "svo_mm_set_analysis_budget")
+
+
+TreeletMemoryManagerCuda.setAnalysisBudget = _set_analysis_budget
 
 
 # ---- teardown ------------------------------------------------------------------

@@ -675,6 +675,15 @@ int svo_mm_analyse_feedback_device(svo_mm* mm, const svo_feedback* d_feedback, u
   });
 }
 
+int svo_mm_set_analysis_budget(svo_mm* mm, uint64_t bytes) {
+  if (!mm) return SVO_ERR_INVALID;
+  const uint64_t tb = mm->impl.treelet_bytes();
+  const uint64_t n = bytes / tb;
+  if (bytes && n == 0) return SVO_ERR_RANGE;
+  mm->impl.set_max_new_treelets((uint32_t)std::min<uint64_t>(n, 0xFFFFFFFFull));
+  return SVO_OK;
+}
+
 int svo_mm_analysis_step(svo_mm* mm, const svo_frame_params* frame, uint32_t divisor,
                          float jitter_x, float jitter_y, int32_t stack_size, void* stream,
                          uint32_t* num_new, uint32_t* num_old) {

@@ -750,7 +750,7 @@ int TreeletMemoryManagerCuda::analysis_step(const svo_frame_params& frame, uint3
   if (rc != SVO_OK) return rc;
   // the records stay on the GPU; only per-treelet results come back
   std::vector<std::pair<int32_t, float>> nw, old;
-  rc = analyse_feedback_device(d_fb, n, default_max_new_treelets(), nw, old, s);
+  rc = analyse_feedback_device(d_fb, n, max_new_treelets(), nw, old, s);
   if (num_new) *num_new = (uint32_t)nw.size();
   if (num_old) *num_old = (uint32_t)old.size();
   if (num_requested) *num_requested = (uint32_t)nw.size();

@@ -73,6 +73,18 @@ class TreeletMemoryManager {
                        std::vector<std::pair<int32_t, float>>& out_old) const;
   // 12 MB worth of treelets (RenderPassAnalyse.cpp:340).
   uint32_t default_max_new_treelets() const;
+  // Newly visible treelets one analysis step may place: the reference's
+  // 12 MB worth (src/RenderPassAnalyse.cpp:340) unless set; 0 restores it.
+  void set_max_new_treelets(uint32_t n) { max_new_ = n; }
+  uint32_t max_new_treelets() const { return max_new_ ? max_new_ : default_max_new_treelets(); }
+  // Marks every resident treelet but the root unseen (visibility -1), as if
+  // it had not been seen for as many passes as the reference's visibility
+  // counter lasts: the next analysis pass marks what its view sees again, and
+  // everything else can be evicted at once instead of after 9 passes.
+  void mark_all_unseen() {
+    for (uint32_t i = 1; i < slots_.size(); ++i)
+      if (slots_[i].treelet_gid >= 0) slots_[i].visibility = -1;
+  }
   // freeIncorePosition evicts a treelet only when it and its parent are both
   // invisible (src/TreeletMemoryManager.cpp:571-579); since the root's slot
   // never ages, the root's own sub-treelets then stay for good.  With `any`
@@ -110,6 +122,7 @@ class TreeletMemoryManager {
   uint32_t search_pos_ = 1;
   float upload_ratio_ = 0.6f;
   bool evict_any_invisible_ = false;
+  uint32_t max_new_ = 0;
 };
 
 class TreeletMemoryManagerCuda : public TreeletMemoryManager {

@@ -17,8 +17,8 @@
 // are evicted least recently used first when the pool is full.  A host
 // callback on each batch's stream timestamps completion.
 //
-// An octree whose pools take more than half the budget (or one registered
-// with svo_server_add_octree_paged) is not made resident whole: it keeps a fixed
+// An octree whose pools exceed the budget (or one registered with
+// svo_server_add_octree_paged) is not made resident whole: it keeps a fixed
 // region of treelet slots in the pool and a worker thread of its own, which
 // serves its requests one by one, each after analysis passes over the
 // request's view at full resolution until no new treelet is placed
@@ -305,6 +305,8 @@ void paged_worker_loop(svo_server* s, uint32_t id) {
     uint32_t placed = 0;
     int rc = SVO_OK;
     bool converged = false;
+    // a new view: what it does not see may make room at once
+    mm->mark_all_unseen();
     for (uint32_t step = 0; step < kMaxPagingSteps; ++step) {
       // converged when the pass asks for nothing new; a pass may also place
       // nothing because the region is full of treelets still marked visible
@@ -819,7 +821,7 @@ int add_octree(svo_server* s, const svo_scene* scene, int32_t stack_size, bool p
     svo_scene copy = *scene;
     const uint64_t tb = scene->treelet_bytes;
     const uint64_t whole = 2 * ((tb * scene->treelets.size() + 255) & ~255ull);
-    if (!paged && whole > s->pool.size() / 2) {  // too large to page whole: a quarter of the budget
+    if (!paged && whole > s->pool.size()) {  // cannot be resident whole: a quarter of the budget
       paged = true;
       region_bytes = s->pool.size() / 4;
     }
@@ -835,8 +837,10 @@ int add_octree(svo_server* s, const svo_scene* scene, int32_t stack_size, bool p
       rc = o.mm->insert_all(&n);
       if (rc != SVO_OK) return rc;
     } else {
-      // requests look anywhere: any treelet their views no longer see may go
+      // requests look anywhere: any treelet their views no longer see may go,
+      // and one pass may fill the whole region
       o.mm->set_evict_any_invisible(true);
+      o.mm->set_max_new_treelets((uint32_t)slots);
     }
     o.stack_size = stack_size;
     o.node_bytes = o.mm->incore_nodes() * sizeof(svo_node);
