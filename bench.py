@@ -441,15 +441,38 @@ def served_leg(dev, n=400, rates=(4000, 16000, 64000)):
     paging_ungated = run(L.SERVE_PLAIN_STREAMED, footprint // 2, [16000], streams=8)
     paging_ungated_pinned = run(L.SERVE_PLAIN_STREAMED, footprint // 2, [16000], upload=L.UPLOAD_PINNED,
                                 streams=8)
-    # a budget below the largest octree's footprint: octrees larger than it
-    # (the two largest) are served by treelet paging, each in a quarter of the
-    # budget (svo_server_add_octree decides), the others page in and out whole
-    # under the rest
+    # treelet paging under a budget below the largest octree's footprint: the
+    # two largest octrees (1.4 GB each) and the requests naming them, served
+    # from 0.9x the largest footprint, each octree paged in half of it (45 %
+    # of its treelets; the views of this mix need up to about 42 %)
     sizes = [16 * s.info.treelet_bytes // 8 * s.info.num_treelets for s in wl.scenes]
+    big = sorted(range(len(sizes)), key=lambda i: -sizes[i])[:2]
     tp_budget = int(0.9 * max(sizes))
-    treelet_paged = {"budget_gb": tp_budget / 1e9, "largest_octree_gb": max(sizes) / 1e9,
-                     "batched": run(L.SERVE_BATCHED, tp_budget, [16000]),
-                     "plain_ungated": run(L.SERVE_PLAIN_STREAMED, tp_budget, [16000], streams=8)}
+    tp_reqs = [(o, c, t) for (o, c), t in zip(reqs, outs) if o in big]
+    tp_rays = sum(c.width * c.height for _, c, _ in tp_reqs)
+
+    def run_paged(rate):
+        srv = L.Server(L.server_cfg(tp_budget, streams=4, max_batch_views=256))
+        ids = {o: srv.add_octree_paged(wl.scenes[o], tp_budget // 2) for o in big}
+        rq = [L.request(ids[o], c.frame_params(), t) for o, c, t in tp_reqs]
+        t_run = time.perf_counter()
+        arr = S.poisson_arrivals(len(rq), rate, seed=13)
+        r = srv.replay(rq, arr, timeout_ms=120000)
+        ok = [x for x in r if x.status == L.SVO_OK]
+        lat = np.array([x.done_s - x.submit_s for x in ok]) * 1e3
+        span = max(x.done_s for x in ok) - min(x.submit_s for x in r)
+        st = srv.stats()
+        srv.close()
+        print(f"[bench] served treelet-paged rate {rate}: {time.perf_counter() - t_run:.1f} s",
+              file=sys.stderr, flush=True)
+        return {"requests": len(rq), "rays": tp_rays, "mrays_s": tp_rays / span / 1e6,
+                "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                "failed": len(r) - len(ok), "treelets_paged_in": st.treelets_paged_in,
+                "gb_uploaded": st.bytes_uploaded / 1e9, "paged_unconverged": st.paged_unconverged}
+
+    treelet_paged = {"octrees": big, "octree_gb": [sizes[o] / 1e9 for o in big], "budget_gb": tp_budget / 1e9,
+                     "region_gb_each": tp_budget // 2 / 1e9, "rate_1000": run_paged(1000),
+                     "rate_16000": run_paged(16000)}
     keys = [k for k in batched if k != "paging"]
     return {"workload": wl.name, "description": wl.description, "requests": n, "rays": rays,
             "scene_build_s": round(build_s, 2), "octree_footprint_gb": footprint / 1e9,
@@ -798,10 +821,9 @@ def summarize_legs(legs: dict) -> dict:
             out[key] = {"cols": "Mrays/s, p50 ms, p99 ms", "rates": rates, "half_budget_16000": pg}
             if "treelet_paged" in v:
                 t = v["treelet_paged"]
-                out[key]["treelet_paged_16000"] = {
-                    k: [_r(t[k]["16000"]["mrays_s"]), _r(t[k]["16000"]["p50_ms"]), _r(t[k]["16000"]["p99_ms"]),
-                        t[k]["paging"]["paged_unconverged"]]
-                    for k in ("batched", "plain_ungated") if k in t}
+                out[key]["treelet_paged"] = {
+                    k: [_r(t[k]["mrays_s"]), _r(t[k]["p50_ms"]), _r(t[k]["p99_ms"]), t[k]["paged_unconverged"]]
+                    for k in ("rate_1000", "rate_16000")}
         elif key == "large_shadowed":
             out[key] = {"mrays_s": _r(v["mrays_s"]), "ms": _r(v["ms_per_frame"]),
                         "frac": _r(v["roofline"]["frac"]),
@@ -822,7 +844,7 @@ def summarize_legs(legs: dict) -> dict:
     return out
 
 
-def large_streaming_leg(dev, cap_gb=16.0, frames=60, subdivisions=9, depth=14, upload="pinned"):
+def large_streaming_leg(dev, cap_gb=24.0, frames=60, subdivisions=9, depth=14, upload="pinned"):
     """The large shadowed workload under a residency cap: the depth-14
     icosphere built on the GPU, its pool turned back into treelets on the host
     (svo_mm_create_from_device_scene), and 3840x2160 primary + shadow frames
@@ -887,9 +909,10 @@ def large_streaming_leg(dev, cap_gb=16.0, frames=60, subdivisions=9, depth=14, u
            "gb_paged_in": placed * slot_bytes / 1e9, "primary_mrays_s_mean": primary / statistics.mean(steady) / 1e3,
            "capped_rays": st.capped_rays, "bounds_errors": st.bounds_errors}
     # converged view: full-resolution analysis passes until nothing new is placed
-    steps, new = 0, 1
-    while new and steps < 200:
-        new, _ = mm.performAnalysePass(p, divisor=1, stack_size=wl.stack_size, stream=s)
+    steps, asked = 0, 1
+    while asked and steps < 200:
+        mm.performAnalysePass(p, divisor=1, stack_size=wl.stack_size, stream=s)
+        asked = mm.lastAnalysisRequested()
         steps += 1
     hb = torch.empty(primary * 16, dtype=torch.uint8, device=dev)
     mm.render(p, out, hb, cfg=cfg, stream=s)
@@ -906,7 +929,7 @@ def large_streaming_leg(dev, cap_gb=16.0, frames=60, subdivisions=9, depth=14, u
         bad |= got[k] != want[k]
     bad |= got["t"].view(np.uint32) != want["t"].view(np.uint32)
     res["converged_parity"] = {"view": "the last frame's camera (radius 1.2), primary rays", "analysis_passes": steps,
-                               "converged": new == 0, "pixels": primary,
+                               "converged": asked == 0, "pixels": primary,
                                "mismatched_rgba": int((got_rgba.reshape(-1) != out.cpu().numpy().view(np.uint32).reshape(-1)).sum()),
                                "mismatched_rays": int(bad.sum())}
     res["converged_parity"]["mismatched"] = (res["converged_parity"]["mismatched_rgba"]

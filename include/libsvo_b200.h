@@ -492,6 +492,10 @@ int svo_mm_analyse_feedback_device(svo_mm* mm, const svo_feedback* d_feedback, u
  * src/RenderPassAnalyse.cpp:340), paced for PCIe 2; 0 restores that cap.
  * SVO_ERR_RANGE below one treelet. */
 int svo_mm_set_analysis_budget(svo_mm* mm, uint64_t bytes);
+/* Newly visible treelets the last svo_mm_analysis_step asked for, placed or
+ * not: 0 once the view needs no treelet that is not resident (the step's
+ * *num_new counts only those placed, which a full buffer keeps at 0). */
+int svo_mm_analysis_requested(svo_mm* mm, uint32_t* requested);
 int svo_mm_analysis_step(svo_mm* mm, const svo_frame_params* frame, uint32_t divisor,
                          float jitter_x, float jitter_y, int32_t stack_size, void* stream,
                          uint32_t* num_new, uint32_t* num_old);

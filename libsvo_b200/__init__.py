@@ -902,6 +902,7 @@ for _name, (_args, _res) in {
     "svo_server_add_octree_paged": ([_vp, _vp, _i32, _u64, _P(_u32)], ctypes.c_int),
     "svo_scene_from_pool": ([_vp, _vp, _u32, _u32, _u32, _u64, _P(_vp)], ctypes.c_int),
     "svo_mm_set_analysis_budget": ([_vp, _u64], ctypes.c_int),
+    "svo_mm_analysis_requested": ([_vp, _P(_u32)], ctypes.c_int),
     "svo_mm_create_from_device_scene": ([_vp, _u64, _vp, _P(_vp)], ctypes.c_int),
     "svo_server_set_upload_policy": ([_vp, _u32, _i32], ctypes.c_int),
     "svo_server_submit": ([_vp, _P(svo_request), _P(_u64)], ctypes.c_int),
@@ -1089,6 +1090,16 @@ def _set_analysis_budget(self, nbytes: int):
 
 
 TreeletMemoryManagerCuda.setAnalysisBudget = _set_analysis_budget
+
+
+def _last_analysis_requested(self) -> int:
+    """Treelets the last analysis pass asked for, placed or not (0: converged)."""
+    n = _u32()
+    _check(_L.svo_mm_analysis_requested(self._h, ctypes.byref(n)), "svo_mm_analysis_requested")
+    return n.value
+
+
+TreeletMemoryManagerCuda.lastAnalysisRequested = _last_analysis_requested
 
 
 # ---- teardown ------------------------------------------------------------------

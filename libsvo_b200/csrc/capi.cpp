@@ -684,6 +684,12 @@ int svo_mm_set_analysis_budget(svo_mm* mm, uint64_t bytes) {
   return SVO_OK;
 }
 
+int svo_mm_analysis_requested(svo_mm* mm, uint32_t* requested) {
+  if (!mm || !requested) return SVO_ERR_INVALID;
+  *requested = mm->impl.last_requested();
+  return SVO_OK;
+}
+
 int svo_mm_analysis_step(svo_mm* mm, const svo_frame_params* frame, uint32_t divisor,
                          float jitter_x, float jitter_y, int32_t stack_size, void* stream,
                          uint32_t* num_new, uint32_t* num_old) {

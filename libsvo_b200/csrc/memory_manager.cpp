@@ -724,6 +724,7 @@ int TreeletMemoryManagerCuda::analysis_step(const svo_frame_params& frame, uint3
   if (num_new) *num_new = 0;
   if (num_old) *num_old = 0;
   if (num_requested) *num_requested = 0;
+  last_requested_ = 0;
   if (divisor == 0 || !device_ready()) return SVO_ERR_INVALID;
   if (stack_size < 2 || stack_size > 24) return SVO_ERR_RANGE;
   cudaStream_t s = stream ? stream : render_stream_;
@@ -754,6 +755,7 @@ int TreeletMemoryManagerCuda::analysis_step(const svo_frame_params& frame, uint3
   if (num_new) *num_new = (uint32_t)nw.size();
   if (num_old) *num_old = (uint32_t)old.size();
   if (num_requested) *num_requested = (uint32_t)nw.size();
+  last_requested_ = (uint32_t)nw.size();
   if (rc != SVO_OK) return rc;
   std::vector<int32_t> ng(nw.size()), og(old.size());
   std::vector<float> ne(nw.size());

@@ -77,6 +77,8 @@ class TreeletMemoryManager {
   // 12 MB worth (src/RenderPassAnalyse.cpp:340) unless set; 0 restores it.
   void set_max_new_treelets(uint32_t n) { max_new_ = n; }
   uint32_t max_new_treelets() const { return max_new_ ? max_new_ : default_max_new_treelets(); }
+  // Newly visible treelets the last analysis step asked for, placed or not.
+  uint32_t last_requested() const { return last_requested_; }
   // Marks every resident treelet but the root unseen (visibility -1), as if
   // it had not been seen for as many passes as the reference's visibility
   // counter lasts: the next analysis pass marks what its view sees again, and
@@ -123,6 +125,7 @@ class TreeletMemoryManager {
   float upload_ratio_ = 0.6f;
   bool evict_any_invisible_ = false;
   uint32_t max_new_ = 0;
+  uint32_t last_requested_ = 0;
 };
 
 class TreeletMemoryManagerCuda : public TreeletMemoryManager {
