@@ -879,6 +879,9 @@ def large_streaming_leg(dev, cap_gb=24.0, frames=60, subdivisions=9, depth=14, u
     # the reference places 12 MB of treelets per pass (paced for PCIe 2);
     # 256 MB per pass is about 6 ms of the page-locked gather here
     mm.setAnalysisBudget(256 << 20)
+    # every treelet below the root hangs off the root, whose slot never ages:
+    # under the reference's eviction rule none could leave a full buffer
+    mm.setEviction(L.EVICT_ANY_UNSEEN)
     mm.initDeviceBuffer()
     cfg = L.trace_cfg(L.TRAVERSAL_TREELET, wl.stack_size)
     sc = L.shadow_cfg(wl.light)

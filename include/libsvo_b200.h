@@ -492,6 +492,16 @@ int svo_mm_analyse_feedback_device(svo_mm* mm, const svo_feedback* d_feedback, u
  * src/RenderPassAnalyse.cpp:340), paced for PCIe 2; 0 restores that cap.
  * SVO_ERR_RANGE below one treelet. */
 int svo_mm_set_analysis_budget(svo_mm* mm, uint64_t bytes);
+/* Which treelet freeIncorePosition may evict.  SVO_EVICT_REFERENCE (default,
+ * src/TreeletMemoryManager.cpp:571-579): one unseen for the visibility
+ * counter's 9 passes whose parent is unseen too; the root's slot never ages,
+ * so its own sub-treelets are never evicted.  SVO_EVICT_ANY_UNSEEN: any
+ * unseen treelet, whatever its parent (its attached subtree goes with it),
+ * so that a buffer full of treelets one view no longer sees makes room for
+ * the next.  No reference counterpart. */
+#define SVO_EVICT_REFERENCE 0
+#define SVO_EVICT_ANY_UNSEEN 1
+int svo_mm_set_eviction(svo_mm* mm, int32_t rule);
 /* Newly visible treelets the last svo_mm_analysis_step asked for, placed or
  * not: 0 once the view needs no treelet that is not resident (the step's
  * *num_new counts only those placed, which a full buffer keeps at 0). */

@@ -903,6 +903,7 @@ for _name, (_args, _res) in {
     "svo_scene_from_pool": ([_vp, _vp, _u32, _u32, _u32, _u64, _P(_vp)], ctypes.c_int),
     "svo_mm_set_analysis_budget": ([_vp, _u64], ctypes.c_int),
     "svo_mm_analysis_requested": ([_vp, _P(_u32)], ctypes.c_int),
+    "svo_mm_set_eviction": ([_vp, _i32], ctypes.c_int),
     "svo_mm_create_from_device_scene": ([_vp, _u64, _vp, _P(_vp)], ctypes.c_int),
     "svo_server_set_upload_policy": ([_vp, _u32, _i32], ctypes.c_int),
     "svo_server_submit": ([_vp, _P(svo_request), _P(_u64)], ctypes.c_int),
@@ -1100,6 +1101,17 @@ def _last_analysis_requested(self) -> int:
 
 
 TreeletMemoryManagerCuda.lastAnalysisRequested = _last_analysis_requested
+
+EVICT_REFERENCE = 0
+EVICT_ANY_UNSEEN = 1
+
+
+def _set_eviction(self, rule: int):
+    """EVICT_REFERENCE (the reference's rule) or EVICT_ANY_UNSEEN."""
+    _check(_L.svo_mm_set_eviction(self._h, int(rule)), "svo_mm_set_eviction")
+
+
+TreeletMemoryManagerCuda.setEviction = _set_eviction
 
 
 # ---- teardown ------------------------------------------------------------------

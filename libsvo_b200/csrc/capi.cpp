@@ -684,6 +684,13 @@ int svo_mm_set_analysis_budget(svo_mm* mm, uint64_t bytes) {
   return SVO_OK;
 }
 
+int svo_mm_set_eviction(svo_mm* mm, int32_t rule) {
+  if (!mm) return SVO_ERR_INVALID;
+  if (rule != SVO_EVICT_REFERENCE && rule != SVO_EVICT_ANY_UNSEEN) return SVO_ERR_NOTSUP;
+  mm->impl.set_evict_any_invisible(rule == SVO_EVICT_ANY_UNSEEN);
+  return SVO_OK;
+}
+
 int svo_mm_analysis_requested(svo_mm* mm, uint32_t* requested) {
   if (!mm || !requested) return SVO_ERR_INVALID;
   *requested = mm->impl.last_requested();
