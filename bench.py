@@ -853,8 +853,8 @@ def large_streaming_leg(dev, cap_gb=24.0, frames=60, subdivisions=9, depth=14, u
     1/8 resolution with a jittered far plane (the reference's dynamic loading:
     treelets paged in by visibility, evicted when the buffer is full) and
     then the frame; the camera moves in along the orbit from radius 2.5 to
-    1.2; a pass may place 256 MB of treelets (the reference's 12 MB cap is
-    paced for PCIe 2).  Then the last view is converged by analysis passes at full
+    1.2; a pass places at most 12 MB of treelets, as in the reference.  Then
+    the last view is converged by analysis passes (256 MB each) at full
     resolution and its primary-ray frame compared with the same frame over the
     fully resident pool (RGBA8 and, per ray, hit, depth, t and loop count;
     node indices differ between the two pools)."""
@@ -876,9 +876,6 @@ def large_streaming_leg(dev, cap_gb=24.0, frames=60, subdivisions=9, depth=14, u
     host_s = time.perf_counter() - t0
     if upload == "pinned":
         mm.setUploadPolicy(L.UPLOAD_PINNED)
-    # the reference places 12 MB of treelets per pass (paced for PCIe 2);
-    # 256 MB per pass is about 6 ms of the page-locked gather here
-    mm.setAnalysisBudget(256 << 20)
     # every treelet below the root hangs off the root, whose slot never ages:
     # under the reference's eviction rule none could leave a full buffer
     mm.setEviction(L.EVICT_ANY_UNSEEN)
@@ -911,7 +908,10 @@ def large_streaming_leg(dev, cap_gb=24.0, frames=60, subdivisions=9, depth=14, u
            "ms_first": ms[0], "treelets_paged_in": placed,
            "gb_paged_in": placed * slot_bytes / 1e9, "primary_mrays_s_mean": primary / statistics.mean(steady) / 1e3,
            "capped_rays": st.capped_rays, "bounds_errors": st.bounds_errors}
-    # converged view: full-resolution analysis passes until nothing new is placed
+    # converged view: full-resolution analysis passes until nothing new is
+    # asked for, each placing up to 256 MB (the frames above keep the
+    # reference's 12 MB per pass)
+    mm.setAnalysisBudget(256 << 20)
     steps, asked = 0, 1
     while asked and steps < 200:
         mm.performAnalysePass(p, divisor=1, stack_size=wl.stack_size, stream=s)

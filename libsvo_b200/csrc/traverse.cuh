@@ -110,6 +110,20 @@ struct StagedFetch {
   }
 };
 
+// A saved traversal state for the cycle search of very long rays (descend):
+// frame node, scale and tMin bits, the stacked frames, and the loop and fetch
+// counts when it was saved.  Lives in local memory (volatile, so the hot
+// loop's registers are not spent on it); only rays that run kCycleFrom
+// iterations or more touch it -- on the 1080p icosphere frame the 8 rays the
+// watchdog stops, which otherwise run alone for 980 iterations after the rest
+// of the frame is done (a search from iteration 64 or 256 made the many long
+// rays below 512 pay for the checks and the frame slower).
+constexpr uint32_t kCycleFrom = 512;
+struct CycleMark {
+  uint32_t node, scale, tmin, loops, fetches, next_save;
+  uint32_t stack[2 * kMaxStack];
+};
+
 // The descent loop.  kFlat selects the CpuRaycasterSingleRay3 rules; S is
 // the stack size (treelet) or the octree depth (flat).  `stack` points at
 // this thread's column of the shared-memory stack, `stride` words apart.
@@ -152,6 +166,8 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
   // one 32-bit compare against the last index
   const uint32_t last_node = num_nodes ? (uint32_t)(num_nodes - 1u) : 0u;
   uint2* sp = stack;  // the next free stack word: level S-1-scale
+  uint32_t check_at = max_loops < kCycleFrom ? max_loops : kCycleFrom;
+  volatile CycleMark mark;
   auto capped = [&]() {
     h.flags = SVO_HITFLAG_CAPPED;
     h.loops = loops;
@@ -173,9 +189,52 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
 
   for (;;) {  // ends by a return, or by a pop above the root
     ++loops;
-    if (loops == max_loops) {
-      capped();
-      return;
+    if (loops >= check_at) {
+      if (loops == max_loops) {
+        capped();
+        return;
+      }
+      // Cold path (rays past kCycleFrom iterations only).  The state at the
+      // start of an iteration is the frame's node, scale and tMin and the
+      // stacked frames: a frame's tMax depends only on its box and the ray,
+      // and the box on the nodes stacked above it.  Once that state recurs,
+      // the ray repeats the same iterations with period p until the
+      // watchdog, so whole periods are skipped (loop and fetch counts
+      // advanced by them) and the iterations left run as usual: the watchdog
+      // then stops the ray in the state, and with the counts, the reference
+      // reaches.  States are saved at iterations kCycleFrom, 2 kCycleFrom, ...
+      // (Brent's cycle search) and compared with every later iteration.
+      check_at = loops + 1u;
+      const uint32_t depth = (uint32_t)(S - 1 - scale);
+      bool same = loops > kCycleFrom && mark.node == node && mark.scale == (uint32_t)scale &&
+                  mark.tmin == __float_as_uint(tmin);
+      for (uint32_t j = 0; same && j < depth; ++j) {
+        const uint2 a = stack[j * stride];
+        same = a.x == mark.stack[2 * j] && a.y == mark.stack[2 * j + 1];
+      }
+      if (same) {
+        const uint32_t period = loops - mark.loops;
+        const uint32_t skip = (max_loops - loops) / period;
+        fetches += skip * (fetches - mark.fetches);
+        loops += skip * period;
+        check_at = max_loops;
+        if (loops == max_loops) {
+          capped();
+          return;
+        }
+      } else if (loops == kCycleFrom || loops == mark.next_save) {
+        mark.node = node;
+        mark.scale = (uint32_t)scale;
+        mark.tmin = __float_as_uint(tmin);
+        mark.loops = loops;
+        mark.fetches = fetches;
+        mark.next_save = 2u * loops;
+        for (uint32_t j = 0; j < depth; ++j) {
+          const uint2 a = stack[j * stride];
+          mark.stack[2 * j] = a.x;
+          mark.stack[2 * j + 1] = a.y;
+        }
+      }
     }
     bool pop;
     if (kFlat)
