@@ -375,7 +375,8 @@ def batched_leg(dev, reps=10):
             "batched_mrays_s": rays / ms_batch / 1e3, "speedup": ms_plain / ms_batch,
             "batched_ms": ms_batch, "per_view_ms": ms_plain,
             "autotuned": {"tile": [best.tile_w, best.tile_h], "block_threads": best.block_threads,
-                          "top_nodes": best.top_nodes, "graph": True}}
+                          "top_nodes": best.top_nodes, "rays_per_lane": best.rays_per_lane,
+                          "graph": True}}
 
 
 def served_leg(dev, n=400, rates=(4000, 16000, 64000)):
@@ -468,7 +469,8 @@ def served_leg(dev, n=400, rates=(4000, 16000, 64000)):
         return {"requests": len(rq), "rays": tp_rays, "mrays_s": tp_rays / span / 1e6,
                 "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                 "failed": len(r) - len(ok), "treelets_paged_in": st.treelets_paged_in,
-                "gb_uploaded": st.bytes_uploaded / 1e9, "paged_unconverged": st.paged_unconverged}
+                "gb_uploaded": st.bytes_uploaded / 1e9, "paged_unconverged": st.paged_unconverged,
+                "analysis_passes": st.analysis_passes, "paging_s": st.paging_us / 1e6}
 
     treelet_paged = {"octrees": big, "octree_gb": [sizes[o] / 1e9 for o in big], "budget_gb": tp_budget / 1e9,
                      "region_gb_each": tp_budget // 2 / 1e9, "rate_1000": run_paged(1000),
@@ -806,7 +808,8 @@ def summarize_legs(legs: dict) -> dict:
         elif key == "batched":
             out[key] = {"per_view_mrays_s": _r(v["per_view_launches_mrays_s"]),
                         "batched_mrays_s": _r(v["batched_mrays_s"]), "speedup": _r(v["speedup"]),
-                        "tile": v["autotuned"]["tile"], "threads": v["autotuned"]["block_threads"]}
+                        "tile": v["autotuned"]["tile"], "threads": v["autotuned"]["block_threads"],
+                        "rays_per_lane": v["autotuned"].get("rays_per_lane", 1)}
         elif key == "served":
             rates = {}
             for k in v["speedup_vs_plain_ungated"]:

@@ -538,6 +538,9 @@ typedef struct svo_batch_cfg {
   uint32_t blocks_per_sm;   /* persistent blocks per SM, 0 = as many as fit  */
   uint32_t top_nodes;       /* records of octree 0 staged in shared memory   */
   uint32_t use_graph;       /* replay a captured CUDA graph                  */
+  uint32_t rays_per_lane;   /* rays a lane casts per tile: 1, 2 or 4 (0 = 1);
+                               a tile is tile_w x (tile_h * rays_per_lane)
+                               pixels, one counter pull per tile              */
 } svo_batch_cfg;
 
 /* The launch unit of the reference is one frame (renderToBuffer enqueue,
@@ -559,9 +562,9 @@ int svo_batcher_set(svo_batcher* b, const svo_octree_desc* octrees, uint32_t num
  * and the kernel are captured as a CUDA graph on the first launch and
  * replayed afterwards. */
 int svo_batcher_launch(svo_batcher* b, svo_stats* d_stats, void* stream);
-/* Times each tile shape, block size and top-node staging on the current
- * batch (`reps` launches each), keeps the fastest as the batch's
- * configuration and returns it with its time per launch. */
+/* Times each tile shape, block size, top-node staging and rays per lane
+ * on the current batch (`reps` launches each), keeps the fastest as the
+ * batch's configuration and returns it with its time per launch. */
 int svo_batcher_autotune(svo_batcher* b, uint32_t reps, void* stream, svo_batch_cfg* best,
                          float* best_ms);
 /* Total tiles and rays of the current batch. */
@@ -640,6 +643,9 @@ typedef struct svo_server_stats {
   uint32_t paged_unconverged; /* paged requests cast after the last analysis
                                  pass still placed treelets (region too small
                                  for the view)                                */
+  uint64_t analysis_passes;   /* analysis passes run for paged requests       */
+  uint64_t paging_us;         /* time paged workers spent in those passes and
+                                 their uploads, summed over workers           */
 } svo_server_stats;
 
 typedef struct svo_server svo_server;

@@ -122,7 +122,8 @@ class svo_view_desc(ctypes.Structure):
 class svo_batch_cfg(ctypes.Structure):
     _fields_ = [("tile_w", ctypes.c_uint32), ("tile_h", ctypes.c_uint32),
                 ("block_threads", ctypes.c_uint32), ("blocks_per_sm", ctypes.c_uint32),
-                ("top_nodes", ctypes.c_uint32), ("use_graph", ctypes.c_uint32)]
+                ("top_nodes", ctypes.c_uint32), ("use_graph", ctypes.c_uint32),
+                ("rays_per_lane", ctypes.c_uint32)]
 
 
 class svo_shadow_cfg(ctypes.Structure):
@@ -783,10 +784,12 @@ def trace_rays(d_nodes, num_nodes: int, d_origins, d_dirs, n: int, t_scale_ratio
 
 
 # ---- batched views -------------------------------------------------------------
-def batch_cfg(tile_w=8, tile_h=4, block_threads=256, blocks_per_sm=0, top_nodes=0, use_graph=True):
+def batch_cfg(tile_w=8, tile_h=4, block_threads=256, blocks_per_sm=0, top_nodes=0, use_graph=True,
+              rays_per_lane=1):
     c = svo_batch_cfg()
     c.tile_w, c.tile_h, c.block_threads = tile_w, tile_h, block_threads
     c.blocks_per_sm, c.top_nodes, c.use_graph = blocks_per_sm, top_nodes, int(bool(use_graph))
+    c.rays_per_lane = rays_per_lane
     return c
 
 
@@ -892,7 +895,8 @@ class svo_server_stats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in ("requests_done", "rays_done", "batches", "octree_loads",
                                                 "octree_evictions", "treelets_paged_in",
                                                 "bytes_uploaded", "resident_bytes")] + \
-               [("resident_octrees", ctypes.c_uint32), ("paged_unconverged", ctypes.c_uint32)]
+               [("resident_octrees", ctypes.c_uint32), ("paged_unconverged", ctypes.c_uint32),
+                ("analysis_passes", ctypes.c_uint64), ("paging_us", ctypes.c_uint64)]
 
 
 for _name, (_args, _res) in {

@@ -3,13 +3,14 @@
 //
 // The reference renders one frame per kernel enqueue
 // (raycast_serialized_opencl.cpp:729-747).  Here the launch unit is a ragged
-// table of views: every view is cut into tiles of 32 pixels (tile_w x
-// tile_h), the tiles of all views are numbered one after another, and a
-// persistent grid of warps pulls tile numbers from a global counter until
-// the table is exhausted.  A warp finds its view by binary search over the
-// views' first tile numbers, casts its 32 rays with the same traversal as the
-// per-frame kernel, and writes RGBA8 (and optional hit records) into that
-// view's output.  Blocks may stage the top records of octree 0 in shared
+// table of views: every view is cut into tiles of 32 x R pixels (tile_w x
+// tile_h*R, R rays per lane), the tiles of all views are numbered one after
+// another, and a persistent grid of warps pulls tile numbers from a global
+// counter until the table is exhausted.  A warp finds its view by binary
+// search over the views' first tile numbers, casts the tile's rays with the
+// same traversal as the per-frame kernel (a lane takes R of them, one below
+// the other tile_h rows apart), and writes RGBA8 (and optional hit records)
+// into that view's output.  Blocks may stage the top records of octree 0 in shared
 // memory.  Everything the launch reads lives in device descriptor tables, so
 // the counter reset plus the launch are captured once as a CUDA graph and
 // replayed.
@@ -68,8 +69,8 @@ template <int TW, int TH, bool kExt, bool kTreelet>
 __global__ void batch_kernel(const BatchView* __restrict__ views, uint32_t num_views,
                              const BatchOctree* __restrict__ octrees, uint64_t total_tiles,
                              unsigned long long* __restrict__ counter, svo_stats* stats, int max_s,
-                             uint32_t top_nodes) {
-  static_assert(TW * TH == 32, "a tile is one warp of rays");
+                             uint32_t top_nodes, uint32_t rays_per_lane) {
+  static_assert(TW * TH == 32, "a tile row is one warp of rays");
   extern __shared__ uint2 smem[];
   uint2* stack = smem + threadIdx.x;
   const int stride = blockDim.x;
@@ -99,17 +100,20 @@ __global__ void batch_kernel(const BatchView* __restrict__ views, uint32_t num_v
     const BatchView& v = views[lo];
     const uint64_t local = tile - v.tile_begin;
     const uint32_t ty = (uint32_t)(local / v.tiles_x), tx = (uint32_t)(local % v.tiles_x);
-    const uint32_t x = tx * TW + lane % TW, y = ty * TH + lane / TW;
-    if (x < v.params.width && y < v.params.height) {
-      const BatchOctree& oct = octrees[v.octree];
-      trace_tile_pixel<kExt, kTreelet>(v, oct, x, y, top, v.octree == 0 ? top_count : 0u, stack, stride, stats);
+    const uint32_t x = tx * TW + lane % TW;
+    const BatchOctree& oct = octrees[v.octree];
+    for (uint32_t r = 0; r < rays_per_lane; ++r) {
+      const uint32_t y = (ty * rays_per_lane + r) * TH + lane / TW;
+      if (x < v.params.width && y < v.params.height)
+        trace_tile_pixel<kExt, kTreelet>(v, oct, x, y, top, v.octree == 0 ? top_count : 0u, stack, stride,
+                                         stats);
     }
     __syncwarp();
   }
 }
 
 typedef void (*BatchKernelFn)(const BatchView*, uint32_t, const BatchOctree*, uint64_t,
-                              unsigned long long*, svo_stats*, int, uint32_t);
+                              unsigned long long*, svo_stats*, int, uint32_t, uint32_t);
 
 template <bool kExt, bool kTreelet>
 BatchKernelFn kernel_for_t(uint32_t tw, uint32_t th) {
@@ -157,8 +161,9 @@ int launch_batch(const BatchLaunch& L, cudaStream_t stream) {
   if (smem > 48u * 1024u) {
     SVO_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   }
+  if (L.rays_per_lane < 1 || L.rays_per_lane > 4) return SVO_ERR_RANGE;
   fn<<<L.blocks, L.threads, smem, stream>>>(L.views, L.num_views, L.octrees, L.total_tiles,
-                                             L.counter, L.stats, L.max_s, L.top_nodes);
+                                             L.counter, L.stats, L.max_s, L.top_nodes, L.rays_per_lane);
   return cuda_status(cudaGetLastError());
 }
 

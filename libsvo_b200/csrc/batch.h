@@ -40,6 +40,7 @@ struct BatchLaunch {
   int max_s = 13;
   uint32_t top_nodes = 0;
   uint32_t tile_w = 8, tile_h = 4;
+  uint32_t rays_per_lane = 1;  // a tile is tile_w x (tile_h * rays_per_lane) pixels
   uint32_t threads = 256, blocks = 0;
   bool ext = false;           // some view uses view mode 2, 6 or 7
   bool treelet_only = false;  // treelet traversal everywhere, nothing staged

@@ -83,6 +83,8 @@ int check_cfg(const svo_batch_cfg& c) {
   if (!svo::batch_tile_supported(c.tile_w, c.tile_h)) return SVO_ERR_NOTSUP;
   if (c.block_threads < 64 || c.block_threads > 1024 || c.block_threads % 32) return SVO_ERR_RANGE;
   if (c.top_nodes > 16384) return SVO_ERR_RANGE;
+  if (c.rays_per_lane != 0 && c.rays_per_lane != 1 && c.rays_per_lane != 2 && c.rays_per_lane != 4)
+    return SVO_ERR_RANGE;
   return SVO_OK;
 }
 
@@ -92,7 +94,9 @@ int apply(svo_batcher* b, const svo_batch_cfg& c, cudaStream_t stream) {
   if (rc != SVO_OK) return rc;
   const uint32_t nv = (uint32_t)b->views.size(), no = (uint32_t)b->octrees.size();
   SVO_CUDA_TRY(cudaStreamSynchronize(stream));  // staging may still feed earlier copies
-  const uint64_t tiles = svo::layout_views(b->views.data(), nv, no, c.tile_w, c.tile_h, b->h_views);
+  const uint32_t rays_per_lane = c.rays_per_lane ? c.rays_per_lane : 1u;
+  const uint64_t tiles =
+      svo::layout_views(b->views.data(), nv, no, c.tile_w, c.tile_h * rays_per_lane, b->h_views);
   if (tiles == 0) return SVO_ERR_INVALID;
   int max_s = 2;
   for (uint32_t i = 0; i < no; ++i) {
@@ -121,6 +125,7 @@ int apply(svo_batcher* b, const svo_batch_cfg& c, cudaStream_t stream) {
   L.top_nodes = c.top_nodes;
   L.tile_w = c.tile_w;
   L.tile_h = c.tile_h;
+  L.rays_per_lane = rays_per_lane;
   L.threads = c.block_threads;
   L.ext = svo::batch_needs_ext(b->h_views, nv);
   L.treelet_only = svo::batch_treelet_only(b->h_octrees, no, c.top_nodes);
@@ -224,6 +229,7 @@ int svo_batcher_autotune(svo_batcher* b, uint32_t reps, void* stream, svo_batch_
   static const uint32_t shapes[][2] = {{8, 4}, {16, 2}, {4, 8}, {32, 1}};
   static const uint32_t threads[] = {128, 256, 512};
   static const uint32_t tops[] = {0, 1024};
+  static const uint32_t rays[] = {1, 2, 4};
   const svo_batch_cfg base = b->cfg;
   svo_batch_cfg win = base;
   float win_ms = 1e30f;
@@ -231,31 +237,37 @@ int svo_batcher_autotune(svo_batcher* b, uint32_t reps, void* stream, svo_batch_
   SVO_CUDA_TRY(cudaEventCreate(&e0));
   SVO_CUDA_TRY(cudaEventCreate(&e1));
   int rc = SVO_OK;
+  std::vector<svo_batch_cfg> cands;
   for (const auto& sh : shapes)
     for (uint32_t t : threads)
-      for (uint32_t top : tops) {
-        svo_batch_cfg c = base;
-        c.tile_w = sh[0];
-        c.tile_h = sh[1];
-        c.block_threads = t;
-        c.top_nodes = top;
-        c.use_graph = 0;
-        if (apply(b, c, s) != SVO_OK) continue;  // e.g. does not fit in shared memory
-        rc = launch_plain(b, nullptr, s);  // warm-up
-        if (rc != SVO_OK) break;
-        rc = svo::cuda_status(cudaEventRecord(e0, s));
-        for (uint32_t r = 0; r < reps && rc == SVO_OK; ++r) rc = launch_plain(b, nullptr, s);
-        if (rc == SVO_OK) rc = svo::cuda_status(cudaEventRecord(e1, s));
-        if (rc == SVO_OK) rc = svo::cuda_status(cudaEventSynchronize(e1));
-        float ms = 0.0f;
-        if (rc == SVO_OK) rc = svo::cuda_status(cudaEventElapsedTime(&ms, e0, e1));
-        if (rc != SVO_OK) break;
-        ms /= (float)reps;
-        if (ms < win_ms) {
-          win_ms = ms;
-          win = c;
+      for (uint32_t top : tops)
+        for (uint32_t rpl : rays) {
+          svo_batch_cfg c = base;
+          c.tile_w = sh[0];
+          c.tile_h = sh[1];
+          c.block_threads = t;
+          c.top_nodes = top;
+          c.rays_per_lane = rpl;
+          c.use_graph = 0;
+          cands.push_back(c);
         }
-      }
+  for (const svo_batch_cfg& c : cands) {
+    if (apply(b, c, s) != SVO_OK) continue;  // e.g. does not fit in shared memory
+    rc = launch_plain(b, nullptr, s);  // warm-up
+    if (rc != SVO_OK) break;
+    rc = svo::cuda_status(cudaEventRecord(e0, s));
+    for (uint32_t r = 0; r < reps && rc == SVO_OK; ++r) rc = launch_plain(b, nullptr, s);
+    if (rc == SVO_OK) rc = svo::cuda_status(cudaEventRecord(e1, s));
+    if (rc == SVO_OK) rc = svo::cuda_status(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    if (rc == SVO_OK) rc = svo::cuda_status(cudaEventElapsedTime(&ms, e0, e1));
+    if (rc != SVO_OK) break;
+    ms /= (float)reps;
+    if (ms < win_ms) {
+      win_ms = ms;
+      win = c;
+    }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc != SVO_OK) return rc;

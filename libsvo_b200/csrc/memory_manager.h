@@ -87,6 +87,23 @@ class TreeletMemoryManager {
     for (uint32_t i = 1; i < slots_.size(); ++i)
       if (slots_[i].treelet_gid >= 0) slots_[i].visibility = -1;
   }
+  // After an analysis step that placed nothing, the steps that follow for
+  // the same view see the same pool and repeat it, except that treelets the
+  // view does not see count down towards eviction.  This jumps to the end of
+  // that countdown (every treelet the last step did not see becomes
+  // invisible at once) and returns whether that changed any slot; false
+  // means the treelets the view sees fill the pool and no further step can
+  // place anything.
+  bool expire_unseen() {
+    bool changed = false;
+    for (uint32_t i = 1; i < slots_.size(); ++i)
+      if (slots_[i].treelet_gid >= 0 && slots_[i].visibility >= 0 &&
+          slots_[i].visibility < kMaxVisibility) {
+        slots_[i].visibility = -1;
+        changed = true;
+      }
+    return changed;
+  }
   // freeIncorePosition evicts a treelet only when it and its parent are both
   // invisible (src/TreeletMemoryManager.cpp:571-579); since the root's slot
   // never ages, the root's own sub-treelets then stay for good.  With `any`

@@ -307,21 +307,31 @@ void paged_worker_loop(svo_server* s, uint32_t id) {
     bool converged = false;
     // a new view: what it does not see may make room at once
     mm->mark_all_unseen();
+    const auto paging_start = std::chrono::steady_clock::now();
+    uint32_t passes = 0;
     for (uint32_t step = 0; step < kMaxPagingSteps; ++step) {
-      // converged when the pass asks for nothing new; a pass may also place
-      // nothing because the region is full of treelets still marked visible
-      // from earlier views, whose visibility runs down pass by pass until
-      // they can be evicted
+      // converged when the pass asks for nothing new.  A pass that places
+      // nothing leaves the pool as it was, so the next passes would repeat
+      // it while the treelets this view does not see count down to
+      // eviction: skip to the end of the countdown, or, when the view sees
+      // every treelet of the region, stop (the view does not fit and is
+      // cast from what is resident, coarser where treelets are missing)
       uint32_t nw = 0, old = 0, asked = 0;
       rc = mm->analysis_step(r.params, 1, 0.0f, 0.0f, S, w->stream, &nw, &old, &asked);
       if (rc != SVO_OK) break;
+      ++passes;
       placed += nw;
       if (asked == 0) {
         converged = true;
         break;
       }
+      if (nw == 0 && !mm->expire_unseen()) break;
     }
     if (rc == SVO_OK) rc = mm->wait_uploads(w->stream);
+    if (rc == SVO_OK) rc = svo::cuda_status(cudaStreamSynchronize(w->stream));
+    const uint64_t paging_us = (uint64_t)std::chrono::duration_cast<std::chrono::microseconds>(
+                                   std::chrono::steady_clock::now() - paging_start)
+                                   .count();
     if (rc == SVO_OK) {
       const svo_trace_cfg tc{SVO_TRAVERSAL_TREELET, S};
       rc = svo::launch_render(mm->device_nodes(), mm->device_attribs(), mm->incore_nodes(), r.params, tc,
@@ -337,6 +347,8 @@ void paged_worker_loop(svo_server* s, uint32_t id) {
     s->stats.rays_done += (uint64_t)r.params.width * r.params.height;
     s->stats.treelets_paged_in += placed;
     s->stats.bytes_uploaded += placed * slot_bytes;
+    s->stats.analysis_passes += passes;
+    s->stats.paging_us += paging_us;
     if (rc == SVO_OK && !converged) s->stats.paged_unconverged++;
     s->cv_user.notify_all();
   }

@@ -150,9 +150,11 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
                                         const float o[3], float dx, float dy, float dz, float rx,
                                         float px, float ry, float py, float rz, float pz,
                                         float t_min, float t_max, float tsr, int S, uint2* stack,
-                                        int stride, RayHit& h) {
+                                        int stride, RayHit& h, uint32_t loop_cap) {
   const float eps = 0.00001f;
-  const uint32_t max_loops = (uint32_t)((S + 1) * (S + 1) * 5);
+  // the reference's watchdog, or the caller's smaller cap (cost estimates)
+  const uint32_t watchdog = (uint32_t)((S + 1) * (S + 1) * 5);
+  const uint32_t max_loops = loop_cap && loop_cap < watchdog ? loop_cap : watchdog;
   int scale = S - 1;
   uint32_t node = 0u;
   float tmin = t_min, tmax = t_max;
@@ -391,11 +393,14 @@ __device__ __forceinline__ void descend(const Fetch& fetch, uint64_t num_nodes,
   h.fetches = fetches;
 }
 
-// One ray: root box test, direction clamp, then the descent.
+// One ray: root box test, direction clamp, then the descent.  loop_cap > 0
+// stops the ray after that many iterations instead of the watchdog's (S+1)^2*5
+// (used only to estimate costs; results under a cap are not the reference's).
 template <bool kFlat, class Fetch>
 __device__ __forceinline__ RayHit cast_ray(const Fetch& fetch, uint64_t num_nodes,
                                            const float o[3], float dx, float dy, float dz,
-                                           float tsr, int S, uint2* stack, int stride) {
+                                           float tsr, int S, uint2* stack, int stride,
+                                           uint32_t loop_cap = 0u) {
   RayHit h;
   h.node = 0u;
   h.t = 0.0f;
@@ -444,10 +449,10 @@ __device__ __forceinline__ RayHit cast_ray(const Fetch& fetch, uint64_t num_node
                         __float_as_uint(o[2]) == 0x80000000u;
   if (isfinite(rx) && isfinite(ry) && isfinite(rz) && !neg_zero)
     descend<kFlat, true>(fetch, num_nodes, o, dx, dy, dz, rx, px, ry, py, rz, pz, t_min, t_max,
-                         tsr, S, stack, stride, h);
+                         tsr, S, stack, stride, h, loop_cap);
   else
     descend<kFlat, false>(fetch, num_nodes, o, dx, dy, dz, rx, px, ry, py, rz, pz, t_min, t_max,
-                          tsr, S, stack, stride, h);
+                          tsr, S, stack, stride, h, loop_cap);
   return h;
 }
 

@@ -102,6 +102,24 @@ def test_mixed_batch_matches_per_frame(octrees, cuda, tile):
     b.close()
 
 
+@pytest.mark.parametrize("tile,rays_per_lane", [((8, 4), 2), ((16, 2), 4), ((32, 1), 4), ((4, 8), 2)])
+def test_rays_per_lane_matches_per_frame(octrees, cuda, tile, rays_per_lane):
+    """A lane casting 2 or 4 rays of a taller tile: same pixels and hit records
+    as the per-frame kernel (views whose height is no multiple of the tile's
+    included)."""
+    torch = _torch()
+    views, bufs, params = make_views(cuda)
+    b = L.Batcher(max_views=64, max_octrees=8)
+    b.set(octrees["descs"], views, L.batch_cfg(*tile, use_graph=False, rays_per_lane=rays_per_lane))
+    b.launch()
+    torch.cuda.synchronize()
+    check_batch(octrees, bufs, params, cuda)
+    tiles, rays = b.size()
+    assert rays == sum(w * h for _, w, h, *_ in VIEWS)
+    assert tiles >= rays // (32 * rays_per_lane)
+    b.close()
+
+
 def test_graph_replay_and_staged_top_nodes(octrees, cuda):
     torch = _torch()
     views, bufs, params = make_views(cuda)
@@ -137,6 +155,9 @@ def test_batch_argument_errors(octrees, cuda):
     b = L.Batcher(max_views=4, max_octrees=2)
     with pytest.raises(L.SvoError) as e:
         b.set(octrees["descs"], views)
+    assert e.value.code == L.SVO_ERR_RANGE
+    with pytest.raises(L.SvoError) as e:
+        b.set(octrees["descs"][:2], views[:1], L.batch_cfg(rays_per_lane=3))
     assert e.value.code == L.SVO_ERR_RANGE
     bad = L.view_desc(params[0], 7, bufs[0][0])
     with pytest.raises(L.SvoError) as e:

@@ -10,7 +10,8 @@
   the largest) carry hit records and are compared in full;
 * the large primary + shadow frame: the icosphere subdivided 9 times (5.2 M
   triangles) built on the GPU, 3840x2160 primary rays and one shadow ray per
-  hit, compared over a band of 96 rows.  The test uses the depth-12 octree
+  hit, compared over a band of 96 rows, and the primary frame alone over
+  three bands (top, middle, bottom rows).  The test uses the depth-12 octree
   (a 2.6 GB pool, copied to host memory for the CPU side); bench.py's
   large_shadowed measurement makes the same comparison over the depth-14
   pool (40.3 GB) when the host has the memory for its copy.
@@ -150,8 +151,20 @@ def test_large_shadowed_frame_band(cuda):
     got_rgba = rgba.cpu().numpy().view(np.uint32)[y0:y1]
     got = _hits(hb).reshape(p.height, p.width)[y0:y1]
     got_s = _hits(sb).reshape(p.height, p.width)[y0:y1]
+    # the primary frame alone: 64,800 blocks cast in estimated-cost order
+    # (the sort's per-block costs take 64 KB of shared memory)
+    pb = torch.empty(px * 16, dtype=torch.uint8, device=cuda)
+    L.render(d_nodes, d_attribs, n, p, rgba, pb, cfg=cfg)
+    torch.cuda.synchronize()
+    got_p = _hits(pb).reshape(p.height, p.width)
     nodes, attribs = wl.scene.getIncoreBuffer()
     wl.scene.close()
+    o, d = oracle.pixel_rays(bytes(p))
+    for r0, r1 in ((0, 16), (y0, y1), (p.height - 16, p.height)):
+        sl = slice(r0 * p.width, r1 * p.width)
+        want, _ = oracle.cast_rays(nodes, o[sl], d[sl], p.t_scale_ratio, stack_size=wl.stack_size)
+        assert_hits_equal(got_p[r0:r1], want, f"large primary frame rows {r0}-{r1}")
+    assert got_p[y0:y1]["hit"].sum() > 100_000
     o_rgba, o_hits, o_shadow, _, _ = oracle.render_shadow(nodes, attribs, bytes(p), wl.light,
                                                          stack_size=wl.stack_size, rows=(y0, y1))
     assert_hits_equal(got, o_hits, "large frame band, primary rays")
