@@ -52,10 +52,10 @@ def build(force: bool = False) -> Path:
     return LIB
 
 
-def build_reference(force: bool = False):
+def build_reference(force: bool = False, reference=None):
     from . import build_ref
 
-    return build_ref.build(force=force)
+    return build_ref.build(force=force, reference=reference)
 
 
 _lib = None

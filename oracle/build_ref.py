@@ -1,7 +1,8 @@
 """Builds the reference's own OpenCL C ray cast as a host shared library.
 
 TEST INFRASTRUCTURE ONLY.  Reads ``opencl/treeletRenderer_rgba.cl`` from the
-reference checkout (default ``/root/reference``, or ``$LIBSVO_REFERENCE``),
+reference checkout named by ``$LIBSVO_REFERENCE`` (or the path given on the
+command line: ``python oracle/build_ref.py <reference checkout>``),
 rewrites its OpenCL vector literals ``(float3)(...)`` to ``make_float3(...)``
 in memory, and pipes ``#include cl_shim.h`` + that text + ``ref_harness.inc``
 to g++ over stdin.  No reference source is written to disk; the only output
@@ -24,8 +25,10 @@ OUT = OUT_DIR / "libsvo_ref_cl.so"
 CL_REL = "opencl/treeletRenderer_rgba.cl"
 
 
-def reference_root() -> Path:
-    return Path(os.environ.get("LIBSVO_REFERENCE", "/root/reference"))
+def reference_root() -> Path | None:
+    """The reference checkout named by $LIBSVO_REFERENCE, or None."""
+    root = os.environ.get("LIBSVO_REFERENCE")
+    return Path(root) if root else None
 
 
 def transformed_source(cl_text: str) -> str:
@@ -37,11 +40,13 @@ def transformed_source(cl_text: str) -> str:
     )
 
 
-def build(force: bool = False) -> Path | None:
-    """Compiles the reference kernel for the host; returns the .so path, or
-    None when the reference checkout is not present on this machine."""
-    cl = reference_root() / CL_REL
-    if not cl.is_file():
+def build(force: bool = False, reference: Path | str | None = None) -> Path | None:
+    """Compiles the reference kernel for the host from the checkout at
+    `reference` (default: $LIBSVO_REFERENCE); returns the .so path, or the
+    one built earlier, or None when no checkout is named or present."""
+    root = Path(reference) if reference else reference_root()
+    cl = root / CL_REL if root else None
+    if cl is None or not cl.is_file():
         return OUT if OUT.is_file() else None
     deps = [cl, HERE / "cl_shim.h", HERE / "ref_harness.inc", Path(__file__)]
     if OUT.is_file() and not force:
@@ -58,5 +63,6 @@ def build(force: bool = False) -> Path | None:
 
 
 if __name__ == "__main__":
-    p = build(force="--force" in sys.argv)
+    paths = [a for a in sys.argv[1:] if not a.startswith("--")]
+    p = build(force="--force" in sys.argv, reference=paths[0] if paths else None)
     print(p if p else "reference not present; nothing built")

@@ -6,7 +6,8 @@ import pytest
 import libsvo_b200 as L
 from oracle.build_ref import reference_root
 
-REF_PLY = reference_root() / "data" / "meshes" / "frog2_seperated.ply"
+# the reference's sample scan, where $LIBSVO_REFERENCE names its checkout
+REF_PLY = (reference_root() / "data" / "meshes" / "frog2_seperated.ply") if reference_root() else None
 
 
 def write_ply(path, v, t, n=None, c=None, binary=True, quads=False):
@@ -90,7 +91,8 @@ def test_fit_unit_cube():
     assert np.allclose(rn[:, 2], fn[:, 1], atol=1e-5) and np.allclose(rn[:, 1], -fn[:, 2], atol=1e-5)
 
 
-@pytest.mark.skipif(not REF_PLY.is_file(), reason="the reference checkout's sample mesh is not present")
+@pytest.mark.skipif(REF_PLY is None or not REF_PLY.is_file(),
+                    reason="the reference checkout's sample mesh is not present")
 def test_reference_sample_mesh_builds():
     """The reference's own sample mesh (a scanned frog with per-vertex normals
     and colours) through the builder's placement and the attributed build."""
