@@ -23,23 +23,104 @@ constexpr int kBlockW = 16;  // 128 threads: finer blocks balance the tail of a 
 constexpr int kBlockH = 8;
 constexpr int kThreads = kBlockW * kBlockH;
 
+// ---- longest-first dispatch ------------------------------------------------
+// A frame's blocks differ in cost by two orders of magnitude (rays that graze
+// a surface run hundreds of iterations, most rays a dozen), and raster order
+// starts some of the longest blocks last, where they run on after the other
+// SMs are done.  Large frames therefore estimate each 16x8 block's cost first
+// (its two 8x8 cells' top-left rays, cut off at kCostCap iterations) and
+// append the block to the list of its cost bucket; block r of the frame
+// kernel then casts the r-th block of the buckets taken costliest first.
+// Every pixel is still cast by the same code: only the order the blocks
+// start in changes.  On the 1920x1080 icosphere frame the ordered frame
+// kernel takes 254 us against 311 us in raster order, about the 246 us of
+// its longest block alone.  The estimate is a chain of dependent node reads
+// per ray, so its time grows with the cap: 48 iterations measured best (32
+// and 96 order the frame worse or cost more than they save).
+constexpr uint32_t kCostCap = 48;
+constexpr uint32_t kCostBuckets = kCostCap + 1;
+constexpr uint32_t kCostSamples = kBlockW / 8;  // one ray per 8x8 cell of a block
+constexpr uint64_t kOrderMinPixels = 1ull << 20;
+constexpr uint32_t kOrderMaxBlocks = 1u << 20;
+static_assert(kCostSamples == 2, "a block's cost is the larger of two adjacent lanes' samples");
+static_assert(kCostBuckets > 32 && kCostBuckets <= 64, "one warp scans the buckets, two per lane");
+
+// count[k]: blocks of estimated cost k; list[k * nblocks + j]: the j-th of
+// them.  count == nullptr: raster order.
+struct BlockOrder {
+  const uint32_t* count;
+  const uint32_t* list;
+  uint32_t nblocks;
+};
+
+// The lanes of the warp whose key equals this lane's, for keys below 128:
+// seven ballots, one per key bit.  All 32 lanes take part.
+__device__ __forceinline__ uint32_t same_key_lanes(uint32_t k) {
+  uint32_t peers = 0xFFFFFFFFu;
+#pragma unroll
+  for (int bit = 0; bit < 7; ++bit) {
+    const bool set = (k >> bit) & 1u;
+    const uint32_t b = __ballot_sync(0xFFFFFFFFu, set);
+    peers &= set ? b : ~b;
+  }
+  return peers;
+}
+
+// The r-th block in cost order (buckets kCostCap down to 0, each in the
+// order its blocks were appended).  Called by one whole warp; every lane
+// returns the block.
+__device__ __forceinline__ uint32_t ordered_block(const BlockOrder& o, uint32_t r, uint32_t lane) {
+  const uint32_t k1 = lane + 32 < kCostBuckets ? kCostCap - 32 - lane : 0u;
+  const uint32_t c0 = __ldg(o.count + (kCostCap - lane));
+  const uint32_t c1 = lane + 32 < kCostBuckets ? __ldg(o.count + k1) : 0u;
+  uint32_t p0 = c0, p1 = c1;  // inclusive prefix sums, bucket kCostCap first
+  for (uint32_t d = 1; d < 32; d <<= 1) {
+    const uint32_t y0 = __shfl_up_sync(0xFFFFFFFFu, p0, d);
+    const uint32_t y1 = __shfl_up_sync(0xFFFFFFFFu, p1, d);
+    if (lane >= d) {
+      p0 += y0;
+      p1 += y1;
+    }
+  }
+  p1 += __shfl_sync(0xFFFFFFFFu, p0, 31);
+  uint32_t m = __ballot_sync(0xFFFFFFFFu, p0 > r);
+  uint32_t bucket, before;
+  if (m != 0u) {
+    const int l = __ffs(m) - 1;
+    bucket = kCostCap - (uint32_t)l;
+    before = __shfl_sync(0xFFFFFFFFu, p0 - c0, l);
+  } else {
+    m = __ballot_sync(0xFFFFFFFFu, p1 > r);
+    if (m == 0u) return r;  // not reached: the buckets hold every block once
+    const int l = __ffs(m) - 1;
+    bucket = kCostCap - 32 - (uint32_t)l;
+    before = __shfl_sync(0xFFFFFFFFu, p1 - c1, l);
+  }
+  return __ldg(o.list + (uint64_t)bucket * o.nblocks + (r - before));
+}
+
 // kExt: view modes 2, 6 and 7 (shade_ext); the other modes compile without
-// the extra exit state.  `order` (optional, 1-D grid): block b casts the
-// 16x8 block order[b] of a frame gx blocks wide, so blocks go to the SMs in
-// that order; without it the grid is the frame's blocks in raster order.
+// the extra exit state.  With `order` (1-D grid) block r casts the r-th block
+// in estimated-cost order of a frame gx blocks wide; without it the grid is
+// the frame's blocks in raster order.
 template <bool kFlat, bool kExt>
 __global__ void __launch_bounds__(kThreads) render_frame_kernel(
     const uint2* __restrict__ nodes, const uint2* __restrict__ attribs, uint64_t num_nodes,
     const svo_frame_params p, int S, uint32_t* __restrict__ rgba, svo_hit* __restrict__ hits,
-    svo_stats* __restrict__ stats, uint32_t y0, const uint32_t* __restrict__ order, uint32_t gx) {
+    svo_stats* __restrict__ stats, uint32_t y0, const BlockOrder order, uint32_t gx) {
   extern __shared__ uint2 stack_smem[];
   const int t = threadIdx.x;
   const int warp = t >> 5, lane = t & 31;
   uint32_t bx = blockIdx.x, by = blockIdx.y;
-  if (order != nullptr) {
-    const uint32_t b = order[blockIdx.x];
-    bx = b % gx;
-    by = b / gx;
+  if (order.count != nullptr) {
+    __shared__ uint32_t block;
+    if (warp == 0) {
+      const uint32_t b = ordered_block(order, blockIdx.x, (uint32_t)lane);
+      if (lane == 0) block = b;
+    }
+    __syncthreads();
+    bx = block % gx;
+    by = block / gx;
   }
   // warp w covers pixels [8*(w&1), +8) x [4*(w>>1), +4) of the 16x8 block;
   // rows start at y0 (frames taller than one grid's rows take several launches)
@@ -57,163 +138,38 @@ __global__ void __launch_bounds__(kThreads) render_frame_kernel(
   count_stats(stats, h);
 }
 
-// ---- longest-first dispatch ------------------------------------------------
-// A frame's blocks differ in cost by two orders of magnitude (rays that graze
-// a surface run hundreds of iterations, most rays a dozen), and raster order
-// starts some of the longest blocks last, where they run on after the other
-// SMs are done.  Large frames therefore estimate each 16x8 block's cost first
-// (its two 8x8 cells' top-left rays, cut off at kCostCap iterations), sort the
-// blocks by it, costliest first, and hand the frame kernel that order.  Every
-// pixel is still cast by the same code: only the order the blocks start in
-// changes.  On the 1920x1080 icosphere frame the ordered frame kernel takes
-// 254 us against 311 us in raster order, about the 246 us of its longest
-// block alone.  The estimate is a chain of dependent node reads per ray, so
-// its time grows with the cap: 48 iterations measured best (32 and 96 order
-// the frame worse or cost more than they save).
-constexpr uint32_t kCostCap = 48;
-constexpr uint32_t kCostSamples = kBlockW / 8;  // one ray per 8x8 cell of a block
-constexpr uint64_t kOrderMinPixels = 1ull << 20;
-constexpr uint32_t kSortThreads = 1024;
-// the sort keeps one byte per block in shared memory
-constexpr uint32_t kOrderMaxBlocks = 160u * 1024u;
-
-// sample_cost[b * 2 + c]: iterations of block b's sample ray c, capped (0
-// for a sample outside the frame).  One byte per sample, every byte written,
-// so the array needs no clearing.
+// The cost estimate: one thread per sample ray, the two samples of block b
+// in lanes 2b and 2b+1 of a warp.  The block's cost (the larger sample,
+// capped) picks its bucket, and the block is appended to that bucket's list
+// (one atomic per bucket and warp, so neighbouring blocks of a bucket stay
+// together).
 template <bool kFlat>
 __global__ void __launch_bounds__(kThreads) block_cost_kernel(
     const uint2* __restrict__ nodes, uint64_t num_nodes, const svo_frame_params p, int S,
-    uint32_t gx, uint32_t nblocks, uint8_t* __restrict__ sample_cost) {
+    uint32_t gx, uint32_t nblocks, uint32_t* __restrict__ count, uint32_t* __restrict__ list) {
   extern __shared__ uint2 stack_smem[];
   const uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
-  if (i >= (uint64_t)nblocks * kCostSamples) return;
+  const uint32_t lane = threadIdx.x % 32;
+  const bool live = i < (uint64_t)nblocks * kCostSamples;
   const uint32_t b = (uint32_t)(i / kCostSamples), c = (uint32_t)(i % kCostSamples);
   const uint32_t x = (b % gx) * kBlockW + c * 8, y = (b / gx) * kBlockH;
   uint32_t loops = 0u;
-  if (x < p.width && y < p.height) {
+  if (live && x < p.width && y < p.height) {
     float o[3], dx, dy, dz;
     pixel_ray(p, x, y, o, dx, dy, dz);
     loops = cast_ray<kFlat>(GlobalFetch{nodes}, num_nodes, o, dx, dy, dz, p.t_scale_ratio, S,
                             stack_smem + threadIdx.x, kThreads, kCostCap)
                 .loops;
   }
-  sample_cost[i] = (uint8_t)min(loops, kCostCap);
-}
-
-// The lanes of the warp whose key equals this lane's, for keys below 128:
-// seven ballots, one per key bit (cheaper than __match_any_sync, whose
-// latency made the sort several times slower).
-__device__ __forceinline__ uint32_t same_key_lanes(uint32_t k) {
-  uint32_t peers = 0xFFFFFFFFu;
-#pragma unroll
-  for (int bit = 0; bit < 7; ++bit) {
-    const bool set = (k >> bit) & 1u;
-    const uint32_t b = __ballot_sync(0xFFFFFFFFu, set);
-    peers &= set ? b : ~b;
-  }
-  return peers;
-}
-
-// One block of kSortThreads: order[] = block indices sorted by cost,
-// costliest first, blocks of equal cost in raster order (a stable counting
-// sort, so neighbouring blocks of a bucket still start together).  The
-// sample costs come in as 16-byte loads, all of a thread's issued before any
-// is used, and each block's cost (the larger of its two samples) is kept in
-// shared memory.  Warp w sorts the w-th contiguous run of blocks: per-warp
-// bucket counts, one scan over (bucket, warp), then each warp places its run
-// 32 blocks at a time, ranking equal buckets inside a step by lane order.
-// sample_cost is padded to a multiple of 16 bytes.
-__global__ void __launch_bounds__(kSortThreads) block_order_kernel(
-    const uint8_t* __restrict__ sample_cost, uint32_t n, uint32_t* __restrict__ order) {
-  static_assert(kCostSamples == 2, "a block's cost is the larger of two samples");
-  static_assert(kCostCap + 1 < 128, "bucket keys (and the dead-lane key) fit 7 bits");
-  constexpr uint32_t kWarps = kSortThreads / 32, kBuckets = kCostCap + 1;
-  extern __shared__ __align__(16) uint8_t block_cost[];  // n rounded up to 8 bytes
-  __shared__ uint32_t count[kBuckets][kWarps];
-  __shared__ uint32_t warp_total[kWarps];
-  const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  {  // 16 sample bytes -> 8 block costs per load
-    const uint4* src = reinterpret_cast<const uint4*>(sample_cost);
-    const uint32_t vecs = (n + 7) / 8;
-    constexpr uint32_t kUnroll = 8;
-    for (uint32_t base = 0; base < vecs; base += kUnroll * kSortThreads) {
-      uint4 v[kUnroll];
-#pragma unroll
-      for (uint32_t u = 0; u < kUnroll; ++u) {
-        const uint32_t q = base + u * kSortThreads + threadIdx.x;
-        v[u] = q < vecs ? src[q] : make_uint4(0u, 0u, 0u, 0u);
-      }
-#pragma unroll
-      for (uint32_t u = 0; u < kUnroll; ++u) {
-        const uint32_t q = base + u * kSortThreads + threadIdx.x;
-        if (q < vecs) {
-          // byte 2j of __vmaxu4(w, w >> 8) is max(byte 2j, byte 2j+1) of w
-          const uint32_t mx = __vmaxu4(v[u].x, v[u].x >> 8), my = __vmaxu4(v[u].y, v[u].y >> 8);
-          const uint32_t mz = __vmaxu4(v[u].z, v[u].z >> 8), mw = __vmaxu4(v[u].w, v[u].w >> 8);
-          *reinterpret_cast<uint2*>(block_cost + 8 * q) =
-              make_uint2(__byte_perm(mx, my, 0x6420), __byte_perm(mz, mw, 0x6420));
-        }
-      }
-    }
-  }
-  for (uint32_t k = threadIdx.x; k < kBuckets * kWarps; k += kSortThreads) (&count[0][0])[k] = 0;
-  __syncthreads();
-  const uint32_t run = (n + kWarps - 1) / kWarps;
-  const uint32_t lo = min(warp * run, n), hi = min(lo + run, n);
-  for (uint32_t base = lo; base < hi; base += 32) {  // per-warp bucket counts
-    const uint32_t i = base + lane;
-    const uint32_t k = i < hi ? block_cost[i] : kBuckets;  // kBuckets matches no live lane
-    const uint32_t peers = same_key_lanes(k);
-    if (i < hi && __popc(peers & ((1u << lane) - 1u)) == 0) count[k][warp] += __popc(peers);
-    __syncwarp();
-  }
-  __syncthreads();
-  {  // run starts: exclusive scan over j = (kCostCap - bucket) * kWarps + warp
-    constexpr uint32_t kEntries = kBuckets * kWarps;
-    constexpr uint32_t kPer = (kEntries + kSortThreads - 1) / kSortThreads;
-    auto at = [&](uint32_t j) -> uint32_t& { return count[kCostCap - j / kWarps][j % kWarps]; };
-    uint32_t v[kPer], s = 0;
-    for (uint32_t q = 0; q < kPer; ++q) {
-      const uint32_t j = threadIdx.x * kPer + q;
-      v[q] = j < kEntries ? at(j) : 0u;
-      s += v[q];
-    }
-    uint32_t x = s;  // inclusive scan of s over the warp
-    for (uint32_t d = 1; d < 32; d <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
-      if (lane >= d) x += y;
-    }
-    if (lane == 31) warp_total[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-      uint32_t w = warp_total[lane];
-      for (uint32_t d = 1; d < 32; d <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, d);
-        if (lane >= d) w += y;
-      }
-      warp_total[lane] = w;
-    }
-    __syncthreads();
-    uint32_t pos = x - s + (warp ? warp_total[warp - 1] : 0u);
-    for (uint32_t q = 0; q < kPer; ++q) {
-      const uint32_t j = threadIdx.x * kPer + q;
-      if (j < kEntries) {
-        at(j) = pos;
-        pos += v[q];
-      }
-    }
-  }
-  __syncthreads();
-  for (uint32_t base = lo; base < hi; base += 32) {
-    const uint32_t i = base + lane;
-    const bool live = i < hi;
-    const uint32_t k = live ? block_cost[i] : kBuckets;
-    const uint32_t peers = same_key_lanes(k);
-    const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
-    if (live) order[count[k][warp] + rank] = i;
-    __syncwarp();
-    if (live && rank == 0) count[k][warp] += __popc(peers);
-    __syncwarp();
+  const uint32_t cost = min(max(loops, __shfl_xor_sync(0xFFFFFFFFu, loops, 1)), kCostCap);
+  const bool appends = live && c == 0;
+  const uint32_t peers = same_key_lanes(appends ? cost : kCostBuckets) & 0x55555555u;
+  if (appends) {
+    const int first = __ffs(peers) - 1;
+    uint32_t base = 0u;
+    if ((int)lane == first) base = atomicAdd(count + cost, (uint32_t)__popc(peers));
+    base = __shfl_sync(peers, base, first);
+    list[(uint64_t)cost * nblocks + base + __popc(peers & ((1u << lane) - 1u))] = b;
   }
 }
 
@@ -325,39 +281,36 @@ cudaMemPool_t order_pool() {
 }
 
 // Longest-first order of the frame's blocks into *order (stream-ordered
-// scratch the caller frees); false when the frame is small or scratch is not
-// available, and the raster launch is used instead.
+// scratch the caller frees with cudaFreeAsync(order->count)); false when the
+// frame is small or scratch is not available, and the raster launch is used
+// instead.
 bool order_blocks(const uint2* nodes, uint64_t num_nodes, const svo_frame_params& p, int S,
-                  bool flat, uint32_t gx, uint32_t nblocks, cudaStream_t stream, uint32_t** order) {
+                  bool flat, uint32_t gx, uint32_t nblocks, cudaStream_t stream, BlockOrder* order) {
   if ((uint64_t)p.width * p.height < kOrderMinPixels || nblocks > kOrderMaxBlocks) return false;
   cudaMemPool_t pool = order_pool();
   if (!pool) {
     cudaGetLastError();
     return false;
   }
-  // scratch: order[nblocks] (padded to 16 bytes), then the sample costs
-  // (2 bytes a block, padded to whole 16-byte loads of the sort)
-  const size_t padded = (nblocks + 7u) & ~7u;
-  const size_t order_bytes = padded * sizeof(uint32_t);
+  // scratch: the bucket counts (256 bytes), then the bucket lists
+  constexpr size_t kCountBytes = 256;
+  static_assert(kCostBuckets * sizeof(uint32_t) <= kCountBytes, "counts fit their header");
   uint32_t* scratch = nullptr;
-  if (cudaMallocFromPoolAsync((void**)&scratch, order_bytes + 2 * padded, pool, stream) != cudaSuccess) {
+  const size_t bytes = kCountBytes + (size_t)kCostBuckets * nblocks * sizeof(uint32_t);
+  if (cudaMallocFromPoolAsync((void**)&scratch, bytes, pool, stream) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  uint8_t* sample_cost = reinterpret_cast<uint8_t*>(scratch) + order_bytes;
+  uint32_t* list = scratch + kCountBytes / sizeof(uint32_t);
   const uint64_t samples = (uint64_t)nblocks * kCostSamples;
   const unsigned grid = (unsigned)((samples + kThreads - 1) / kThreads);
   const size_t smem = render_smem_bytes(S);
-  if (flat)
-    block_cost_kernel<true><<<grid, kThreads, smem, stream>>>(nodes, num_nodes, p, S, gx, nblocks, sample_cost);
-  else
-    block_cost_kernel<false><<<grid, kThreads, smem, stream>>>(nodes, num_nodes, p, S, gx, nblocks, sample_cost);
-  bool ok = cudaGetLastError() == cudaSuccess;
-  if (ok && padded > 48u * 1024u)
-    ok = cudaFuncSetAttribute(block_order_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)padded) == cudaSuccess;
+  bool ok = cudaMemsetAsync(scratch, 0, kCountBytes, stream) == cudaSuccess;
   if (ok) {
-    block_order_kernel<<<1, kSortThreads, padded, stream>>>(sample_cost, nblocks, scratch);
+    if (flat)
+      block_cost_kernel<true><<<grid, kThreads, smem, stream>>>(nodes, num_nodes, p, S, gx, nblocks, scratch, list);
+    else
+      block_cost_kernel<false><<<grid, kThreads, smem, stream>>>(nodes, num_nodes, p, S, gx, nblocks, scratch, list);
     ok = cudaGetLastError() == cudaSuccess;
   }
   if (!ok) {
@@ -365,7 +318,7 @@ bool order_blocks(const uint2* nodes, uint64_t num_nodes, const svo_frame_params
     cudaGetLastError();
     return false;
   }
-  *order = scratch;
+  *order = BlockOrder{scratch, list, nblocks};
   return true;
 }
 
@@ -386,19 +339,20 @@ int launch_render(const svo_node* nodes, const svo_attrib* attribs, uint64_t num
                   : (ext ? render_frame_kernel<false, true> : render_frame_kernel<false, false>);
   const uint32_t gx = (p.width + kBlockW - 1) / kBlockW;
   const uint64_t nblocks64 = (uint64_t)gx * ((p.height + kBlockH - 1) / kBlockH);
-  uint32_t* order = nullptr;
+  BlockOrder order{nullptr, nullptr, 0u};
   if (nblocks64 <= 0x7FFFFFFFull &&
       order_blocks(n2, num_nodes, p, S, flat, gx, (uint32_t)nblocks64, stream, &order)) {
     fn<<<(unsigned)nblocks64, kThreads, smem, stream>>>(n2, a2, num_nodes, p, S, rgba, hits, stats, 0u,
                                                        order, gx);
     const cudaError_t e = cudaGetLastError();
-    cudaFreeAsync(order, stream);
+    cudaFreeAsync(const_cast<uint32_t*>(order.count), stream);
     return e == cudaSuccess ? SVO_OK : SVO_ERR_CUDA;
   }
   for (uint32_t y0 = 0; y0 < p.height; y0 += kRowsPerLaunch) {
     const uint32_t rows = p.height - y0 < kRowsPerLaunch ? p.height - y0 : kRowsPerLaunch;
     const dim3 grid(gx, (rows + kBlockH - 1) / kBlockH);
-    fn<<<grid, kThreads, smem, stream>>>(n2, a2, num_nodes, p, S, rgba, hits, stats, y0, nullptr, gx);
+    fn<<<grid, kThreads, smem, stream>>>(n2, a2, num_nodes, p, S, rgba, hits, stats, y0,
+                                         BlockOrder{nullptr, nullptr, 0u}, gx);
     if (cudaGetLastError() != cudaSuccess) return SVO_ERR_CUDA;
   }
   return SVO_OK;

@@ -129,6 +129,11 @@ struct ServedOctree {
 // Analysis passes before a paged request gives up converging and renders
 // with what is resident.
 constexpr uint32_t kMaxPagingSteps = 64;
+// A request also stops paging once it has placed this many times its
+// region's slots: a view whose treelets fit is placed once (treelets of
+// earlier views go first, its own stay marked visible while it converges),
+// so beyond that the view is swapping its own treelets in and out.
+constexpr uint32_t kMaxRegionRefills = 2;
 
 struct Request {
   svo_request r{};
@@ -326,6 +331,7 @@ void paged_worker_loop(svo_server* s, uint32_t id) {
         break;
       }
       if (nw == 0 && !mm->expire_unseen()) break;
+      if (placed >= kMaxRegionRefills * mm->num_slots()) break;
     }
     if (rc == SVO_OK) rc = mm->wait_uploads(w->stream);
     if (rc == SVO_OK) rc = svo::cuda_status(cudaStreamSynchronize(w->stream));
