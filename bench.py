@@ -320,10 +320,21 @@ def job_mrays_per_s(world: int, rays_per_rank: int, ms_per_step: float) -> float
 
 
 def _profiled_traffic(workload: str):
-    """DRAM bytes per launch of the workload's frame kernel from the
-    committed ncu summaries (profiles/), or None."""
+    """(DRAM bytes per launch of the workload's frame kernel, the capture
+    they come from) from the committed ncu summaries (profiles/); (None,
+    why) when no capture of the current kernel covers the workload."""
     tp = ROOT / "profiles" / "render_frame_kernel_dram_traffic.json"
-    return json.loads(tp.read_text()).get(workload) if tp.is_file() else None
+    entry = json.loads(tp.read_text()).get(workload) if tp.is_file() else None
+    if not isinstance(entry, dict):
+        return None, "no ncu capture of this workload's kernel"
+    return entry.get("bytes"), entry.get("capture")
+
+
+def _kernels_per_render(p, shadow: bool) -> int:
+    """Kernels of this library one render launches: the per-frame kernel,
+    preceded for primary-ray frames of a million pixels or more by the
+    block-cost estimate of longest-first dispatch (csrc/render.cu)."""
+    return 1 if shadow or p.width * p.height < (1 << 20) else 2
 
 
 def _event_ms(torch, fn, reps):
@@ -776,7 +787,8 @@ def large_shadow_leg(dev, reps=10, cap_gb=60.0, subdivisions=9, depth=14, cpu_ba
            "capped_rays": int(stats[0].item()), "bounds_errors": int(stats[1].item()),
            "roofline": {"algorithmic_bytes_per_frame": algo_bytes, "achieved_gbs": algo_bytes / ms / 1e6,
                         "frac": algo_bytes / ms / 1e6 / peak, "node_reads_per_ray": fetches / rays,
-                        "traffic": _profiled_traffic(wl.name)}}
+                        "traffic": _profiled_traffic(wl.name)[0],
+                        "traffic_source": _profiled_traffic(wl.name)[1]}}
     del flush, rgba
     if cpu_baseline:
         try:
@@ -1108,7 +1120,7 @@ def main():
     if rank == 0:
         peak, peak_kind = load_peaks()
         achieved = algo_bytes / (ms * 1e-3) / 1e9
-        traffic = _profiled_traffic(wl.name + ("_shadow" if shadow else ""))
+        traffic, traffic_source = _profiled_traffic(wl.name + ("_shadow" if shadow else ""))
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -1130,9 +1142,9 @@ def main():
                              "host memory on a second stream (overlapping the next cast), all waited for")
                             + "; host wall clock over the steps, the 256 MB L2 flush of every step included; "
                             "frame parameters travel as kernel arguments"},
-            "gpu_launches": args.steps * len(params),
+            "gpu_launches": args.steps * sum(_kernels_per_render(p, shadow) for p in params),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
+                         "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_source,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                          if peak_kind == "measured" else "fallback 6650 GB/s",
                          "algorithmic_bytes_per_step": algo_bytes,

@@ -707,11 +707,14 @@ int TreeletMemoryManagerCuda::analyse_feedback_device(
 
 int TreeletMemoryManagerCuda::feedback_scratch(uint64_t records, svo_feedback** out) {
   if (records > d_feedback_records_) {
+    // grown at least twofold (cudaFree waits for the whole device, so views
+    // of random sizes should reallocate only a few times)
+    const uint64_t grow = std::max<uint64_t>(records, 2 * d_feedback_records_);
     cudaFree(d_feedback_);
     d_feedback_ = nullptr;
     d_feedback_records_ = 0;
-    SVO_CUDA_TRY(cudaMalloc(&d_feedback_, records * sizeof(svo_feedback)));
-    d_feedback_records_ = records;
+    SVO_CUDA_TRY(cudaMalloc(&d_feedback_, grow * sizeof(svo_feedback)));
+    d_feedback_records_ = grow;
   }
   *out = d_feedback_;
   return SVO_OK;
