@@ -71,20 +71,28 @@ int TreeletMemoryManager::insert_treelet(const SlotInfo& tve) {
   slots_[slot] = tve;
   slot_of_[gid] = (int32_t)slot;
   const uint64_t pos = (uint64_t)slot * N_;
-  std::memcpy(incore_ + pos, t.nodes.data(), (size_t)t.num_nodes * sizeof(svo_node));
-  std::memset(incore_ + pos + t.num_nodes, 0, (size_t)(N_ - t.num_nodes) * sizeof(svo_node));
-  std::memcpy(incore_attr_ + pos, t.attribs.data(), (size_t)t.num_nodes * sizeof(svo_attrib));
-  std::memset(incore_attr_ + pos + t.num_nodes, 0, (size_t)(N_ - t.num_nodes) * sizeof(svo_attrib));
+  if (defer_) {
+    pending_gid_[slot] = gid;
+    pending_ops_[slot].clear();
+    pending_slots_.push_back(slot);
+  } else {
+    copy_body(slot, gid);
+  }
   mark_upload(slot);
   if (gid == 0) return SVO_OK;
-  // patch the parent's leaf (TreeletMemoryManager.cpp:518-545)
-  const uint64_t pslot = (uint64_t)slot_of_[t.parent_gid];
-  const uint64_t leaf = pslot * N_ + (uint64_t)t.parent_leaf_position;
-  const uint64_t leaf_parent = pslot * N_ + (uint64_t)t.parent_leaf_parent_position;
-  incore_[leaf] = incore_[pos];
-  incore_[leaf_parent].masks &= ~(1u << (uint32_t)t.parent_leaf_idx);
-  incore_[leaf].first_child = (uint32_t)((int64_t)(pos + 1) - (int64_t)leaf);
-  mark_upload((uint32_t)pslot);
+  // patch the parent's leaf (TreeletMemoryManager.cpp:518-545): the leaf
+  // becomes a copy of the treelet's root pointing into its slot, and its
+  // flag in the leaf's parent is cleared
+  const uint32_t pslot = (uint32_t)slot_of_[t.parent_gid];
+  LeafWrite w;
+  w.leaf = (uint64_t)pslot * N_ + (uint64_t)t.parent_leaf_position;
+  w.leaf_parent = (uint64_t)pslot * N_ + (uint64_t)t.parent_leaf_parent_position;
+  w.value = t.nodes[0];
+  w.value.first_child = (uint32_t)((int64_t)(pos + 1) - (int64_t)w.leaf);
+  w.bit = 1u << (uint32_t)t.parent_leaf_idx;
+  w.set = false;
+  write_leaf(pslot, w);
+  mark_upload(pslot);
   children_[t.parent_gid].insert(gid);
   return SVO_OK;
 }
@@ -97,20 +105,92 @@ int TreeletMemoryManager::remove_treelet(int32_t gid) {
   if (pslot < 0) return SVO_ERR_INVALID;
   before_host_write();
   const uint32_t slot = (uint32_t)slot_of_[gid];
-  const uint64_t leaf = (uint64_t)pslot * N_ + (uint64_t)t.parent_leaf_position;
-  const uint64_t leaf_parent = (uint64_t)pslot * N_ + (uint64_t)t.parent_leaf_parent_position;
+  complete_pending(slot);
   // restore the original leaf and its leaf flag (TreeletMemoryManager.cpp:679-683)
   const TreeletData& pt = scene_.treelets[t.parent_gid];
-  incore_[leaf] = (uint32_t)t.parent_leaf_position < pt.num_nodes
-                      ? pt.nodes[t.parent_leaf_position]
-                      : svo_node{0u, 0u};
-  incore_[leaf_parent].masks |= 1u << (uint32_t)t.parent_leaf_idx;
+  LeafWrite w;
+  w.leaf = (uint64_t)pslot * N_ + (uint64_t)t.parent_leaf_position;
+  w.leaf_parent = (uint64_t)pslot * N_ + (uint64_t)t.parent_leaf_parent_position;
+  w.value = (uint32_t)t.parent_leaf_position < pt.num_nodes ? pt.nodes[t.parent_leaf_position]
+                                                            : svo_node{0u, 0u};
+  w.bit = 1u << (uint32_t)t.parent_leaf_idx;
+  w.set = true;
+  write_leaf((uint32_t)pslot, w);
   mark_upload((uint32_t)pslot);
   slots_[slot] = SlotInfo();
   free_.push_back(slot);
   slot_of_[gid] = -1;
   children_[t.parent_gid].erase(gid);
   return SVO_OK;
+}
+
+void TreeletMemoryManager::copy_body(uint32_t slot, int32_t gid) {
+  const TreeletData& t = scene_.treelets[gid];
+  const uint64_t pos = (uint64_t)slot * N_;
+  std::memcpy(incore_ + pos, t.nodes.data(), (size_t)t.num_nodes * sizeof(svo_node));
+  std::memset(incore_ + pos + t.num_nodes, 0, (size_t)(N_ - t.num_nodes) * sizeof(svo_node));
+  std::memcpy(incore_attr_ + pos, t.attribs.data(), (size_t)t.num_nodes * sizeof(svo_attrib));
+  std::memset(incore_attr_ + pos + t.num_nodes, 0, (size_t)(N_ - t.num_nodes) * sizeof(svo_attrib));
+}
+
+void TreeletMemoryManager::write_leaf(uint32_t pslot, const LeafWrite& w) {
+  if (defer_ && pending_gid_[pslot] >= 0) {
+    pending_ops_[pslot].push_back(w);
+    return;
+  }
+  incore_[w.leaf] = w.value;
+  if (w.set)
+    incore_[w.leaf_parent].masks |= w.bit;
+  else
+    incore_[w.leaf_parent].masks &= ~w.bit;
+}
+
+void TreeletMemoryManager::complete_pending(uint32_t slot) {
+  if (!defer_ || pending_gid_[slot] < 0) return;
+  const int32_t gid = pending_gid_[slot];
+  pending_gid_[slot] = -1;
+  copy_body(slot, gid);
+  for (const LeafWrite& w : pending_ops_[slot]) write_leaf(slot, w);
+  pending_ops_[slot].clear();
+}
+
+void TreeletMemoryManager::begin_deferred() {
+  pending_gid_.assign(slots_.size(), -1);
+  pending_ops_.resize(slots_.size());
+  pending_slots_.clear();
+  defer_ = true;
+}
+
+void TreeletMemoryManager::end_deferred() {
+  std::vector<uint32_t> todo;
+  for (uint32_t s : pending_slots_)
+    if (pending_gid_[s] >= 0) todo.push_back(s);  // a slot placed twice is listed twice
+  std::sort(todo.begin(), todo.end());
+  todo.erase(std::unique(todo.begin(), todo.end()), todo.end());
+  // bodies first, on up to 8 threads for more than 16 slots ...
+  auto bodies = [&](size_t lo, size_t hi) {
+    for (size_t i = lo; i < hi; ++i) copy_body(todo[i], pending_gid_[todo[i]]);
+  };
+  static const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t parts = todo.size() > 16 ? std::min<size_t>(std::min<size_t>(8, hw), todo.size() / 8) : 1;
+  std::vector<std::thread> workers;
+  size_t started = 1;  // part 0 runs on this thread
+  try {
+    for (; started < parts; ++started)
+      workers.emplace_back(bodies, todo.size() * started / parts, todo.size() * (started + 1) / parts);
+  } catch (...) {  // no more threads: the rest runs here
+  }
+  bodies(0, parts ? todo.size() / parts : todo.size());
+  if (started < parts) bodies(todo.size() * started / parts, todo.size());
+  for (std::thread& w : workers) w.join();
+  // ... then, per slot in order, the writes aimed at it
+  defer_ = false;
+  for (uint32_t s : todo) {
+    for (const LeafWrite& w : pending_ops_[s]) write_leaf(s, w);
+    pending_ops_[s].clear();
+    pending_gid_[s] = -1;
+  }
+  pending_slots_.clear();
 }
 
 int TreeletMemoryManager::free_incore_position() {
@@ -152,6 +232,7 @@ int TreeletMemoryManager::free_incore_position() {
   for (int32_t c : to_clear) {
     const int32_t s = slot_of_[c];
     if (s > 0) {
+      complete_pending((uint32_t)s);
       free_.push_back((uint32_t)s);
       slot_of_[c] = -1;
       slots_[s] = SlotInfo();
@@ -172,6 +253,7 @@ int TreeletMemoryManager::update_client_side(const int32_t* new_gids, const floa
     slots_[slot_of_[g]].visibility = kMaxVisibility;
   }
   int rc = SVO_OK;
+  begin_deferred();
   for (uint32_t i = 0; i < num_new; ++i) {
     SlotInfo s;
     s.treelet_gid = new_gids[i];
@@ -192,6 +274,7 @@ int TreeletMemoryManager::update_client_side(const int32_t* new_gids, const floa
     if (skip_unplaceable && (r == SVO_ERR_BUSY || (r == SVO_ERR_INVALID && parent_gone))) continue;
     if (rc == SVO_OK) rc = r;  // keep going, report the first failure
   }
+  end_deferred();
   return rc;
 }
 

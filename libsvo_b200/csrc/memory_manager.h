@@ -143,6 +143,31 @@ class TreeletMemoryManager {
   bool evict_any_invisible_ = false;
   uint32_t max_new_ = 0;
   uint32_t last_requested_ = 0;
+
+  // Deferred slot bodies.  update_client_side places many treelets at once;
+  // copying each one's records into the host mirror as it is placed made the
+  // copies (about 200 KB a treelet) run one after another on one thread.
+  // While deferring, a placed treelet's body is copied at the end of the
+  // update, all bodies in parallel; the leaf patches and restores aimed at a
+  // slot whose body is still pending are kept in order and applied after
+  // it, and a pending slot that is evicted or freed during the update is
+  // completed on the spot first.  The mirror then ends up exactly as with
+  // immediate copies.
+  struct LeafWrite {
+    uint64_t leaf, leaf_parent;
+    svo_node value;
+    uint32_t bit;
+    bool set;  // set the leaf flag (a restore) or clear it (a patch)
+  };
+  void begin_deferred();
+  void end_deferred();
+  void copy_body(uint32_t slot, int32_t gid);
+  void complete_pending(uint32_t slot);
+  void write_leaf(uint32_t pslot, const LeafWrite& w);
+  bool defer_ = false;
+  std::vector<int32_t> pending_gid_;                // per slot: gid whose body is pending, or -1
+  std::vector<std::vector<LeafWrite>> pending_ops_;  // per slot: writes after that body
+  std::vector<uint32_t> pending_slots_;
 };
 
 class TreeletMemoryManagerCuda : public TreeletMemoryManager {

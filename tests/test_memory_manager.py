@@ -219,3 +219,51 @@ def test_insert_all_and_reset(scene):
     assert mm.info.free_slots == n - 1
     small = L.TreeletMemoryManagerCuda(scene, scene.info.treelet_bytes * 5)
     assert small.insertAll() == 4
+
+
+@pytest.mark.parametrize("evict_any", [False, True])
+def test_batched_update_matches_one_insertion_at_a_time(evict_any):
+    """updateClientSideIncoreBuffer copies the bodies of the treelets it
+    places at the end, in parallel; the mirror (free slots included), the
+    slot table and the slots to upload must be those of the same update
+    done as a visibility update followed by one insertion at a time.  The
+    lists place children after their parents in the same update, under
+    eviction pressure, so patches aimed at not-yet-copied slots occur."""
+    scene = L.Scene.menger(level=3, depth=7, seed=5, treelet_levels=2)
+    n = scene.info.num_treelets
+    parent = {c: scene.treelet(c)["parent_gid"] for c in range(1, n)}
+    kids = {}
+    for c, p in parent.items():
+        kids.setdefault(p, []).append(c)
+    a = L.TreeletMemoryManagerCuda(scene, scene.info.treelet_bytes * 48)
+    b = L.TreeletMemoryManagerCuda(scene, scene.info.treelet_bytes * 48)
+    for m in (a, b):
+        m.setEviction(L.EVICT_ANY_UNSEEN if evict_any else L.EVICT_REFERENCE)
+    rng = np.random.default_rng(11)
+    placed_total = 0
+    in_batch_children = 0
+    for frame in range(100):
+        resident = [g for g in range(n) if a.getSlotGid(g) >= 0]
+        new = []
+        for g in rng.choice(resident, size=min(len(resident), 4), replace=False):
+            for c in kids.get(int(g), []):  # children, then some of their children
+                if a.getSlotGid(c) < 0 and c not in new:
+                    new.append(c)
+                    new += [d for d in kids.get(c, [])[:2] if d not in new]
+        new = new[:30]
+        old = [int(g) for g in rng.choice(resident, size=len(resident) // 8, replace=False) if g]
+        errs = rng.random(len(new)).astype(np.float32)
+        a.updateClientSideIncoreBuffer(new, errs, old)
+        b.updateClientSideIncoreBuffer([], None, old)
+        for g, e in zip(new, errs):
+            b.insertTreeletIntoIncoreBuffer(g, b.MAX_VISIBILITY, float(e))
+        assert a.getSlots() == b.getSlots(), f"frame {frame}"
+        na, aa = a.getIncoreBuffer()
+        nb, ab = b.getIncoreBuffer()
+        assert np.array_equal(na, nb) and np.array_equal(aa, ab), f"frame {frame}"
+        assert list(a.getIncoreSlotsToUpload()) == list(b.getIncoreSlotsToUpload())
+        placed_total += sum(1 for g in new if a.getSlotGid(g) >= 0)
+        in_batch_children += sum(1 for g in new if a.getSlotGid(g) >= 0 and parent[g] in new)
+    assert placed_total > 100 and in_batch_children > 10
+    a.close()
+    b.close()
