@@ -617,7 +617,7 @@ typedef struct svo_server_cfg {
   uint32_t max_batch_views;   /* requests per batched launch                 */
   uint32_t mode;              /* SVO_SERVE_*                                 */
   uint32_t tile_w, tile_h;    /* batch tile shape (0 = 8x4)                   */
-  uint32_t block_threads;     /* batch block size (0 = 256)                  */
+  uint32_t block_threads;     /* batch block size (0 = 128)                  */
 } svo_server_cfg;
 
 typedef struct svo_request {

@@ -925,7 +925,7 @@ for _name, (_args, _res) in {
 
 
 def server_cfg(hbm_budget_bytes, max_inflight_rays=64 << 20, streams=4, max_batch_views=256,
-               mode=SERVE_BATCHED, tile=(8, 4), block_threads=256) -> svo_server_cfg:
+               mode=SERVE_BATCHED, tile=(8, 4), block_threads=128) -> svo_server_cfg:
     c = svo_server_cfg()
     c.hbm_budget_bytes, c.max_inflight_rays = int(hbm_budget_bytes), int(max_inflight_rays)
     c.streams, c.max_batch_views, c.mode = streams, max_batch_views, mode

@@ -747,7 +747,7 @@ int svo_server_create(const svo_server_cfg* cfg, svo_server** out) {
   if (!s) return SVO_ERR_NOMEM;
   s->cfg = *cfg;
   if (s->cfg.tile_w == 0) s->cfg.tile_w = 8, s->cfg.tile_h = 4;
-  if (s->cfg.block_threads == 0) s->cfg.block_threads = 256;
+  if (s->cfg.block_threads == 0) s->cfg.block_threads = 128;
   s->t0 = Clock::now();
   int rc = SVO_OK;
   try {
