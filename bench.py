@@ -472,14 +472,20 @@ def served_leg(dev, n=400, rates=(4000, 16000, 64000)):
         for i in ids.values():
             srv.set_upload_policy(i, L.UPLOAD_PINNED)
         rq = [L.request(ids[o], c.frame_params(), t) for o, c, t in tp_reqs]
+        # untimed warm-up (kernel loading, scratch growth), as the other runs' first loads
+        srv.replay(rq[:8], np.zeros(8), timeout_ms=120000)
+        st0 = srv.stats()
         t_run = time.perf_counter()
         arr = S.poisson_arrivals(len(rq), rate, seed=13)
         r = srv.replay(rq, arr, timeout_ms=120000)
         ok = [x for x in r if x.status == L.SVO_OK]
         lat = np.array([x.done_s - x.submit_s for x in ok]) * 1e3
         span = max(x.done_s for x in ok) - min(x.submit_s for x in r)
-        st = srv.stats()
+        st1 = srv.stats()
         srv.close()
+        st = type("Delta", (), {k: getattr(st1, k) - getattr(st0, k) for k in
+                                ("treelets_paged_in", "bytes_uploaded", "paged_unconverged",
+                                 "analysis_passes", "paging_us")})
         print(f"[bench] served treelet-paged {len(octrees)} octree(s) rate {rate}: "
               f"{time.perf_counter() - t_run:.1f} s", file=sys.stderr, flush=True)
         return {"requests": len(rq), "rays": tp_rays, "mrays_s": tp_rays / span / 1e6,
@@ -573,10 +579,11 @@ def streaming_leg(dev, scene, **kw):
 
     return {"coalesced_0.6": streaming_run(dev, scene, L.UPLOAD_COALESCED, **kw),
             "pinned_mirror_gather": streaming_run(dev, scene, L.UPLOAD_PINNED, **kw),
+            "pinned_pipelined": streaming_run(dev, scene, L.UPLOAD_PINNED, pipelined=True, **kw),
             "reference_thesis": "mostly above 50 Hz, GTX 580 (ergebnisse_diskussionen.tex:158)"}
 
 
-def streaming_run(dev, scene, policy, frames=150, incore_mb=256, size=1024):
+def streaming_run(dev, scene, policy, frames=150, incore_mb=256, size=1024, pipelined=False):
     """The loop the reference measured itself (its thesis: "out-of-core cycle
     + ray cast run sequentially, 1024x1024", mostly above 50 Hz on a GTX 580):
     per frame the analysis pass at 1/8 resolution (feedback kernel, records to
@@ -584,7 +591,12 @@ def streaming_run(dev, scene, policy, frames=150, incore_mb=256, size=1024):
     then the 1024x1024 frame.  The incore buffer holds 256 MB (the thesis'
     size; 87 % of the icosphere's treelets), only the root treelet is
     resident at the start, and the camera orbits 3 degrees per frame while
-    moving in from radius 2.5 to 1.2, so treelets keep paging in and out."""
+    moving in from radius 2.5 to 1.2, so treelets keep paging in and out.
+    pipelined: the analysis pass of view k+1 runs on a second stream beside
+    the cast of frame k (svo_mm_analysis_begin/_end), and its upload goes
+    after that cast; the pool states and frames are the sequential loop's.
+    Its frame times are the intervals between frame completions (CUDA
+    events), as the loop never waits for a frame."""
     import torch
 
     import libsvo_b200 as L
@@ -596,9 +608,24 @@ def streaming_run(dev, scene, policy, frames=150, incore_mb=256, size=1024):
     out = torch.empty((size, size), dtype=torch.int32, device=dev)
     s = torch.cuda.current_stream()
     ms, new_total = [], 0
-    for f in range(frames):
-        r = 2.5 - 1.3 * f / max(1, frames - 1)
-        p = S.orbit_pose(r, 3.0 * f, 20.0, size, size, 25.0).frame_params()
+    poses = [S.orbit_pose(2.5 - 1.3 * f / max(1, frames - 1), 3.0 * f, 20.0, size, size, 25.0).frame_params()
+             for f in range(frames)]
+    if pipelined:
+        sa = torch.cuda.Stream()
+        done = [torch.cuda.Event(enable_timing=True) for _ in range(frames)]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for f, p in enumerate(poses):
+            mm.beginAnalysePass(p, divisor=8, stream=sa)  # beside the cast of frame f-1
+            new, _ = mm.endAnalysePass(after_stream=s)  # its upload after that cast
+            mm.render(p, out, stream=s)
+            done[f].record(s)
+            new_total += new
+        s.synchronize()
+        wall = time.perf_counter() - t0
+        ms = [wall / frames * 1e3] + [done[f - 1].elapsed_time(done[f]) for f in range(1, frames)]
+    for f in range(0 if not pipelined else frames, frames):
+        p = poses[f]
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         new, _ = mm.performAnalysePass(p, divisor=8, stream=s)

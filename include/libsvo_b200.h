@@ -509,6 +509,20 @@ int svo_mm_analysis_requested(svo_mm* mm, uint32_t* requested);
 int svo_mm_analysis_step(svo_mm* mm, const svo_frame_params* frame, uint32_t divisor,
                          float jitter_x, float jitter_y, int32_t stack_size, void* stream,
                          uint32_t* num_new, uint32_t* num_old);
+/* svo_mm_analysis_step in two halves (no reference counterpart: the
+ * reference runs the analysis pass, the update and the frame one after the
+ * other).  _begin launches the analysis rays and the GPU fold on `stream`
+ * (after the manager's pending uploads) and returns; _end waits for them,
+ * inserts and evicts on the host and uploads the dirty slots once the work
+ * already queued on `after_stream` is done.  A loop that begins the analysis
+ * of view k+1 before casting frame k on another stream, and ends it after,
+ * overlaps the two and produces the frames of the sequential loop: both read
+ * the same pool.  No insertion, removal or other analysis may come between
+ * _begin and _end (SVO_ERR_BUSY for a second _begin; _end without _begin is
+ * SVO_ERR_INVALID). */
+int svo_mm_analysis_begin(svo_mm* mm, const svo_frame_params* frame, uint32_t divisor,
+                          float jitter_x, float jitter_y, int32_t stack_size, void* stream);
+int svo_mm_analysis_end(svo_mm* mm, void* after_stream, uint32_t* num_new, uint32_t* num_old);
 
 /* ---- batched views: one persistent launch ------------------------------ */
 

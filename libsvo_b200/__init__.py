@@ -1030,6 +1030,8 @@ for _name, (_args, _res) in {
                                         _P(_u32)], ctypes.c_int),
     "svo_mm_analysis_step": ([_vp, _P(svo_frame_params), _u32, _f32, _f32, _i32, _vp, _P(_u32), _P(_u32)],
                              ctypes.c_int),
+    "svo_mm_analysis_begin": ([_vp, _P(svo_frame_params), _u32, _f32, _f32, _i32, _vp], ctypes.c_int),
+    "svo_mm_analysis_end": ([_vp, _vp, _P(_u32), _P(_u32)], ctypes.c_int),
 }.items():
     _fn = getattr(_L, _name)
     _fn.argtypes = _args
@@ -1084,6 +1086,26 @@ def _perform_analyse_pass(self, frame: svo_frame_params, divisor=8, jitter=(0.0,
     return nn.value, no.value
 
 
+def _begin_analyse_pass(self, frame: svo_frame_params, divisor=8, jitter=(0.0, 0.0), stack_size=13,
+                        stream=None):
+    """First half of performAnalysePass: the analysis rays and the GPU fold,
+    launched on `stream`; endAnalysePass finishes the step."""
+    _check(_L.svo_mm_analysis_begin(self._h, ctypes.byref(frame), divisor, float(jitter[0]),
+                                    float(jitter[1]), stack_size, _stream_ptr(stream)),
+           "svo_mm_analysis_begin")
+
+
+def _end_analyse_pass(self, after_stream=None):
+    """Second half: insert and evict, then upload once the work queued on
+    `after_stream` (a frame reading the pool) is done: (new, old) counts."""
+    nn, no = _u32(), _u32()
+    _check(_L.svo_mm_analysis_end(self._h, _stream_ptr(after_stream), ctypes.byref(nn), ctypes.byref(no)),
+           "svo_mm_analysis_end")
+    return nn.value, no.value
+
+
+TreeletMemoryManagerCuda.beginAnalysePass = _begin_analyse_pass
+TreeletMemoryManagerCuda.endAnalysePass = _end_analyse_pass
 TreeletMemoryManagerCuda.analyseFeedback = _analyse_feedback
 TreeletMemoryManagerCuda.analyseFeedbackDevice = _analyse_feedback_device
 TreeletMemoryManagerCuda.performAnalysePass = _perform_analyse_pass

@@ -708,4 +708,19 @@ int svo_mm_analysis_step(svo_mm* mm, const svo_frame_params* frame, uint32_t div
   });
 }
 
+int svo_mm_analysis_begin(svo_mm* mm, const svo_frame_params* frame, uint32_t divisor,
+                          float jitter_x, float jitter_y, int32_t stack_size, void* stream) {
+  if (!mm || !frame || divisor == 0 || !mm->impl.device_ready()) return SVO_ERR_INVALID;
+  if (stack_size < 2 || stack_size > 24) return SVO_ERR_RANGE;
+  return guarded([&] {
+    return mm->impl.analysis_begin(*frame, divisor, jitter_x, jitter_y, stack_size,
+                                   (cudaStream_t)stream);
+  });
+}
+
+int svo_mm_analysis_end(svo_mm* mm, void* after_stream, uint32_t* num_new, uint32_t* num_old) {
+  if (!mm || !mm->impl.device_ready()) return SVO_ERR_INVALID;
+  return guarded([&] { return mm->impl.analysis_end((cudaStream_t)after_stream, num_new, num_old); });
+}
+
 }  // extern "C"

@@ -367,6 +367,8 @@ TreeletMemoryManagerCuda::~TreeletMemoryManagerCuda() {
     cudaFree(d_ids_[i]);
   }
   if (upload_done_) cudaEventDestroy(upload_done_);
+  if (analysis_done_) cudaEventDestroy(analysis_done_);
+  if (after_done_) cudaEventDestroy(after_done_);
   if (copy_stream_) cudaStreamDestroy(copy_stream_);
 }
 
@@ -742,12 +744,7 @@ int TreeletMemoryManagerCuda::init_analysis() {
   return SVO_OK;
 }
 
-int TreeletMemoryManagerCuda::analyse_feedback_device(
-    const svo_feedback* d_fb, uint64_t n, uint32_t max_new,
-    std::vector<std::pair<int32_t, float>>& out_new, std::vector<std::pair<int32_t, float>>& out_old,
-    cudaStream_t stream) {
-  out_new.clear();
-  out_old.clear();
+int TreeletMemoryManagerCuda::launch_fold(const svo_feedback* d_fb, uint64_t n, cudaStream_t stream) {
   if (n > 0 && !d_fb) return SVO_ERR_INVALID;
   int rc = init_analysis();
   if (rc != SVO_OK) return rc;
@@ -756,8 +753,8 @@ int TreeletMemoryManagerCuda::analyse_feedback_device(
   uint32_t* d_new = d_keys_;
   uint32_t* d_old = d_keys_ + (T + 1);
   uint32_t* d_status = d_keys_ + 2 * ((size_t)T + 1);
-  // The page-locked slot table is free: every pass, failed ones included,
-  // waits for its copies before it returns.
+  // The page-locked slot table is free: every fold's copies are waited for
+  // (read_fold, or a failed launch's synchronisation) before the next one.
   for (uint32_t i = 0; i < S; ++i) h_slot_gid_[i] = slots_[i].treelet_gid;
   cudaError_t e = cudaMemcpyAsync(d_slot_gid_, h_slot_gid_, (size_t)S * sizeof(int32_t),
                                   cudaMemcpyHostToDevice, stream);
@@ -768,10 +765,17 @@ int TreeletMemoryManagerCuda::analyse_feedback_device(
       e = cudaMemcpyAsync(h_keys_, d_keys_, words * sizeof(uint32_t), cudaMemcpyDeviceToHost,
                           stream);
   }
-  const cudaError_t waited = cudaStreamSynchronize(stream);
-  if (e != cudaSuccess) return cuda_status(e);
-  if (rc != SVO_OK) return rc;
-  if (waited != cudaSuccess) return cuda_status(waited);
+  if (e != cudaSuccess || rc != SVO_OK) {
+    cudaStreamSynchronize(stream);  // the copies may still read the slot table
+    return e != cudaSuccess ? cuda_status(e) : rc;
+  }
+  return SVO_OK;
+}
+
+int TreeletMemoryManagerCuda::read_fold(uint32_t max_new,
+                                        std::vector<std::pair<int32_t, float>>& out_new,
+                                        std::vector<std::pair<int32_t, float>>& out_old) {
+  const uint32_t T = num_treelets();
   if (h_keys_[2 * ((size_t)T + 1)] & kAnalyseRejected) return SVO_ERR_RANGE;
   const uint32_t* h_new = h_keys_;
   const uint32_t* h_old = h_keys_ + (T + 1);
@@ -786,6 +790,18 @@ int TreeletMemoryManagerCuda::analyse_feedback_device(
   std::stable_sort(out_old.begin(), out_old.end(), by_error);
   if (out_new.size() > max_new) out_new.resize(max_new);
   return SVO_OK;
+}
+
+int TreeletMemoryManagerCuda::analyse_feedback_device(
+    const svo_feedback* d_fb, uint64_t n, uint32_t max_new,
+    std::vector<std::pair<int32_t, float>>& out_new, std::vector<std::pair<int32_t, float>>& out_old,
+    cudaStream_t stream) {
+  out_new.clear();
+  out_old.clear();
+  const int rc = launch_fold(d_fb, n, stream);
+  if (rc != SVO_OK) return rc;
+  SVO_CUDA_TRY(cudaStreamSynchronize(stream));
+  return read_fold(max_new, out_new, out_old);
 }
 
 int TreeletMemoryManagerCuda::feedback_scratch(uint64_t records, svo_feedback** out) {
@@ -803,14 +819,11 @@ int TreeletMemoryManagerCuda::feedback_scratch(uint64_t records, svo_feedback** 
   return SVO_OK;
 }
 
-int TreeletMemoryManagerCuda::analysis_step(const svo_frame_params& frame, uint32_t divisor,
-                                            float jitter_x, float jitter_y, int32_t stack_size,
-                                            cudaStream_t stream, uint32_t* num_new,
-                                            uint32_t* num_old, uint32_t* num_requested) {
-  if (num_new) *num_new = 0;
-  if (num_old) *num_old = 0;
-  if (num_requested) *num_requested = 0;
+int TreeletMemoryManagerCuda::analysis_begin(const svo_frame_params& frame, uint32_t divisor,
+                                             float jitter_x, float jitter_y, int32_t stack_size,
+                                             cudaStream_t stream) {
   last_requested_ = 0;
+  if (analysis_pending_) return SVO_ERR_BUSY;  // the previous half-step was not ended
   if (divisor == 0 || !device_ready()) return SVO_ERR_INVALID;
   if (stack_size < 2 || stack_size > 24) return SVO_ERR_RANGE;
   cudaStream_t s = stream ? stream : render_stream_;
@@ -833,11 +846,27 @@ int TreeletMemoryManagerCuda::analysis_step(const svo_frame_params& frame, uint3
   if (rc != SVO_OK) return rc;
   rc = wait_uploads(s);
   if (rc != SVO_OK) return rc;
+  if (!analysis_done_) SVO_CUDA_TRY(cudaEventCreateWithFlags(&analysis_done_, cudaEventDisableTiming));
   rc = launch_feedback(device_nodes(), incore_nodes(), a, stack_size, d_fb, nullptr, s);
   if (rc != SVO_OK) return rc;
   // the records stay on the GPU; only per-treelet results come back
+  rc = launch_fold(d_fb, n, s);
+  if (rc != SVO_OK) return rc;
+  SVO_CUDA_TRY(cudaEventRecord(analysis_done_, s));
+  analysis_pending_ = true;
+  return SVO_OK;
+}
+
+int TreeletMemoryManagerCuda::analysis_end(cudaStream_t after, uint32_t* num_new, uint32_t* num_old,
+                                           uint32_t* num_requested) {
+  if (num_new) *num_new = 0;
+  if (num_old) *num_old = 0;
+  if (num_requested) *num_requested = 0;
+  if (!analysis_pending_) return SVO_ERR_INVALID;
+  analysis_pending_ = false;
+  SVO_CUDA_TRY(cudaEventSynchronize(analysis_done_));
   std::vector<std::pair<int32_t, float>> nw, old;
-  rc = analyse_feedback_device(d_fb, n, max_new_treelets(), nw, old, s);
+  int rc = read_fold(max_new_treelets(), nw, old);
   if (num_new) *num_new = (uint32_t)nw.size();
   if (num_old) *num_old = (uint32_t)old.size();
   if (num_requested) *num_requested = (uint32_t)nw.size();
@@ -851,8 +880,32 @@ int TreeletMemoryManagerCuda::analysis_step(const svo_frame_params& frame, uint3
   rc = update_client_side(ng.data(), ne.data(), (uint32_t)ng.size(), og.data(), (uint32_t)og.size(),
                           true, &placed);
   if (num_new) *num_new = placed;
+  // the upload overwrites slots that the work already queued on `after` (a
+  // frame cast from the pool) may still read
+  if (!upload_.empty()) {
+    cudaStream_t w = after ? after : render_stream_;
+    if (!after_done_) SVO_CUDA_TRY(cudaEventCreateWithFlags(&after_done_, cudaEventDisableTiming));
+    if (!copy_stream_) {  // created with the staging by init_transfer
+      const int t = init_transfer();
+      if (t != SVO_OK) return t;
+    }
+    SVO_CUDA_TRY(cudaEventRecord(after_done_, w));
+    SVO_CUDA_TRY(cudaStreamWaitEvent(copy_stream_, after_done_, 0));
+  }
   const int up = update_device_memory(nullptr);
   return rc != SVO_OK ? rc : up;
+}
+
+int TreeletMemoryManagerCuda::analysis_step(const svo_frame_params& frame, uint32_t divisor,
+                                            float jitter_x, float jitter_y, int32_t stack_size,
+                                            cudaStream_t stream, uint32_t* num_new,
+                                            uint32_t* num_old, uint32_t* num_requested) {
+  if (num_new) *num_new = 0;
+  if (num_old) *num_old = 0;
+  if (num_requested) *num_requested = 0;
+  const int rc = analysis_begin(frame, divisor, jitter_x, jitter_y, stack_size, stream);
+  if (rc != SVO_OK) return rc;
+  return analysis_end(stream ? stream : render_stream_, num_new, num_old, num_requested);
 }
 
 }  // namespace svo

@@ -236,9 +236,28 @@ class TreeletMemoryManagerCuda : public TreeletMemoryManager {
   int analysis_step(const svo_frame_params& frame, uint32_t divisor, float jitter_x,
                     float jitter_y, int32_t stack_size, cudaStream_t stream, uint32_t* num_new,
                     uint32_t* num_old, uint32_t* num_requested = nullptr);
+  // The same step in two halves, so that the analysis of the next view can
+  // run beside the frame still being cast: begin launches the analysis rays
+  // and the fold on `stream` (after this manager's pending uploads) and
+  // returns; end waits for them, inserts and evicts on the host and uploads
+  // the dirty slots once the work already queued on `after` (the frame
+  // reading the pool) is done.  Nothing may change the slots in between.
+  // analysis_step(..., s, ...) is analysis_begin(..., s) + analysis_end(s, ...).
+  int analysis_begin(const svo_frame_params& frame, uint32_t divisor, float jitter_x,
+                     float jitter_y, int32_t stack_size, cudaStream_t stream);
+  int analysis_end(cudaStream_t after, uint32_t* num_new, uint32_t* num_old,
+                   uint32_t* num_requested = nullptr);
 
  private:
   int init_analysis();
+  // the device fold of analyse_feedback_device, launched on `stream` (keys
+  // copied back asynchronously), and the reading of its keys once done
+  int launch_fold(const svo_feedback* d_fb, uint64_t n, cudaStream_t stream);
+  int read_fold(uint32_t max_new, std::vector<std::pair<int32_t, float>>& out_new,
+                std::vector<std::pair<int32_t, float>>& out_old);
+  bool analysis_pending_ = false;
+  cudaEvent_t analysis_done_ = nullptr;
+  cudaEvent_t after_done_ = nullptr;
   // One host-to-device copy through the pinned ring.
   struct StagedCopy {
     void* dst;

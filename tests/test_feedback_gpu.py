@@ -108,3 +108,64 @@ def test_analysis_steps_under_memory_pressure(cuda):
     # the pool ran full: the later steps placed treelets only by eviction
     assert mm.info.free_slots == 0 and total >= 39
     mm.close()
+
+
+@pytest.mark.parametrize("policy", [L.UPLOAD_COALESCED, L.UPLOAD_PINNED])
+def test_pipelined_analysis_gives_the_sequential_frames(cuda, policy):
+    """The analysis of view k+1 begun beside the cast of frame k (another
+    stream) and ended after it: every frame and the counts of placed treelets
+    equal the sequential loop's (analysis step, then frame), under paging
+    with eviction in a buffer much smaller than the octree."""
+    import torch
+
+    v, t = L.icosphere(4, seed=2)
+    scene = L.Scene.from_mesh(v, t, 8, treelet_levels=3)
+    info = scene.info
+    slots = max(8, info.num_treelets // 3)
+    from libsvo_b200 import scenes as S
+
+    poses = [S.orbit_pose(2.2 - 0.04 * f, 9.0 * f, 15.0, 192, 128, 30.0).frame_params(t_scale_ratio=0.0)
+             for f in range(24)]
+
+    def loop(pipelined):
+        mm = L.TreeletMemoryManagerCuda(scene, info.treelet_bytes * slots)
+        mm.setUploadPolicy(policy)
+        mm.setEviction(L.EVICT_ANY_UNSEEN)
+        mm.initDeviceBuffer()
+        s, sa = torch.cuda.Stream(), torch.cuda.Stream()
+        outs = [torch.empty((p.height, p.width), dtype=torch.int32, device=cuda) for p in poses]
+        placed = []
+        for p, o in zip(poses, outs):
+            if pipelined:
+                mm.beginAnalysePass(p, divisor=4, stream=sa)
+                placed.append(mm.endAnalysePass(after_stream=s))
+            else:
+                placed.append(mm.performAnalysePass(p, divisor=4, stream=s))
+            mm.render(p, o, stream=s)
+        s.synchronize()
+        frames = [o.cpu().numpy() for o in outs]
+        mm.close()
+        return frames, placed
+
+    seq, seq_placed = loop(False)
+    pipe, pipe_placed = loop(True)
+    assert seq_placed == pipe_placed
+    assert sum(n for n, _ in seq_placed) > slots  # treelets were evicted and paged in again
+    for k, (a, b) in enumerate(zip(seq, pipe)):
+        assert np.array_equal(a, b), f"frame {k}"
+
+
+def test_analysis_halves_misuse(cuda):
+    scene = L.Scene.menger(level=3, depth=6, seed=9, treelet_levels=2)
+    mm = L.TreeletMemoryManagerCuda(scene, scene.info.treelet_bytes * 8)
+    mm.initDeviceBuffer()
+    p = L.orbit_camera(1, 64, 64, radius=1.6).frame_params()
+    with pytest.raises(L.SvoError) as e:
+        mm.endAnalysePass()
+    assert e.value.code == L.SVO_ERR_INVALID
+    mm.beginAnalysePass(p, divisor=4)
+    with pytest.raises(L.SvoError) as e:
+        mm.beginAnalysePass(p, divisor=4)
+    assert e.value.code == L.SVO_ERR_BUSY
+    mm.endAnalysePass()
+    mm.close()
