@@ -148,6 +148,23 @@ class TreeletMemoryManagerCuda {
     return placed;
   }
 
+  // performAnalysePass in two halves (no reference counterpart): begin
+  // launches the analysis on `stream`; end places and evicts, then uploads
+  // after the work queued on `afterStream`.  Begun for view k+1 before frame
+  // k is cast on another stream and ended after, the step runs beside that
+  // frame and the frames are those of the sequential loop.
+  void beginAnalysePass(const svo_frame_params& frame, uint32_t divisor = 8, float jitterX = 0.0f,
+                        float jitterY = 0.0f, int32_t stackSize = 13, void* stream = nullptr) {
+    check(svo_mm_analysis_begin(mm_, &frame, divisor, jitterX, jitterY, stackSize, stream),
+          "svo_mm_analysis_begin");
+  }
+  uint32_t endAnalysePass(void* afterStream = nullptr, uint32_t* numVisibleResident = nullptr) {
+    uint32_t placed = 0, old = 0;
+    check(svo_mm_analysis_end(mm_, afterStream, &placed, &old), "svo_mm_analysis_end");
+    if (numVisibleResident) *numVisibleResident = old;
+    return placed;
+  }
+
   // insertTreeletIntoIncoreBuffer (src/TreeletMemoryManager.cpp:456-548).
   bool insertTreeletIntoIncoreBuffer(const SlotInfo& tve) {
     return svo_mm_insert_treelet(mm_, tve._treeletGid, tve._visibility, tve._error) == SVO_OK;
