@@ -883,7 +883,8 @@ def summarize_legs(legs: dict) -> dict:
             cp = v["converged_parity"]
             out[key] = {"cap_gb": v["residency_cap_gb"], "hz": _r(v["hz_mean"]), "p50_ms": _r(v["ms_p50"]),
                         "p99_ms": _r(v["ms_p99"]), "gb_paged": _r(v["gb_paged_in"]),
-                        "parity_mismatched": cp["mismatched"], "converged": cp["converged"]}
+                        "parity_mismatched": cp["mismatched"], "converged": cp["converged"],
+                        "hz_pipelined": _r(v.get("pipelined", {}).get("hz_mean"))}
         elif key == "incore_update":
             out[key] = {k: _r(r["ms_mean"]) for k, r in v.items() if isinstance(r, dict) and "ms_mean" in r}
         elif key == "streaming":
@@ -987,6 +988,31 @@ def large_streaming_leg(dev, cap_gb=24.0, frames=60, subdivisions=9, depth=14, u
                                "mismatched_rays": int(bad.sum())}
     res["converged_parity"]["mismatched"] = (res["converged_parity"]["mismatched_rgba"]
                                              + res["converged_parity"]["mismatched_rays"])
+    # the same frames with the next view's analysis run beside the current
+    # frame (svo_mm_analysis_begin/_end: same pool states, same frames), on a
+    # fresh manager; frame times from CUDA events at the frames' ends
+    mm = L.TreeletMemoryManagerCuda(wl.scene, incore, stream=s)
+    if upload == "pinned":
+        mm.setUploadPolicy(L.UPLOAD_PINNED)
+    mm.setEviction(L.EVICT_ANY_UNSEEN)
+    mm.initDeviceBuffer()
+    rng = np.random.default_rng(7)
+    sa = torch.cuda.Stream()
+    done = [torch.cuda.Event(enable_timing=True) for _ in range(frames)]
+    torch.cuda.synchronize()
+    for f in range(frames):
+        r = 2.5 - 1.3 * f / max(1, frames - 1)
+        p = S.orbit_pose(r, 40.0 + 3.0 * f, 15.0, cam.width, cam.height, 25.0).frame_params()
+        mm.beginAnalysePass(p, divisor=8, jitter=tuple(rng.uniform(-1, 1, 2)), stack_size=wl.stack_size,
+                            stream=sa)
+        mm.endAnalysePass(after_stream=s)
+        mm.render_shadow(p, out, sc, cfg=cfg, stream=s)
+        done[f].record(s)
+    s.synchronize()
+    iv = [done[f - 1].elapsed_time(done[f]) for f in range(6, frames)]
+    mm.close()
+    res["pipelined"] = {"hz_mean": 1e3 / statistics.mean(iv), "ms_p50": statistics.median(iv),
+                        "ms_p99": float(np.percentile(iv, 99))}
     del hb, out
     wl.scene.close()
     return res
