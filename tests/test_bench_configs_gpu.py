@@ -1,4 +1,5 @@
-"""Bit-exact parity at the configurations bench.py measures, at full size.
+"""Bit-exact parity at the configurations bench.py measures, at full size
+(the flat traversal of the headline view included).
 
 * the headline frame: icosphere subdivided 6 times, depth-11 octree in
   6-level treelets, 1920x1080 (2,073,600 rays), every hit record field and
@@ -177,3 +178,30 @@ def test_large_shadowed_frame_band(cuda):
         assert np.array_equal(got_rgba, oracle.to_rgba8(ref_rgbaf))
         for k in ("node", "depth", "hit", "loops"):
             assert np.array_equal(got_s[k], ref_shadow[k]), f"shadow rays vs reference sample(): {k}"
+
+
+def test_flat_traversal_full_size(cuda):
+    """The CpuRaycasterSingleRay3 traversal (flat breadth-first pool, absolute
+    first-child indices, stack = the octree's depth) on the headline frame at
+    full size: the depth-11 icosphere flattened (17.3 M nodes), 1920x1080,
+    cast longest first, every hit record and pixel against the oracle's
+    traversSvo restatement (parity unpinned: the reference's CPU raycaster
+    does not build)."""
+    import torch
+
+    from libsvo_b200 import scenes
+
+    wl = scenes.icosphere()
+    depth = int(wl.scene.info.max_depth)
+    nodes, attribs = wl.scene.flatten()
+    dn = torch.from_numpy(nodes.view(np.int32)).to(cuda)
+    da = torch.from_numpy(attribs.view(np.int32)).to(cuda)
+    p = wl.cameras[0].frame_params()
+    rgba = torch.empty((p.height, p.width), dtype=torch.int32, device=cuda)
+    hits = torch.empty(p.width * p.height * 16, dtype=torch.uint8, device=cuda)
+    L.render(dn, da, nodes.shape[0], p, rgba, hits, cfg=L.trace_cfg(L.TRAVERSAL_FLAT, depth))
+    torch.cuda.synchronize()
+    o_rgba, o_hits, _, _ = oracle.render(nodes, attribs, bytes(p), flat=True, stack_size=depth)
+    assert_hits_equal(_hits(hits), o_hits, "flat icosphere 1080p")
+    assert np.array_equal(rgba.cpu().numpy().view(np.uint32), o_rgba)
+    assert _hits(hits)["hit"].sum() > 400_000
