@@ -168,6 +168,9 @@ def test_treelet_paged_octree_same_alone_and_in_the_mix(workload, cuda, mode):
     assert all(r.status == L.SVO_OK for r in res)
     st = srv.stats()
     assert st.requests_done == len(rq) and st.treelets_paged_in > 0 and st.paged_unconverged == 0
+    # every paged request ran at least one analysis pass (one that asks for
+    # nothing more ends it), and the passes were timed
+    assert st.analysis_passes >= sum(o == big for o, _ in reqs) and st.paging_us > 0
     torch.cuda.synchronize()
     for (o, cam), t in zip(reqs, outs):
         assert np.array_equal(t.cpu().numpy(), alone(workload.scenes[o], cam, cuda)), f"octree {o}"
