@@ -517,9 +517,9 @@ int svo_mm_analysis_step(svo_mm* mm, const svo_frame_params* frame, uint32_t div
  * already queued on `after_stream` is done.  A loop that begins the analysis
  * of view k+1 before casting frame k on another stream, and ends it after,
  * overlaps the two and produces the frames of the sequential loop: both read
- * the same pool.  No insertion, removal or other analysis may come between
- * _begin and _end (SVO_ERR_BUSY for a second _begin; _end without _begin is
- * SVO_ERR_INVALID). */
+ * the same pool.  No insertion, removal, update or other analysis may come
+ * between _begin and _end: those calls return SVO_ERR_BUSY meanwhile, as
+ * does a second _begin; _end without _begin is SVO_ERR_INVALID. */
 int svo_mm_analysis_begin(svo_mm* mm, const svo_frame_params* frame, uint32_t divisor,
                           float jitter_x, float jitter_y, int32_t stack_size, void* stream);
 int svo_mm_analysis_end(svo_mm* mm, void* after_stream, uint32_t* num_new, uint32_t* num_old);

@@ -404,6 +404,7 @@ int svo_mm_get_device_buffers(svo_mm* mm, const svo_node** d_nodes, const svo_at
 
 int svo_mm_insert_treelet(svo_mm* mm, int32_t treelet_gid, int32_t visibility, float error) {
   if (!mm) return SVO_ERR_INVALID;
+  if (mm->impl.analysis_pending()) return SVO_ERR_BUSY;  // between _begin and _end
   return guarded([&] {
     svo::TreeletMemoryManager::SlotInfo s;
     s.treelet_gid = treelet_gid;
@@ -415,17 +416,20 @@ int svo_mm_insert_treelet(svo_mm* mm, int32_t treelet_gid, int32_t visibility, f
 
 int svo_mm_remove_treelet(svo_mm* mm, int32_t treelet_gid) {
   if (!mm) return SVO_ERR_INVALID;
+  if (mm->impl.analysis_pending()) return SVO_ERR_BUSY;  // between _begin and _end
   return guarded([&] { return mm->impl.remove_treelet(treelet_gid); });
 }
 
 int svo_mm_free_incore_position(svo_mm* mm) {
   if (!mm) return SVO_ERR_INVALID;
+  if (mm->impl.analysis_pending()) return SVO_ERR_BUSY;  // between _begin and _end
   return guarded([&] { return mm->impl.free_incore_position(); });
 }
 
 int svo_mm_update_client_side(svo_mm* mm, const int32_t* new_gids, const float* new_errors,
                               uint32_t num_new, const int32_t* old_gids, uint32_t num_old) {
   if (!mm || (num_new && !new_gids) || (num_old && !old_gids)) return SVO_ERR_INVALID;
+  if (mm->impl.analysis_pending()) return SVO_ERR_BUSY;  // between _begin and _end
   return guarded([&] {
     return mm->impl.update_client_side(new_gids, new_errors, num_new, old_gids, num_old);
   });
@@ -443,6 +447,7 @@ int svo_mm_set_upload_ratio(svo_mm* mm, float ratio) {
 
 int svo_mm_update_device_memory(svo_mm* mm, uint32_t* num_copy_calls) {
   if (!mm) return SVO_ERR_INVALID;
+  if (mm->impl.analysis_pending()) return SVO_ERR_BUSY;  // between _begin and _end
   return guarded([&] { return mm->impl.update_device_memory(num_copy_calls); });
 }
 
@@ -464,11 +469,13 @@ int svo_mm_plan_uploads(svo_mm* mm, uint32_t* h_first_slots, uint32_t* h_slot_co
 
 int svo_mm_reset(svo_mm* mm) {
   if (!mm) return SVO_ERR_INVALID;
+  if (mm->impl.analysis_pending()) return SVO_ERR_BUSY;  // between _begin and _end
   return guarded([&] { return mm->impl.reset_incore_buffer(); });
 }
 
 int svo_mm_insert_all(svo_mm* mm, uint32_t* num_inserted) {
   if (!mm) return SVO_ERR_INVALID;
+  if (mm->impl.analysis_pending()) return SVO_ERR_BUSY;  // between _begin and _end
   return guarded([&] { return mm->impl.insert_all(num_inserted); });
 }
 

@@ -254,25 +254,30 @@ int TreeletMemoryManager::update_client_side(const int32_t* new_gids, const floa
   }
   int rc = SVO_OK;
   begin_deferred();
-  for (uint32_t i = 0; i < num_new; ++i) {
-    SlotInfo s;
-    s.treelet_gid = new_gids[i];
-    s.visibility = kMaxVisibility;
-    s.error = new_errors ? new_errors[i] : 0.0f;
-    // A treelet is unplaceable when no slot can be freed, or when its parent
-    // is not resident (an earlier insertion of the same update evicted it);
-    // the reference ignores these failures (TreeletMemoryManager.cpp:428-431)
-    // and the next analysis pass asks for the treelet again.
-    const bool parent_gone = s.treelet_gid > 0 && (uint32_t)s.treelet_gid < scene_.treelets.size() &&
-                             slot_of_[s.treelet_gid] < 0 &&
-                             slot_of_[scene_.treelets[s.treelet_gid].parent_gid] < 0;
-    const int r = insert_treelet(s);
-    if (r == SVO_OK) {
-      if (inserted) ++*inserted;
-      continue;
+  try {
+    for (uint32_t i = 0; i < num_new; ++i) {
+      SlotInfo s;
+      s.treelet_gid = new_gids[i];
+      s.visibility = kMaxVisibility;
+      s.error = new_errors ? new_errors[i] : 0.0f;
+      // A treelet is unplaceable when no slot can be freed, or when its parent
+      // is not resident (an earlier insertion of the same update evicted it);
+      // the reference ignores these failures (TreeletMemoryManager.cpp:428-431)
+      // and the next analysis pass asks for the treelet again.
+      const bool parent_gone = s.treelet_gid > 0 && (uint32_t)s.treelet_gid < scene_.treelets.size() &&
+                               slot_of_[s.treelet_gid] < 0 &&
+                               slot_of_[scene_.treelets[s.treelet_gid].parent_gid] < 0;
+      const int r = insert_treelet(s);
+      if (r == SVO_OK) {
+        if (inserted) ++*inserted;
+        continue;
+      }
+      if (skip_unplaceable && (r == SVO_ERR_BUSY || (r == SVO_ERR_INVALID && parent_gone))) continue;
+      if (rc == SVO_OK) rc = r;  // keep going, report the first failure
     }
-    if (skip_unplaceable && (r == SVO_ERR_BUSY || (r == SVO_ERR_INVALID && parent_gone))) continue;
-    if (rc == SVO_OK) rc = r;  // keep going, report the first failure
+  } catch (...) {  // (an allocation failed) the slots placed so far get their bodies
+    end_deferred();
+    throw;
   }
   end_deferred();
   return rc;

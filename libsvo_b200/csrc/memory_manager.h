@@ -247,6 +247,8 @@ class TreeletMemoryManagerCuda : public TreeletMemoryManager {
                      float jitter_y, int32_t stack_size, cudaStream_t stream);
   int analysis_end(cudaStream_t after, uint32_t* num_new, uint32_t* num_old,
                    uint32_t* num_requested = nullptr);
+  // A begun analysis step not yet ended (the slots must not change).
+  bool analysis_pending() const { return analysis_pending_; }
 
  private:
   int init_analysis();

@@ -167,5 +167,10 @@ def test_analysis_halves_misuse(cuda):
     with pytest.raises(L.SvoError) as e:
         mm.beginAnalysePass(p, divisor=4)
     assert e.value.code == L.SVO_ERR_BUSY
+    # the slots may not change while the analysis is pending
+    top = [g for g in range(1, scene.info.num_treelets) if scene.treelet(g)["parent_gid"] == 0]
+    assert not mm.insertTreeletIntoIncoreBuffer(top[0])
+    assert mm.updateClientSideIncoreBuffer([top[0]]) == L.SVO_ERR_BUSY
     mm.endAnalysePass()
+    assert mm.updateClientSideIncoreBuffer([], None, [0]) == L.SVO_OK  # accepted again
     mm.close()
