@@ -93,6 +93,21 @@ def test_ragged_frame_sizes(menger_mm, w, h):
     assert np.array_equal(rgba, o_rgba)
 
 
+@pytest.mark.parametrize("w,h", [(1301, 811), (4099, 257), (1024, 1024)])
+def test_ragged_frames_cast_longest_first(menger_mm, w, h):
+    """Frames of a million pixels or more are cast longest first (a per-block
+    cost estimate, then the blocks in bucket order); ragged widths and
+    heights leave partial blocks on the right and bottom edges.  Every pixel
+    must still match the oracle."""
+    p = L.orbit_camera(7, w, h, radius=1.8).frame_params()
+    assert w * h >= 1 << 20
+    rgba, hits = gpu_frame(menger_mm, p)
+    nodes, attribs = menger_mm.getIncoreBuffer()
+    o_rgba, o_hits, _, _ = oracle.render(nodes, attribs, bytes(p))
+    assert_hits_equal(hits, o_hits, f"{w}x{h}")
+    assert np.array_equal(rgba, o_rgba.reshape(rgba.shape))
+
+
 def test_frame_taller_than_one_grid(menger_mm, cuda):
     """600,001 rows: more than one launch's 65,535 block rows of 8 pixels;
     the per-frame, shadow and feedback kernels each cover it in several
