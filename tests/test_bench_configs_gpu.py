@@ -205,3 +205,36 @@ def test_flat_traversal_full_size(cuda):
     assert_hits_equal(_hits(hits), o_hits, "flat icosphere 1080p")
     assert np.array_equal(rgba.cpu().numpy().view(np.uint32), o_rgba)
     assert _hits(hits)["hit"].sum() > 400_000
+
+
+def test_analysis_records_full_size(cuda):
+    """The analysis (feedback) kernel at full resolution on the headline frame
+    — the pass that treelet-paged serving runs per request — over a partly
+    resident pool (a third of the treelets, placed by two analysis steps):
+    every 16-byte record against the oracle's renderToFeedbackBuffer, and
+    against the reference's own sampleAnalyse where it was built."""
+    import torch
+
+    from libsvo_b200 import scenes
+
+    wl = scenes.icosphere()
+    info = wl.scene.info
+    p = wl.cameras[0].frame_params()
+    mm = L.TreeletMemoryManagerCuda(wl.scene, info.treelet_bytes * (info.num_treelets // 3))
+    mm.setEviction(L.EVICT_ANY_UNSEEN)
+    mm.initDeviceBuffer()
+    for _ in range(2):
+        mm.performAnalysePass(p, divisor=8)
+    torch.cuda.synchronize()
+    d_nodes, _, n = mm.getDeviceIncoreBuffer()
+    nodes, _ = mm.getIncoreBuffer()
+    fb = torch.empty(p.width * p.height * 16, dtype=torch.uint8, device=cuda)
+    L.feedback_render(d_nodes, n, p, fb)
+    torch.cuda.synchronize()
+    got = fb.cpu().numpy().view(oracle.FEEDBACK_DTYPE).reshape(p.height, p.width)
+    rec, _ = oracle.feedback(nodes, bytes(p))
+    assert np.array_equal(got.view(np.uint8), rec.view(np.uint8))
+    ref = oracle.reference_feedback(nodes, bytes(p))
+    if ref is not None:
+        assert np.array_equal(got.view(np.uint8), ref[0].view(np.uint8))
+    mm.close()
