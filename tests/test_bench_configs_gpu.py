@@ -8,7 +8,8 @@
   treeletRenderer_rgba.cl compiled for the host (oracle/_ref);
 * the batched terrain views: the 64 views of uneven size cast in one
   autotuned batched launch; four of them (the smallest, two middle ones and
-  the largest) carry hit records and are compared in full;
+  the largest) carry hit records and are compared in full with the oracle,
+  and all 64 images with the per-frame kernel's;
 * the large primary + shadow frame: the icosphere subdivided 9 times (5.2 M
   triangles) built on the GPU, 3840x2160 primary rays and one shadow ray per
   hit, compared over a band of 96 rows, and the primary frame alone over
@@ -128,6 +129,12 @@ def test_batched_terrain_views_full_size(cuda):
         if ref is not None:
             assert np.array_equal(got_rgba, oracle.to_rgba8(ref)), f"view {i} vs reference"
     assert sum(ps[i].width * ps[i].height for i in checked) > 4_000_000
+    # all 64 views: the batched images equal the per-frame kernel's, bit for bit
+    d_nodes, d_attribs, n = mm.getDeviceIncoreBuffer()
+    for i, p in enumerate(ps):
+        want = torch.empty((p.height, p.width), dtype=torch.int32, device=cuda)
+        L.render(d_nodes, d_attribs, n, p, want)
+        assert torch.equal(outs[i], want), f"view {i} ({p.width}x{p.height}) batched vs per-frame"
     mm.close()
 
 
