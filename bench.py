@@ -443,13 +443,15 @@ def served_leg(dev, n=400, rates=(4000, 16000, 64000)):
         return res
 
     all_rates = list(rates) + [0]
-    batched = run(L.SERVE_BATCHED, 2 * footprint, all_rates)
+    # batched and ungated plain on the same 8 streams; the one-stream plain
+    # loop keeps 4 slots, the reference's pattern of a blocking enqueue
+    batched = run(L.SERVE_BATCHED, 2 * footprint, all_rates, streams=8)
     plain = run(L.SERVE_PLAIN, 2 * footprint, all_rates)
     # the ungated plain baseline: every admitted request's per-frame kernel
     # launched at once, round robin over 8 streams, completion by events
     ungated = run(L.SERVE_PLAIN_STREAMED, 2 * footprint, all_rates, streams=8)
-    paging = run(L.SERVE_BATCHED, footprint // 2, [16000])
-    paging_pinned = run(L.SERVE_BATCHED, footprint // 2, [16000], upload=L.UPLOAD_PINNED)
+    paging = run(L.SERVE_BATCHED, footprint // 2, [16000], streams=8)
+    paging_pinned = run(L.SERVE_BATCHED, footprint // 2, [16000], upload=L.UPLOAD_PINNED, streams=8)
     paging_ungated = run(L.SERVE_PLAIN_STREAMED, footprint // 2, [16000], streams=8)
     paging_ungated_pinned = run(L.SERVE_PLAIN_STREAMED, footprint // 2, [16000], upload=L.UPLOAD_PINNED,
                                 streams=8)
