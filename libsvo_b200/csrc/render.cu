@@ -260,7 +260,7 @@ constexpr uint32_t kRowsPerLaunch = 65535u * kBlockH;
 
 namespace {
 
-// The scratch of longest-first dispatch (8 bytes per block) comes from a
+// The scratch of longest-first dispatch (196 bytes per block) comes from a
 // memory pool of the library's own, one per device, in stream order: calls
 // on different streams get different scratch, and the pool keeps up to 64 MB
 // between calls instead of returning it at every synchronisation.
@@ -384,9 +384,15 @@ int launch_render_shadow(const svo_node* nodes, const svo_attrib* attribs, uint6
   if (p.height > 0xFFFFFFF0u) return SVO_ERR_RANGE;  // row indices stay below 2^32
   const uint2* n2 = reinterpret_cast<const uint2*>(nodes);
   const uint2* a2 = reinterpret_cast<const uint2*>(attribs);
-  // Raster order: ordering by primary-ray cost made the 3840x2160 shadow
-  // frame slower (2.02 against 1.79 ms), the shadow rays' cost being unknown
-  // to the estimate and neighbouring blocks no longer sharing the caches.
+  // One pass in raster order: ordering by primary-ray cost made the
+  // 3840x2160 shadow frame slower (2.02 against 1.79 ms), the shadow rays'
+  // cost being unknown to the estimate and neighbouring blocks no longer
+  // sharing the caches.  Two passes (the primary rays longest first, each
+  // hit appended to a job list, then one shadow ray per job in full warps)
+  // were slower still: 2.22 against 1.79 ms, and 0.626 against 0.529 ms at
+  // 1920x1080, where the shadow pass alone took 330 us for 504 k rays.  A
+  // shadow ray cast right after its primary ray finds the nodes of its
+  // descent in L1; cast in a later pass it reads them from L2 again.
   const uint32_t gx = (p.width + kBlockW - 1) / kBlockW;
   for (uint32_t y0 = 0; y0 < p.height; y0 += kRowsPerLaunch) {
     const uint32_t rows = p.height - y0 < kRowsPerLaunch ? p.height - y0 : kRowsPerLaunch;

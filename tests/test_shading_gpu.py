@@ -131,6 +131,17 @@ def test_shadow_frame_menger(menger_mm):
     check_shadow(menger_mm, L.orbit_camera(4, 128, 128).frame_params(), L.seeded_light(4), 0.05, 0.03)
 
 
+@pytest.mark.parametrize("w,h", [(1301, 811), (4099, 257)])
+def test_large_ragged_shadow_frames(menger_mm, w, h):
+    """Shadow frames of a million pixels or more (many waves of blocks) with
+    ragged sizes that leave partial blocks on the right and bottom edges:
+    every pixel, primary and shadow record must match the oracle."""
+    assert w * h >= 1 << 20
+    p = L.orbit_camera(5, w, h, radius=1.6).frame_params()
+    hits, shits = check_shadow(menger_mm, p, L.seeded_light(5))
+    assert 0 < int(shits["hit"].sum()) < int(hits["hit"].sum())
+
+
 @pytest.mark.parametrize("seed", range(3))
 def test_shadow_random_octrees(cuda, seed):
     torch = _torch()
