@@ -1144,14 +1144,12 @@ def main():
     def e2e_step(i):
         with torch.cuda.stream(stream):
             flush.fill_(i)  # the same L2 flush as the device-timed steps, inside the timed region
-        for p, o, ha, hb in zip(params, outs, host_out, host_out2):
+        for p, ha, hb in zip(params, host_out, host_out2):
             ho = ha if i % 2 == 0 else hb
-            if shadow:  # render, then the image to pinned host memory, waited for
-                mm.render_shadow(p, o, shadow, cfg=cfg, stream=stream)
-                with torch.cuda.stream(stream):
-                    ho.copy_(o, non_blocking=True)
-                stream.synchronize()
-            else:  # cast, copy back on a second stream overlapping the next cast
+            # cast, copy back on a second stream overlapping the next cast
+            if shadow:
+                mm.render_shadow_host_async(p, ho, shadow, cfg=cfg, stream=stream)
+            else:
                 mm.render_host_async(p, ho, cfg=cfg, stream=stream)
 
     for i in range(max(1, args.warmup)):
@@ -1192,9 +1190,9 @@ def main():
             "clocks": clk,
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 4 * primary_rays,
-                    "note": ("svo_mm_render_shadow + RGBA8 image copy to pinned host memory, waited for"
-                             if shadow else "svo_mm_render_host_async: cast + RGBA8 image copied to pinned "
-                             "host memory on a second stream (overlapping the next cast), all waited for")
+                    "note": ("svo_mm_render_shadow_host_async" if shadow else "svo_mm_render_host_async")
+                            + ": cast + RGBA8 image copied to pinned host memory on a second stream "
+                            "(overlapping the next cast), all waited for"
                             + "; host wall clock over the steps, the 256 MB L2 flush of every step included; "
                             "frame parameters travel as kernel arguments"},
             "gpu_launches": args.steps * sum(_kernels_per_render(p, shadow) for p in params),

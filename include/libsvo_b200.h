@@ -432,7 +432,14 @@ int svo_mm_render_shadow(svo_mm* mm, const svo_frame_params* params, const svo_t
  * returns; it must stay valid until then. */
 int svo_mm_render_host_async(svo_mm* mm, const svo_frame_params* params, const svo_trace_cfg* cfg,
                              uint32_t* h_rgba, void* stream);
-/* Waits for `stream` and for every svo_mm_render_host_async copy, and
+/* svo_mm_render_host_async for the primary + shadow ray frame
+ * (svo_mm_render_shadow's image, pipelined the same way; the two calls
+ * share the manager's two device images). */
+int svo_mm_render_shadow_host_async(svo_mm* mm, const svo_frame_params* params,
+                                    const svo_trace_cfg* cfg, const svo_shadow_cfg* shadow,
+                                    uint32_t* h_rgba, void* stream);
+/* Waits for `stream` and for every svo_mm_render_host_async and
+ * svo_mm_render_shadow_host_async copy, and
  * returns the manager's accumulated counters
  * (capped rays = the watchdog status word), then clears them. */
 int svo_mm_sync(svo_mm* mm, void* stream, svo_stats* out);

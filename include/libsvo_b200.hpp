@@ -233,6 +233,18 @@ class TreeletMemoryManagerCuda {
     cfg.stack_size = stackSize;
     return svo_mm_render_host(mm_, &params, &cfg, h_rgba, stream) == SVO_OK;
   }
+  // Frame loops: the image of each call lands in h_rgba (page-locked) by the
+  // next sync(); its copy overlaps the next call's cast.  With `shadow`, the
+  // primary + shadow ray frame.
+  bool renderToHostBufferAsync(const svo_frame_params& params, uint32_t* h_rgba,
+                               const svo_shadow_cfg* shadow = nullptr, void* stream = nullptr,
+                               int32_t stackSize = 13) {
+    svo_trace_cfg cfg;
+    cfg.traversal = SVO_TRAVERSAL_TREELET;
+    cfg.stack_size = stackSize;
+    return (shadow ? svo_mm_render_shadow_host_async(mm_, &params, &cfg, shadow, h_rgba, stream)
+                   : svo_mm_render_host_async(mm_, &params, &cfg, h_rgba, stream)) == SVO_OK;
+  }
   // Waits for `stream` and returns the watchdog and bounds counters of the
   // renders since the last call.
   svo_stats sync(void* stream = nullptr) {

@@ -177,6 +177,8 @@ _SIGS = {
     "svo_mm_render_host": ([_vp, _P(svo_frame_params), _P(svo_trace_cfg), _vp, _vp], ctypes.c_int),
     "svo_mm_sync": ([_vp, _vp, _P(svo_stats)], ctypes.c_int),
     "svo_mm_render_host_async": ([_vp, _P(svo_frame_params), _P(svo_trace_cfg), _vp, _vp], ctypes.c_int),
+    "svo_mm_render_shadow_host_async": ([_vp, _P(svo_frame_params), _P(svo_trace_cfg), _P(svo_shadow_cfg), _vp,
+                                         _vp], ctypes.c_int),
     "svo_mm_set_upload_policy": ([_vp, _i32], ctypes.c_int),
     "svo_mm_set_upload_ratio": ([_vp, _f32], ctypes.c_int),
     "svo_render_shadow": ([_vp, _vp, _u64, _P(svo_frame_params), _P(svo_trace_cfg), _P(svo_shadow_cfg), _vp, _vp,
@@ -704,6 +706,16 @@ class TreeletMemoryManagerCuda:
         ptr = out.data_ptr() if hasattr(out, "data_ptr") else _np_ptr(out)
         _check(_L.svo_mm_render_host_async(self._h, ctypes.byref(params), ctypes.byref(cfg), ptr,
                                            _stream_ptr(stream)), "svo_mm_render_host_async")
+
+    def render_shadow_host_async(self, params: svo_frame_params, out, shadow: svo_shadow_cfg | None = None,
+                                 cfg: svo_trace_cfg | None = None, stream=None):
+        """render_host_async for the primary + shadow ray frame."""
+        cfg = cfg or trace_cfg()
+        shadow = shadow or shadow_cfg()
+        ptr = out.data_ptr() if hasattr(out, "data_ptr") else _np_ptr(out)
+        _check(_L.svo_mm_render_shadow_host_async(self._h, ctypes.byref(params), ctypes.byref(cfg),
+                                                  ctypes.byref(shadow), ptr, _stream_ptr(stream)),
+               "svo_mm_render_shadow_host_async")
 
     def sync(self, stream=None) -> svo_stats:
         s = svo_stats()

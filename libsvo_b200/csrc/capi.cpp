@@ -627,6 +627,18 @@ int svo_mm_render_host_async(svo_mm* mm, const svo_frame_params* params, const s
   return guarded([&] { return mm->impl.render_to_host_async(*params, *cfg, h_rgba, s); });
 }
 
+int svo_mm_render_shadow_host_async(svo_mm* mm, const svo_frame_params* params,
+                                    const svo_trace_cfg* cfg, const svo_shadow_cfg* shadow,
+                                    uint32_t* h_rgba, void* stream) {
+  if (!mm || !params || !shadow || !h_rgba || !mm->impl.device_ready()) return SVO_ERR_INVALID;
+  const int rc = check_cfg(cfg);
+  if (rc != SVO_OK) return rc;
+  if (cfg->traversal != SVO_TRAVERSAL_TREELET) return SVO_ERR_NOTSUP;
+  if (shadow->reserved != 0u) return SVO_ERR_INVALID;
+  cudaStream_t s = stream ? (cudaStream_t)stream : mm->impl.render_stream();
+  return guarded([&] { return mm->impl.render_to_host_async(*params, *cfg, h_rgba, s, shadow); });
+}
+
 int svo_mm_sync(svo_mm* mm, void* stream, svo_stats* out) {
   if (!mm || !mm->impl.device_ready()) return SVO_ERR_INVALID;
   cudaStream_t s = stream ? (cudaStream_t)stream : mm->impl.render_stream();

@@ -673,7 +673,8 @@ int TreeletMemoryManagerCuda::rgba_scratch(uint64_t pixels, uint32_t** out) {
 
 int TreeletMemoryManagerCuda::render_to_host_async(const svo_frame_params& p,
                                                    const svo_trace_cfg& cfg, uint32_t* h_rgba,
-                                                   cudaStream_t stream) {
+                                                   cudaStream_t stream,
+                                                   const svo_shadow_cfg* shadow) {
   const uint64_t pixels = (uint64_t)p.width * p.height;
   if (pixels == 0) return SVO_OK;
   if (!d2h_stream_) {
@@ -698,8 +699,10 @@ int TreeletMemoryManagerCuda::render_to_host_async(const svo_frame_params& p,
   SVO_CUDA_TRY(cudaStreamWaitEvent(stream, copy_done_[k], 0));
   int rc = wait_uploads(stream);
   if (rc != SVO_OK) return rc;
-  rc = launch_render(d_nodes_, d_attribs_, incore_nodes(), p, cfg, d_img_[k], nullptr, d_stats_,
-                     stream);
+  rc = shadow ? launch_render_shadow(d_nodes_, d_attribs_, incore_nodes(), p, *shadow,
+                                     cfg.stack_size, d_img_[k], nullptr, nullptr, d_stats_, stream)
+              : launch_render(d_nodes_, d_attribs_, incore_nodes(), p, cfg, d_img_[k], nullptr,
+                              d_stats_, stream);
   if (rc != SVO_OK) return rc;
   SVO_CUDA_TRY(cudaEventRecord(cast_done_[k], stream));
   SVO_CUDA_TRY(cudaStreamWaitEvent(d2h_stream_, cast_done_[k], 0));

@@ -208,9 +208,10 @@ class TreeletMemoryManagerCuda : public TreeletMemoryManager {
   // Asynchronous host-output frames: cast on `stream` into one of two device
   // images, copied to `h_rgba` on a second stream, so the copy of a frame
   // overlaps the cast of the next.  wait_host_frames() blocks until every
-  // copy issued so far has landed.
+  // copy issued so far has landed.  With `shadow` the frame is the primary +
+  // shadow ray frame (launch_render_shadow) instead of renderToBuffer's.
   int render_to_host_async(const svo_frame_params& p, const svo_trace_cfg& cfg, uint32_t* h_rgba,
-                           cudaStream_t stream);
+                           cudaStream_t stream, const svo_shadow_cfg* shadow = nullptr);
   int wait_host_frames();
   // Device feedback-record scratch for analysis passes (grown on demand).
   int feedback_scratch(uint64_t records, svo_feedback** out);

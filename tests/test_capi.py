@@ -65,6 +65,8 @@ def test_null_arguments_are_status_codes():
     assert lib.svo_mm_render_shadow(None, ctypes.byref(p), ctypes.byref(cfg), ctypes.byref(sc), 1, None, None,
                                     None) == L.SVO_ERR_INVALID
     assert lib.svo_mm_render_host_async(None, ctypes.byref(p), ctypes.byref(cfg), 1, None) == L.SVO_ERR_INVALID
+    assert lib.svo_mm_render_shadow_host_async(None, ctypes.byref(p), ctypes.byref(cfg), ctypes.byref(sc), 1,
+                                               None) == L.SVO_ERR_INVALID
     out = ctypes.c_void_p()
     assert lib.svo_device_scene_build_mesh(None, 3, None, 1, 5, 0, None, ctypes.byref(out)) == L.SVO_ERR_INVALID
     v = (ctypes.c_float * 9)()

@@ -264,3 +264,40 @@ def test_async_host_frames_match_device(menger_mm):
         rgba, _ = gpu_frame(menger_mm, p)
         assert np.array_equal(o.numpy().view(np.uint32), rgba)
     assert st.bounds_errors == 0
+
+
+def test_async_shadow_host_frames_match_device(menger_mm):
+    """svo_mm_render_shadow_host_async, interleaved with
+    svo_mm_render_host_async on the manager's two device images: frames of
+    different sizes (one of a million pixels) in a row; every host image
+    equals the device render of the same kind."""
+    import torch
+
+    menger_mm.sync()
+    light = L.seeded_light(2)
+    sc = L.shadow_cfg(light)
+    frames = [(L.orbit_camera(s, w, h, radius=1.6).frame_params(), shadow) for s, (w, h, shadow) in
+              enumerate([(300, 200, True), (64, 48, False), (1024, 1024, True), (300, 200, True), (17, 13, False)])]
+    outs = [torch.empty((p.height, p.width), dtype=torch.int32).pin_memory() for p, _ in frames]
+    for (p, shadow), o in zip(frames, outs):
+        if shadow:
+            menger_mm.render_shadow_host_async(p, o, sc)
+        else:
+            menger_mm.render_host_async(p, o)
+    st = menger_mm.sync()
+    nodes, attribs = menger_mm.getIncoreBuffer()
+    for (p, shadow), o in zip(frames, outs):
+        if shadow:
+            want = torch.empty((p.height, p.width), dtype=torch.int32, device="cuda")
+            menger_mm.render_shadow(p, want, sc)
+            torch.cuda.synchronize()
+            want = want.cpu().numpy().view(np.uint32)
+            if p.width * p.height < 100_000:
+                assert np.array_equal(want, oracle.render_shadow(nodes, attribs, bytes(p), light)[0])
+        else:
+            want, _ = gpu_frame(menger_mm, p)
+        assert np.array_equal(o.numpy().view(np.uint32), want)
+    assert st.bounds_errors == 0
+    with pytest.raises(L.SvoError) as e:
+        menger_mm.render_shadow_host_async(frames[0][0], outs[0], sc, cfg=L.trace_cfg(L.TRAVERSAL_FLAT))
+    assert e.value.code == L.SVO_ERR_NOTSUP
