@@ -28,7 +28,7 @@ constexpr int kThreads = kBlockW * kBlockH;
 // a surface run hundreds of iterations, most rays a dozen), and raster order
 // starts some of the longest blocks last, where they run on after the other
 // SMs are done.  Large frames therefore estimate each 16x8 block's cost first
-// (its two 8x8 cells' top-left rays, cut off at kCostCap iterations) and
+// (its two 8x8 cells' centre rays, cut off at kCostCap iterations) and
 // append the block to the list of its cost bucket; block r of the frame
 // kernel then casts the r-th block of the buckets taken costliest first.
 // Every pixel is still cast by the same code: only the order the blocks
@@ -37,6 +37,9 @@ constexpr int kThreads = kBlockW * kBlockH;
 // its longest block alone.  The estimate is a chain of dependent node reads
 // per ray, so its time grows with the cap, and a low cap ranks the blocks
 // worse: frames took 0.2910, 0.2900 and 0.2965 ms with caps 40, 48 and 63.
+// The cells' centre rays rank them better than their top-left rays (0.2827
+// against 0.2873 ms); four samples a block (one per warp tile) cost more in
+// the estimate than they gained (0.297 ms).
 constexpr uint32_t kCostCap = 48;
 constexpr uint32_t kCostBuckets = kCostCap + 1;
 constexpr uint32_t kCostSamples = kBlockW / 8;  // one ray per 8x8 cell of a block
@@ -158,9 +161,12 @@ __global__ void __launch_bounds__(kThreads) block_cost_kernel(
   asm volatile("griddepcontrol.launch_dependents;");
   const bool live = i < (uint64_t)nblocks * kCostSamples;
   const uint32_t b = (uint32_t)(i / kCostSamples), c = (uint32_t)(i % kCostSamples);
-  const uint32_t x = (b % gx) * kBlockW + c * 8, y = (b / gx) * kBlockH;
+  // the cell's centre pixel (pixel 4, 4 of the 8x8 cell; clamped to the
+  // frame in cells cut by its edge)
+  const uint32_t x0 = (b % gx) * kBlockW + c * 8, y0 = (b / gx) * kBlockH;
+  const uint32_t x = min(x0 + 4u, p.width - 1u), y = min(y0 + 4u, p.height - 1u);
   uint32_t loops = 0u;
-  if (live && x < p.width && y < p.height) {
+  if (live && x0 < p.width && y0 < p.height) {
     float o[3], dx, dy, dz;
     pixel_ray(p, x, y, o, dx, dy, dz);
     loops = cast_ray<kFlat>(GlobalFetch{nodes}, num_nodes, o, dx, dy, dz, p.t_scale_ratio, S,
